@@ -1,0 +1,113 @@
+"""Seeded synthetic inputs with the shapes of the benchmark workloads.
+
+The reference benchmarks on its own generated blobs (data/artificial/create.py)
+and publishes no dataset for this path, so every workload here is a seeded
+mixture of Gaussian blobs plus uniform noise in the bounding box of the blob
+points, shuffled.  ``generate`` builds a workload with numpy on the host (small
+sizes, tests); ``generate_torch`` builds the same distribution with a torch
+generator directly on a device (the multi-GB benchmark sizes).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass(frozen=True)
+class Workload:
+    name: str
+    n: int
+    d: int
+    blobs: int
+    center_lo: float
+    center_hi: float
+    sigma_lo: float
+    sigma_hi: float
+    anisotropic: bool
+    zipf_s: float  # 0 -> equal blob sizes
+    noise: float
+    k: int
+    mpts: int
+    sample_num: int
+    iterations: int
+    seed: int
+
+
+WORKLOADS = {
+    # 100k x 12, 10 isotropic blobs (sigma 1), 5 % noise, k = mpts = 32
+    "blobs_100k_d12": Workload("blobs_100k_d12", 100_000, 12, 10, -10.0, 10.0, 1.0, 1.0,
+                               False, 0.0, 0.05, 32, 32, 16, 6, 1),
+    # 10M x 12, 100 anisotropic Zipf-sized blobs, 10 % noise
+    "blobs_10m_d12": Workload("blobs_10m_d12", 10_000_000, 12, 100, -10.0, 10.0, 0.3, 2.0,
+                              True, 1.1, 0.10, 32, 32, 16, 6, 2),
+    # 20M x 128, 1000 blobs, sigma in [0.5, 1.5], centres in [-20, 20], 5 % noise
+    "blobs_20m_d128": Workload("blobs_20m_d128", 20_000_000, 128, 1000, -20.0, 20.0, 0.5, 1.5,
+                               False, 0.0, 0.05, 32, 32, 16, 6, 3),
+    # 50M x 96, 200 Zipf-sized blobs, sigma in [0.2, 3.0], 8 % noise
+    "blobs_50m_d96": Workload("blobs_50m_d96", 50_000_000, 96, 200, -20.0, 20.0, 0.2, 3.0,
+                              False, 1.1, 0.08, 32, 32, 16, 6, 5),
+}
+
+
+def scaled(name: str, n: int, seed: int | None = None) -> Workload:
+    """The same distribution as WORKLOADS[name] with n points."""
+    w = WORKLOADS[name]
+    return Workload(w.name + f"_n{n}", n, w.d, min(w.blobs, max(1, n // 200)), w.center_lo,
+                    w.center_hi, w.sigma_lo, w.sigma_hi, w.anisotropic, w.zipf_s, w.noise, w.k,
+                    w.mpts, w.sample_num, w.iterations, w.seed if seed is None else seed)
+
+
+def _layout(w: Workload, rng: np.random.Generator):
+    n_noise = int(round(w.n * w.noise))
+    n_blob = w.n - n_noise
+    if w.zipf_s > 0:
+        p = np.arange(1, w.blobs + 1, dtype=np.float64) ** (-w.zipf_s)
+    else:
+        p = np.ones(w.blobs)
+    p /= p.sum()
+    sizes = np.floor(p * n_blob).astype(np.int64)
+    sizes[: n_blob - sizes.sum()] += 1
+    centers = rng.uniform(w.center_lo, w.center_hi, size=(w.blobs, w.d))
+    if w.anisotropic:
+        sigmas = rng.uniform(w.sigma_lo, w.sigma_hi, size=(w.blobs, w.d))
+    else:
+        sigmas = np.repeat(rng.uniform(w.sigma_lo, w.sigma_hi, size=(w.blobs, 1)), w.d, axis=1)
+    return sizes, centers, sigmas, n_noise
+
+
+def generate(w: Workload) -> np.ndarray:
+    """float32 [n, d] on the host (numpy PCG64 seeded with w.seed)."""
+    rng = np.random.default_rng(w.seed)
+    sizes, centers, sigmas, n_noise = _layout(w, rng)
+    parts = [rng.normal(centers[b], sigmas[b], size=(int(sizes[b]), w.d)) for b in range(w.blobs)]
+    X = np.concatenate(parts, axis=0) if parts else np.zeros((0, w.d))
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    noise = rng.uniform(lo, hi, size=(n_noise, w.d))
+    X = np.concatenate([X, noise], axis=0).astype(np.float32)
+    return X[rng.permutation(w.n)]
+
+
+def generate_torch(w: Workload, device="cuda"):
+    """The same distribution built on `device` with a seeded torch generator."""
+    import torch
+
+    rng = np.random.default_rng(w.seed)
+    sizes, centers, sigmas, n_noise = _layout(w, rng)
+    g = torch.Generator(device=device)
+    g.manual_seed(w.seed)
+    X = torch.empty((w.n, w.d), dtype=torch.float32, device=device)
+    row = 0
+    for b in range(w.blobs):
+        m = int(sizes[b])
+        if m == 0:
+            continue
+        c = torch.as_tensor(centers[b], dtype=torch.float32, device=device)
+        s = torch.as_tensor(sigmas[b], dtype=torch.float32, device=device)
+        X[row:row + m].normal_(generator=g).mul_(s).add_(c)
+        row += m
+    lo = X[:row].amin(dim=0)
+    hi = X[:row].amax(dim=0)
+    X[row:].uniform_(generator=g).mul_(hi - lo).add_(lo)
+    perm = torch.randperm(w.n, generator=g, device=device)
+    return X[perm].contiguous()
