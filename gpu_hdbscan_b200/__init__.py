@@ -1,0 +1,234 @@
+"""B200-native HDBSCAN path (libhdb_b200.so) -- Python front end.
+
+The functions below mirror the reference's C++ stage interface, in the order
+HDBSCAN/_new.cu calls them:
+
+    NNDescent            gpuknn::NNDescent          (gpuknn/nndescent.cuh:40-42)
+    fix_distances        fix_distances              (build_kNNG.cu:131-174)
+    buildEnhancedKNNG    buildEnhancedKNNG          (HDBSCAN/graphs/graph.cuh:24)
+    buildMST             cpuMST + buildMST          (HDBSCAN/mst/mst.cuh:64,91)
+    sort_edges           sort_edges                 (HDBSCAN/merge_sort/merge_sort.cuh:30)
+    build_Linkage_tree   build_Linkage_tree         (HDBSCAN/trees/tree.cuh:33)
+    get_clusters         build_Condensed_tree + compute_stability + get_clusters
+                                                    (HDBSCAN/trees/tree.cuh:39-45)
+    hdbscan              the whole HDBSCAN/_new.cu order
+
+Arrays are torch tensors on the context's CUDA device (PyTorch only provides
+device memory and streams here; all compute is in libhdb_b200.so).  Errors
+raise HdbError with the library's status and message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+from . import _lib
+from ._lib import (HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP32, HDB_STAB_FP32,
+                   HDB_STAB_FP64, HdbError)
+
+__all__ = ["Context", "HdbError", "EnhancedGraph", "HDB_PREC_FP32", "HDB_PREC_BF16",
+           "HDB_DIST_SQRT", "HDB_DIST_SQUARED", "HDB_STAB_FP32", "HDB_STAB_FP64"]
+
+
+def _ptr(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+@dataclass
+class EnhancedGraph:
+    """ECLgraph (HDBSCAN/structs/ECLgraph.h:41-47): views of context-owned memory,
+    valid until the next buildEnhancedKNNG on the same context."""
+    nodes: int
+    edges: int
+    nindex: "object"
+    nlist: "object"
+    eweight: "object"
+    antihubs: "object"
+    raw: _lib.Graph
+
+
+class Context:
+    """One device, one stream (libhdb_b200 hdb_ctx)."""
+
+    def __init__(self, device: int = 0):
+        import torch
+
+        self._torch = torch
+        self.L = _lib.load()
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        h = C.c_void_p()
+        _lib.check(self.L.hdb_create(C.byref(h), device))
+        self.h = h
+        # run on torch's current stream so torch allocations order correctly
+        _lib.check(self.L.hdb_set_stream(self.h, C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hdb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- helpers ----------------------------------------------------------
+    def _dev(self, t, dtype):
+        torch = self._torch
+        t = torch.as_tensor(t)
+        return t.to(device=self.device, dtype=dtype).contiguous()
+
+    # -- stages -----------------------------------------------------------
+    def NNDescent(self, X, k=32, sample_num=16, iterations=6, precision=HDB_PREC_FP32):
+        """X [n, d] float32 -> G [n, k, 2] int32 (NNDElement rows: distance bits, label)."""
+        torch = self._torch
+        X = self._dev(X, torch.float32)
+        n, d = X.shape
+        G = torch.empty((n, k, 2), dtype=torch.int32, device=self.device)
+        p = _lib.KnnParams(k, sample_num, iterations, precision)
+        _lib.check(self.L.hdb_nndescent(self.h, _ptr(X), n, d, C.byref(p), _ptr(G)))
+        return G
+
+    def knn_split(self, G):
+        """G [n, k, 2] -> (ids int32 [n, k] with the old/new flag decoded, dist float32)."""
+        torch = self._torch
+        n, k, _ = G.shape
+        ids = torch.empty((n, k), dtype=torch.int32, device=self.device)
+        dist = torch.empty((n, k), dtype=torch.float32, device=self.device)
+        _lib.check(self.L.hdb_knn_split(self.h, _ptr(G), n, k, _ptr(ids), _ptr(dist)))
+        return ids, dist
+
+    def fix_distances(self, X, ids):
+        torch = self._torch
+        X = self._dev(X, torch.float32)
+        ids = self._dev(ids, torch.int32)
+        n, k = ids.shape
+        dist = torch.empty((n, k), dtype=torch.float32, device=self.device)
+        _lib.check(self.L.hdb_fix_distances(self.h, _ptr(X), n, X.shape[1], _ptr(ids), k,
+                                            _ptr(dist)))
+        return dist
+
+    def buildEnhancedKNNG(self, ids, dist, X) -> EnhancedGraph:
+        torch = self._torch
+        ids = self._dev(ids, torch.int32)
+        dist = self._dev(dist, torch.float32)
+        X = self._dev(X, torch.float32)
+        n, k = ids.shape
+        g = _lib.Graph()
+        _lib.check(self.L.hdb_enhanced_knng(self.h, _ptr(ids), _ptr(dist), _ptr(X), n,
+                                            X.shape[1], k, C.byref(g)))
+        return EnhancedGraph(g.nodes, g.edges, self._view(g.nindex, g.nodes + 1, torch.int64),
+                             self._view(g.nlist, g.edges, torch.int32),
+                             self._view(g.eweight, g.edges, torch.float32),
+                             self._view(g.antihubs, g.num_antihubs, torch.int32), g)
+
+    def _view(self, ptr, count, dtype):
+        """Copies `count` elements of context-owned device memory into a tensor."""
+        torch = self._torch
+        out = torch.empty(count, dtype=dtype, device=self.device)
+        if count:
+            torch.cuda.synchronize(self.device)
+            res = _cudart().cudaMemcpy(C.c_void_p(out.data_ptr()), C.c_void_p(ptr),
+                                       C.c_size_t(count * out.element_size()), 3)
+            if res != 0:
+                raise HdbError(_lib.HDB_ERR_CUDA, f"cudaMemcpy failed ({res})")
+        return out
+
+    def buildMST(self, graph: EnhancedGraph, with_in_mst=False):
+        """-> (mst [n-1, 3] int32 view of MSTedge sorted by (weight, edge index),
+               in_mst uint8 [edges] or None, Boruvka rounds)."""
+        torch = self._torch
+        n = graph.nodes
+        mst = torch.empty((n - 1, 3), dtype=torch.int32, device=self.device)
+        inm = torch.empty(graph.edges, dtype=torch.uint8, device=self.device) if with_in_mst else None
+        rounds = C.c_int32(0)
+        _lib.check(self.L.hdb_mst(self.h, C.byref(graph.raw), _ptr(inm), _ptr(mst),
+                                  C.byref(rounds)))
+        return mst, inm, rounds.value
+
+    def sort_edges(self, mst):
+        """In place: stable ascending sort of MSTedge rows by weight."""
+        _lib.check(self.L.hdb_sort_edges(self.h, _ptr(mst), mst.shape[0]))
+        return mst
+
+    def build_Linkage_tree(self, mst, n):
+        torch = self._torch
+        hier = torch.empty((n - 1, 4), dtype=torch.int32, device=self.device)
+        _lib.check(self.L.hdb_linkage_tree(self.h, _ptr(mst), n, _ptr(hier)))
+        return hier
+
+    def get_clusters(self, hier, n, mpts, stability=HDB_STAB_FP32, want_tree=False):
+        """-> (labels int32 [n], num_clusters, condensed [rows, 4] or None,
+               stabilities [C, 2] or None)."""
+        torch = self._torch
+        labels = torch.empty(n, dtype=torch.int32, device=self.device)
+        ncl = C.c_int32(0)
+        cond = stab = None
+        csize = C.c_int64(0)
+        nst = C.c_int64(0)
+        if want_tree:
+            cap = n + 2 * (n // max(mpts, 1)) + 2
+            cond = torch.empty((cap, 4), dtype=torch.int32, device=self.device)
+            stab = torch.empty((cap, 2), dtype=torch.int32, device=self.device)
+        _lib.check(self.L.hdb_condense_select(self.h, _ptr(hier), n, mpts, stability, _ptr(labels),
+                                              C.byref(ncl), _ptr(cond), C.byref(csize), _ptr(stab),
+                                              C.byref(nst)))
+        if want_tree:
+            cond = cond[: csize.value]
+            stab = stab[: nst.value]
+        return labels, ncl.value, cond, stab
+
+    def hdbscan(self, X, k=32, mpts=32, sample_num=16, iterations=6, precision=HDB_PREC_FP32,
+                distance=HDB_DIST_SQRT, stability=HDB_STAB_FP32, labels_out=None):
+        """The whole path (hdb_run).  X on the host (numpy / CPU tensor) runs with
+        host_io=1: the H2D copy of X and the D2H copy of the labels are inside
+        the call.  X on the device returns device labels."""
+        torch = self._torch
+        host = not (isinstance(X, torch.Tensor) and X.is_cuda)
+        if host:
+            X = torch.as_tensor(X, dtype=torch.float32).contiguous()
+            labels = labels_out if labels_out is not None else torch.empty(X.shape[0], dtype=torch.int32)
+        else:
+            X = X.to(torch.float32).contiguous()
+            labels = labels_out if labels_out is not None else torch.empty(
+                X.shape[0], dtype=torch.int32, device=self.device)
+        n, d = X.shape
+        p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
+                        stability, 1 if host else 0)
+        st = _lib.RunStats()
+        _lib.check(self.L.hdb_run(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels), C.byref(st)))
+        return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
+
+
+_CUDART = None
+
+
+def _cudart():
+    """The CUDA runtime, for device-to-device copies out of context-owned memory."""
+    global _CUDART
+    if _CUDART is None:
+        import glob
+        import os
+        cands = ["libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so.12"]
+        try:
+            import nvidia.cuda_runtime as _nv  # pip CUDA runtime shipped with torch
+            cands += glob.glob(os.path.join(list(_nv.__path__)[0], "lib", "libcudart.so*"))
+        except Exception:
+            pass
+        for c in cands:
+            try:
+                _CUDART = C.CDLL(c)
+                break
+            except OSError:
+                continue
+        if _CUDART is None:
+            raise ImportError("libcudart.so.12 not found")
+        _CUDART.cudaMemcpy.restype = C.c_int
+        _CUDART.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    return _CUDART
+
+
+def version() -> str:
+    return _lib.load().hdb_version().decode()

@@ -1,0 +1,220 @@
+// extern "C" entry points of libhdb_b200 (include/hdb/hdb.h) and the
+// end-to-end pipeline in the reference's HDBSCAN/_new.cu order.
+#include "graph.cuh"
+#include "hdb_internal.cuh"
+#include "knn.cuh"
+#include "mst.cuh"
+#include "trees.cuh"
+
+using namespace hdb;
+
+namespace {
+
+Context *C(hdb_ctx *h) {
+  HDB_REQUIRE(h != nullptr, HDB_ERR_ARG, "NULL context");
+  HDB_CUDA(cudaSetDevice(h->c.device));
+  return &h->c;
+}
+
+void require_ptr(const void *p, const char *what) {
+  HDB_REQUIRE(p != nullptr, HDB_ERR_ARG, std::string("NULL pointer: ") + what);
+}
+
+void check_knn_params(const hdb_knn_params *p) {
+  require_ptr(p, "params");
+  HDB_REQUIRE(p->k >= 1 && p->k <= 32, HDB_ERR_ARG, "k (NEIGHB_NUM_PER_LIST) must be in [1, 32]");
+  HDB_REQUIRE(p->sample_num >= 1 && 2 * p->sample_num <= p->k, HDB_ERR_ARG,
+              "SAMPLE_NUM must satisfy 2*SAMPLE_NUM <= k");
+  HDB_REQUIRE(p->iterations >= 0 && p->iterations <= 1000, HDB_ERR_ARG,
+              "NND_ITERATION must be in [0, 1000]");
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  HDB_CUDA(cudaEventElapsedTime(&ms, a, b));
+  return ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+HDB_API hdb_status hdb_nndescent(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                                 const hdb_knn_params *params, hdb_nnd_element *G) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(X, "X");
+    require_ptr(G, "G");
+    check_knn_params(params);
+    nndescent(ctx, X, n, d, *params, G, nullptr);
+  });
+}
+
+HDB_API hdb_status hdb_knn_split(hdb_ctx *h, const hdb_nnd_element *G, int64_t n, int32_t k,
+                                 int32_t *ids, float *dist) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(G, "G");
+    HDB_REQUIRE(n >= 0 && k >= 1, HDB_ERR_ARG, "bad n or k");
+    knn_split(ctx, G, n, k, ids, dist);
+    ctx->sync();
+  });
+}
+
+HDB_API hdb_status hdb_fix_distances(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                                     const int32_t *ids, int32_t k, float *dist) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(X, "X");
+    require_ptr(ids, "ids");
+    require_ptr(dist, "dist");
+    HDB_REQUIRE(n >= 0 && k >= 1 && d >= 1, HDB_ERR_ARG, "bad n, k or d");
+    fix_distances(ctx, X, n, d, ids, k, dist);
+    ctx->sync();
+  });
+}
+
+HDB_API hdb_status hdb_enhanced_knng(hdb_ctx *h, const int32_t *ids, const float *dist,
+                                     const float *X, int64_t n, int32_t d, int32_t k,
+                                     hdb_graph *graph) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(ids, "ids");
+    require_ptr(dist, "dist");
+    require_ptr(X, "X");
+    require_ptr(graph, "graph");
+    HDB_REQUIRE(n >= 2 && k >= 1 && k <= 32 && k < n && d >= 1, HDB_ERR_ARG,
+                "enhanced kNN graph: need n >= 2, 1 <= k <= 32, k < n, d >= 1");
+    Buf<float> core(ctx, n);
+    core_distances(ctx, dist, X, ids, n, d, k, HDB_DIST_SQUARED, core);
+    build_enhanced_knng(ctx, ids, core, X, n, d, k, graph, nullptr);
+  });
+}
+
+HDB_API hdb_status hdb_mst(hdb_ctx *h, const hdb_graph *graph, uint8_t *in_mst, hdb_mst_edge *mst,
+                           int32_t *rounds) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(graph, "graph");
+    require_ptr(mst, "mst");
+    boruvka_mst(ctx, graph, in_mst, mst, rounds);
+  });
+}
+
+HDB_API hdb_status hdb_sort_edges(hdb_ctx *h, hdb_mst_edge *edges, int64_t m) {
+  return guard([&] {
+    Context *ctx = C(h);
+    HDB_REQUIRE(m >= 0, HDB_ERR_ARG, "negative edge count");
+    if (m > 0) require_ptr(edges, "edges");
+    HDB_REQUIRE(m < (int64_t(1) << 32), HDB_ERR_ARG, "sort_edges: 2^32 or more edges");
+    sort_mst_edges(ctx, edges, m);
+  });
+}
+
+HDB_API hdb_status hdb_linkage_tree(hdb_ctx *h, const hdb_mst_edge *sorted, int64_t n,
+                                    hdb_linkage_node *hierarchy) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(sorted, "sorted");
+    require_ptr(hierarchy, "hierarchy");
+    linkage_tree(ctx, sorted, n, hierarchy);
+  });
+}
+
+HDB_API hdb_status hdb_condense_select(hdb_ctx *h, const hdb_linkage_node *hierarchy, int64_t n,
+                                       int32_t mpts, int32_t stability_mode, int32_t *labels,
+                                       int32_t *num_clusters, hdb_condensed_node *condensed,
+                                       int64_t *condensed_size, hdb_stability *stability,
+                                       int64_t *num_stability) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(hierarchy, "hierarchy");
+    require_ptr(labels, "labels");
+    HDB_REQUIRE(stability_mode == HDB_STAB_FP32 || stability_mode == HDB_STAB_FP64, HDB_ERR_ARG,
+                "unknown stability mode");
+    int32_t nc = 0;
+    condense_select(ctx, hierarchy, n, mpts, stability_mode, labels, &nc, condensed,
+                    condensed_size, stability, num_stability);
+    if (num_clusters) *num_clusters = nc;
+  });
+}
+
+HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                           const hdb_params *params, int32_t *labels, hdb_run_stats *stats) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(X, "X");
+    require_ptr(labels, "labels");
+    require_ptr(params, "params");
+    check_knn_params(&params->knn);
+    const hdb_params &p = *params;
+    const int32_t k = p.knn.k;
+    HDB_REQUIRE(p.mpts >= 2 && p.mpts <= k, HDB_ERR_ARG, "mpts must satisfy 2 <= mpts <= k");
+    HDB_REQUIRE(p.distance == HDB_DIST_SQRT || p.distance == HDB_DIST_SQUARED, HDB_ERR_ARG,
+                "unknown distance mode");
+    HDB_REQUIRE(p.stability == HDB_STAB_FP32 || p.stability == HDB_STAB_FP64, HDB_ERR_ARG,
+                "unknown stability mode");
+    HDB_REQUIRE(n > k && d >= 1, HDB_ERR_ARG, "need n > k and d >= 1");
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t *ev = ctx->ev;
+    HDB_CUDA(cudaEventRecord(ev[0], st));
+    Buf<float> Xd;
+    Buf<int32_t> Ld;
+    const float *Xuse = X;
+    int32_t *Luse = labels;
+    if (p.host_io) {
+      Xd = Buf<float>(ctx, (size_t)n * d);
+      Ld = Buf<int32_t>(ctx, n);
+      HDB_CUDA(cudaMemcpyAsync(Xd, X, (size_t)n * d * sizeof(float), cudaMemcpyHostToDevice, st));
+      Xuse = Xd;
+      Luse = Ld;
+    }
+    HDB_CUDA(cudaEventRecord(ev[1], st));
+    int64_t dropped = 0;
+    Buf<int32_t> ids(ctx, (size_t)n * k);
+    Buf<float> core(ctx, n);
+    {
+      Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
+      nndescent(ctx, Xuse, n, d, p.knn, G, &dropped);
+      HDB_CUDA(cudaEventRecord(ev[2], st));
+      Buf<float> dist;
+      if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
+      knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
+      core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
+    }
+    hdb_graph g;
+    build_enhanced_knng(ctx, ids, core, Xuse, n, d, k, &g, nullptr);
+    HDB_CUDA(cudaEventRecord(ev[3], st));
+    int32_t rounds = 0;
+    Buf<hdb_mst_edge> mst(ctx, n - 1);
+    boruvka_mst(ctx, &g, nullptr, mst, &rounds);
+    HDB_CUDA(cudaEventRecord(ev[4], st));
+    int32_t ncl = 0;
+    {
+      Buf<hdb_linkage_node> hier(ctx, n - 1);
+      linkage_tree(ctx, mst, n, hier);
+      condense_select(ctx, hier, n, p.mpts, p.stability, Luse, &ncl, nullptr, nullptr, nullptr,
+                      nullptr);
+    }
+    HDB_CUDA(cudaEventRecord(ev[5], st));
+    if (p.host_io)
+      HDB_CUDA(cudaMemcpyAsync(labels, Luse, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    HDB_CUDA(cudaEventRecord(ev[6], st));
+    ctx->sync();
+    if (stats) {
+      stats->edges = g.edges;
+      stats->num_antihubs = g.num_antihubs;
+      stats->num_clusters = ncl;
+      stats->condensed_size = 0;
+      stats->mst_rounds = rounds;
+      stats->knn_dropped = dropped;
+      stats->ms_knn = elapsed(ev[1], ev[2]);
+      stats->ms_graph = elapsed(ev[2], ev[3]);
+      stats->ms_mst = elapsed(ev[3], ev[4]);
+      stats->ms_tree = elapsed(ev[4], ev[5]);
+      stats->ms_total = elapsed(ev[0], ev[6]);
+    }
+  });
+}
+
+}  // extern "C"

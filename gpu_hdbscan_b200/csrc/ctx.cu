@@ -1,0 +1,142 @@
+// Context management, error reporting and stream-ordered scratch memory.
+#include <cstdio>
+#include <cstring>
+
+#include "hdb_internal.cuh"
+
+namespace hdb {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+void throw_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error %d (%s) at %s:%d: %s", (int)e, cudaGetErrorString(e),
+           file, line, what);
+  hdb_status s = (e == cudaErrorMemoryAllocation) ? HDB_ERR_ALLOC : HDB_ERR_CUDA;
+  throw Error(s, buf);
+}
+
+Scratch::Scratch(Context *ctx, size_t bytes) { reset(ctx, bytes); }
+
+void Scratch::reset(Context *ctx, size_t bytes) {
+  if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+  ptr_ = nullptr;
+  ctx_ = ctx;
+  bytes_ = bytes;
+  if (bytes == 0) bytes = 16;
+  HDB_CUDA(cudaMallocAsync(&ptr_, bytes, ctx->stream));
+}
+
+Scratch &Scratch::operator=(Scratch &&o) noexcept {
+  if (this != &o) {
+    if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+    ctx_ = o.ctx_;
+    ptr_ = o.ptr_;
+    bytes_ = o.bytes_;
+    o.ptr_ = nullptr;
+    o.bytes_ = 0;
+  }
+  return *this;
+}
+
+Scratch::~Scratch() {
+  if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+}
+
+void Context::sync() { HDB_CUDA(cudaStreamSynchronize(stream)); }
+
+uint32_t Context::take_dev_err() {
+  uint32_t *h = static_cast<uint32_t *>(pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+  HDB_CUDA(cudaMemsetAsync(dev_err, 0, sizeof(uint32_t), stream));
+  sync();
+  return h[0];
+}
+
+void ensure_capacity(Context *ctx, void **ptr, size_t *cap, size_t bytes) {
+  if (bytes <= *cap && *ptr) return;
+  if (*ptr) {
+    HDB_CUDA(cudaStreamSynchronize(ctx->stream));
+    HDB_CUDA(cudaFree(*ptr));
+    *ptr = nullptr;
+    *cap = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  HDB_CUDA(cudaMalloc(ptr, want));
+  *cap = want;
+}
+
+}  // namespace hdb
+
+using namespace hdb;
+
+extern "C" {
+
+HDB_API const char *hdb_version(void) { return "hdb_b200 0.1.0 (sm_100a)"; }
+
+HDB_API const char *hdb_last_error(void) { return g_last_error.c_str(); }
+
+HDB_API hdb_status hdb_create(hdb_ctx **out, int32_t device) {
+  return guard([&] {
+    HDB_REQUIRE(out != nullptr, HDB_ERR_ARG, "hdb_create: out is NULL");
+    int count = 0;
+    HDB_CUDA(cudaGetDeviceCount(&count));
+    HDB_REQUIRE(device >= 0 && device < count, HDB_ERR_ARG, "hdb_create: no such device");
+    HDB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    HDB_CUDA(cudaGetDeviceProperties(&prop, device));
+    HDB_REQUIRE(prop.major == 10 && prop.minor == 0, HDB_ERR_ARG,
+                "hdb_create: libhdb_b200 is built for sm_100a (B200) only");
+    hdb_ctx *h = new hdb_ctx();
+    Context &c = h->c;
+    c.device = device;
+    c.num_sms = prop.multiProcessorCount;
+    try {
+      HDB_CUDA(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
+      c.stream = c.own_stream;
+      HDB_CUDA(cudaMalloc(&c.dev_err, 4 * sizeof(uint32_t)));
+      HDB_CUDA(cudaMemset(c.dev_err, 0, 4 * sizeof(uint32_t)));
+      HDB_CUDA(cudaMallocHost(&c.pinned, 4096));
+      for (auto &e : c.ev) HDB_CUDA(cudaEventCreate(&e));
+      // Keep freed scratch cached in the stream-ordered pool between calls.
+      cudaMemPool_t pool;
+      HDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+      uint64_t thr = UINT64_MAX;
+      HDB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    } catch (...) {
+      hdb_destroy(h);
+      throw;
+    }
+    *out = h;
+  });
+}
+
+HDB_API hdb_status hdb_destroy(hdb_ctx *h) {
+  if (!h) return HDB_OK;
+  return guard([&] {
+    Context &c = h->c;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    cudaFree(c.g_nindex);
+    cudaFree(c.g_nlist);
+    cudaFree(c.g_eweight);
+    cudaFree(c.g_antihubs);
+    cudaFree(c.dev_err);
+    if (c.pinned) cudaFreeHost(c.pinned);
+    for (auto &e : c.ev)
+      if (e) cudaEventDestroy(e);
+    if (c.own_stream) cudaStreamDestroy(c.own_stream);
+    delete h;
+  });
+}
+
+HDB_API hdb_status hdb_set_stream(hdb_ctx *h, void *stream) {
+  return guard([&] {
+    HDB_REQUIRE(h != nullptr, HDB_ERR_ARG, "hdb_set_stream: NULL context");
+    h->c.stream = stream ? static_cast<cudaStream_t>(stream) : h->c.own_stream;
+  });
+}
+
+}  // extern "C"

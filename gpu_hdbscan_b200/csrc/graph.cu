@@ -1,0 +1,417 @@
+// Enhanced kNN graph: in-degrees, antihub selection, the symmetric CSR with
+// the antihub clique, core distances and mutual-reachability weights.
+//
+// Reference: buildEnhancedKNNG / buildECLgraph (HDBSCAN/graphs/graph.cu:16-176)
+// with calculate_degrees (calculates.cu:448-473, counts/count.cu:10-110),
+// calculate_nindex / calculate_nlist (calculates.cu:286-410),
+// calculateCoreDistance (calculates.cu:185-197), calculateMRD (:61-82) and
+// calculate_coreDistance_antihubs (:412-446).  The reference does these as
+// serial host loops plus sharded 3-GPU kernels; here every step is a
+// single-device pass over HBM-resident arrays.
+#include "hdb_internal.cuh"
+#include "graph.cuh"
+
+namespace hdb {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 8;
+constexpr int kDegHistBins = 65536;
+
+// Squared-free sqrt-L2 with the reference's rounding (build_kNNG.cu:4-13,
+// calculates.cu:275-283): float accumulator, each term pow(float diff, 2)
+// evaluated in double, sqrt of the float sum.
+__device__ __forceinline__ float euclid_ref(const float *__restrict__ a,
+                                           const float *__restrict__ b, int d) {
+  float soma = 0.0f;
+  for (int i = 0; i < d; i++) {
+    float diff = __fsub_rn(a[i], b[i]);
+    double sq = __dmul_rn((double)diff, (double)diff);
+    soma = __double2float_rn(__dadd_rn((double)soma, sq));
+  }
+  return __fsqrt_rn(soma);
+}
+
+// One warp per row: validate the row (range, self, duplicates) and count
+// in-degrees (countValues, count.cu:10-19).
+__global__ void k_degrees(const int32_t *__restrict__ ids, int64_t n, int k,
+                          int32_t *__restrict__ deg, uint32_t *err) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  for (; row < n; row += stride) {
+    int32_t v = lane < k ? ids[row * k + lane] : -1 - lane;
+    uint32_t bad = 0;
+    if (lane < k) {
+      if (v < 0 || v >= n) bad |= DEVERR_ID_RANGE;
+      else if (v == row) bad |= DEVERR_SELF_ID;
+    }
+    uint32_t peers = __match_any_sync(0xffffffffu, v);
+    if (lane < k && __popc(peers) > 1) bad |= DEVERR_DUP_ID;
+    if (bad) atomicOr(err, bad);
+    else if (lane < k) atomicAdd(&deg[v], 1);
+  }
+}
+
+// Histogram of degrees (clamped to the last bin), warp-aggregated.
+__global__ void k_degree_hist(const int32_t *__restrict__ deg, int64_t n,
+                              uint32_t *__restrict__ hist) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; i - threadIdx.x < n; i += stride) {
+    bool ok = i < n;
+    int v = ok ? min(deg[i], kDegHistBins - 1) : -1;
+    uint32_t peers = __match_any_sync(0xffffffffu, v);
+    if (ok && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[v], __popc(peers));
+  }
+}
+
+// Finds the threshold degree T = the P-th smallest degree.  out[0] = T,
+// out[1] = #{deg < T}, out[2] = #{deg == T}.  One block of 1024 threads, each
+// owning a chunk of 64 bins.
+__global__ void k_find_threshold(const uint32_t *__restrict__ hist, int64_t P, int64_t *out) {
+  __shared__ int64_t chunk_sum[1024];
+  const int per = kDegHistBins / 1024;
+  int64_t s = 0;
+  for (int b = 0; b < per; b++) s += hist[threadIdx.x * per + b];
+  chunk_sum[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t cum = 0;
+    int c = 0;
+    while (c < 1024 && cum + chunk_sum[c] < P) cum += chunk_sum[c++];
+    int64_t T = -1, below = 0, at = 0;
+    if (c < 1024) {
+      for (int b = c * per; b < (c + 1) * per; b++) {
+        if (cum + (int64_t)hist[b] >= P) {
+          T = b;
+          below = cum;
+          at = hist[b];
+          break;
+        }
+        cum += hist[b];
+      }
+    }
+    out[0] = T;
+    out[1] = below;
+    out[2] = at;
+  }
+}
+
+__global__ void k_flag_eq(const int32_t *__restrict__ deg, int64_t n, int32_t T,
+                          int32_t *__restrict__ flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = deg[i] == T;
+}
+
+// Tied vertices (deg == T) in index order with calculateScore's tie score
+// (calculates.cu:21-36): sum of the neighbours' degrees.
+__global__ void k_tie_keys(const int32_t *__restrict__ deg, const int32_t *__restrict__ flag,
+                           const int64_t *__restrict__ pos, const int32_t *__restrict__ ids,
+                           int64_t n, int k, uint64_t *__restrict__ keys) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    int32_t score = 0;
+    for (int j = 0; j < k; j++) score += deg[ids[i * k + j]];
+    keys[pos[i]] = ((uint64_t)(uint32_t)score << 32) | (uint64_t)(uint32_t)i;
+  }
+}
+
+__global__ void k_mark_selected_ties(const uint64_t *__restrict__ keys, int64_t missing,
+                                     int32_t *__restrict__ is_ah) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < missing;
+       t += (int64_t)gridDim.x * blockDim.x)
+    is_ah[(uint32_t)keys[t]] = 1;
+}
+
+__global__ void k_flag_below(const int32_t *__restrict__ deg, int64_t n, int32_t T,
+                             int32_t *__restrict__ is_ah, int all_ties) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    is_ah[i] = deg[i] < T || (all_ties && deg[i] == T);
+}
+
+__global__ void k_compact_flags(const int32_t *__restrict__ flag, const int64_t *__restrict__ pos,
+                                int64_t n, int32_t *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (flag[i]) out[pos[i]] = (int32_t)i;
+}
+
+// One warp per row i: which of i's neighbours list i back (findKNNlist,
+// getters.cu:41-49).  Non-mutual edges i->v become reverse entries of v.
+__global__ void k_mutual(const int32_t *__restrict__ ids, int64_t n, int k,
+                         uint32_t *__restrict__ mutual, int32_t *__restrict__ revcnt,
+                         int32_t *__restrict__ nonmutual) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  for (; row < n; row += stride) {
+    bool found = false;
+    int32_t v = -1;
+    if (lane < k) {
+      v = ids[row * k + lane];
+      const int32_t *r = ids + (int64_t)v * k;
+      if ((k & 3) == 0) {
+        const int4 *r4 = reinterpret_cast<const int4 *>(r);
+        for (int t = 0; t < (k >> 2); t++) {
+          int4 q = __ldg(r4 + t);
+          found |= (q.x == row) | (q.y == row) | (q.z == row) | (q.w == row);
+        }
+      } else {
+        for (int t = 0; t < k; t++) found |= (__ldg(r + t) == row);
+      }
+    }
+    uint32_t m = __ballot_sync(0xffffffffu, found);
+    if (lane < k && !found) atomicAdd(&revcnt[v], 1);
+    if (lane == 0) {
+      mutual[row] = m;
+      nonmutual[row] = k - __popc(m);
+    }
+  }
+}
+
+__global__ void k_row_sizes(const int32_t *__restrict__ revcnt, const int32_t *__restrict__ is_ah,
+                            int64_t n, int k, int32_t P, int32_t *__restrict__ sizes) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    sizes[i] = k + revcnt[i] + (is_ah[i] ? P - 1 : 0);
+}
+
+// Emits (v, i) for every non-mutual edge i->v in (i, j) order.
+__global__ void k_emit_reverse(const int32_t *__restrict__ ids, const uint32_t *__restrict__ mutual,
+                               const int64_t *__restrict__ off, int64_t n, int k,
+                               uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  const uint32_t valid = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+  for (; row < n; row += stride) {
+    uint32_t nm = ~mutual[row] & valid;
+    if (lane < k && ((nm >> lane) & 1u)) {
+      int64_t p = off[row] + __popc(nm & lanemask_lt());
+      keys[p] = (uint32_t)ids[row * k + lane];
+      vals[p] = (uint32_t)row;
+    }
+  }
+}
+
+__global__ void k_core_from_dist(const float *__restrict__ dist, int64_t n, int k,
+                                 float *__restrict__ core) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    core[i] = dist[i * k + (k - 1)];
+}
+
+// Core distance as the reference's fix_distances would give it for the k-th
+// neighbour (only that entry of each row reaches the MRD weights).
+__global__ void k_core_sqrt(const float *__restrict__ X, const int32_t *__restrict__ ids,
+                            int64_t n, int d, int k, float *__restrict__ core) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t v = ids[i * k + (k - 1)];
+    core[i] = euclid_ref(X + i * d, X + v * d, d);
+  }
+}
+
+__device__ __forceinline__ float mrd(float a, float b) { return a > b ? a : b; }
+
+// One warp per row: own kNN ids, then the sorted reverse entries, with MRD
+// weights (calculate_nlist calculates.cu:340-390, calculateMRD :61-82).
+__global__ void k_fill(const int32_t *__restrict__ ids, const float *__restrict__ core,
+                       const int64_t *__restrict__ nindex, const int32_t *__restrict__ revcnt,
+                       const int64_t *__restrict__ rev_off, const uint32_t *__restrict__ rev_src,
+                       int64_t n, int k, int32_t *__restrict__ nlist,
+                       float *__restrict__ eweight) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  for (; row < n; row += stride) {
+    const int64_t base = nindex[row];
+    const float cr = core[row];
+    if (lane < k) {
+      int32_t u = ids[row * k + lane];
+      nlist[base + lane] = u;
+      eweight[base + lane] = mrd(cr, core[u]);
+    }
+    const int32_t rc = revcnt[row];
+    const int64_t ro = rev_off[row];
+    for (int t = lane; t < rc; t += 32) {
+      int32_t s = (int32_t)rev_src[ro + t];
+      nlist[base + k + t] = s;
+      eweight[base + k + t] = mrd(cr, core[s]);
+    }
+  }
+}
+
+__global__ void k_gather_rows(const float *__restrict__ X, const int32_t *__restrict__ rows,
+                              int64_t m, int d, float *__restrict__ out) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m * d;
+       t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = X[(int64_t)rows[t / d] * d + (t % d)];
+}
+
+// One block per antihub row: the other antihubs in ascending order with
+// max(MRD, sqrt-L2) weights (calculate_nlist :392-407 and
+// calculate_coreDistance_antihubs :412-446).
+__global__ void k_clique(const int32_t *__restrict__ ah, int32_t P, const float *__restrict__ Xah,
+                         int d, const float *__restrict__ core, const int64_t *__restrict__ nindex,
+                         const int32_t *__restrict__ revcnt, int k, int32_t *__restrict__ nlist,
+                         float *__restrict__ eweight) {
+  extern __shared__ float xa[];
+  const int r = blockIdx.x;
+  const int32_t a = ah[r];
+  for (int t = threadIdx.x; t < d; t += blockDim.x) xa[t] = Xah[(int64_t)r * d + t];
+  __syncthreads();
+  const int64_t base = nindex[a] + k + revcnt[a];
+  const float ca = core[a];
+  for (int t = threadIdx.x; t < P - 1; t += blockDim.x) {
+    int o = t < r ? t : t + 1;
+    int32_t b = ah[o];
+    float w = mrd(ca, core[b]);
+    float eu = euclid_ref(xa, Xah + (int64_t)o * d, d);
+    if (w < eu) w = eu;
+    nlist[base + t] = b;
+    eweight[base + t] = w;
+  }
+}
+
+int bits_for(int64_t n) {
+  int b = 0;
+  while (b < 63 && (int64_t(1) << b) < n) b++;
+  return b < 1 ? 1 : b;
+}
+
+}  // namespace
+
+void core_distances(Context *ctx, const float *dist, const float *X, const int32_t *ids,
+                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core) {
+  int g = grid_for(ctx, n, 256);
+  if (mode == HDB_DIST_SQRT)
+    k_core_sqrt<<<g, 256, 0, ctx->stream>>>(X, ids, n, d, k, core);
+  else
+    k_core_from_dist<<<g, 256, 0, ctx->stream>>>(dist, n, k, core);
+  HDB_CHECK_LAUNCH();
+}
+
+void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, const float *X,
+                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times) {
+  HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "enhanced kNN graph: bad n");
+  HDB_REQUIRE(k >= 1 && k <= 32 && k < n, HDB_ERR_ARG, "enhanced kNN graph: k must be in [1, 32]");
+  HDB_REQUIRE(d >= 1, HDB_ERR_ARG, "enhanced kNN graph: bad d");
+  cudaStream_t st = ctx->stream;
+  const int gw = grid_for(ctx, n, kWarpsPerBlock);
+  const int ge = grid_for(ctx, n, 256);
+
+  // 1. in-degrees + validation
+  Buf<int32_t> deg(ctx, n);
+  HDB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(int32_t), st));
+  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err);
+  HDB_CHECK_LAUNCH();
+  uint32_t err = ctx->take_dev_err();
+  HDB_REQUIRE(!(err & DEVERR_ID_RANGE), HDB_ERR_ARG, "kNN graph: neighbour id outside [0, n)");
+  HDB_REQUIRE(!(err & DEVERR_SELF_ID), HDB_ERR_ARG, "kNN graph: a row lists its own id");
+  HDB_REQUIRE(!(err & DEVERR_DUP_ID), HDB_ERR_ARG, "kNN graph: an id repeats within a row");
+
+  // 2. antihubs: the P = (int)sqrt(n) lowest degrees (get_NumThreshold,
+  //    getters.cu:6-9); ties at the threshold by (score, index).
+  const int32_t P = (int32_t)sqrt((double)n);
+  Buf<uint32_t> hist(ctx, kDegHistBins);
+  Buf<int64_t> thr(ctx, 4);
+  HDB_CUDA(cudaMemsetAsync(hist, 0, kDegHistBins * sizeof(uint32_t), st));
+  k_degree_hist<<<ge, 256, 0, st>>>(deg, n, hist);
+  HDB_CHECK_LAUNCH();
+  k_find_threshold<<<1, 1024, 0, st>>>(hist, P, thr);
+  HDB_CHECK_LAUNCH();
+  int64_t *h = static_cast<int64_t *>(ctx->pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, thr, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  const int64_t T = h[0], below = h[1], at = h[2];
+  HDB_REQUIRE(T >= 0 && T < kDegHistBins - 1, HDB_ERR_INTERNAL,
+              "antihub threshold degree out of histogram range");
+  const int64_t missing = P - below;
+  Buf<int32_t> is_ah(ctx, n);
+  Buf<int64_t> pos(ctx, n + 1);
+  Buf<int32_t> flag(ctx, n);
+  k_flag_below<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, is_ah, at == missing ? 1 : 0);
+  HDB_CHECK_LAUNCH();
+  if (at > missing) {
+    k_flag_eq<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, flag);
+    HDB_CHECK_LAUNCH();
+    scan_exclusive_i32_i64(ctx, flag, pos, n, nullptr);
+    Buf<uint64_t> keys(ctx, at);
+    k_tie_keys<<<ge, 256, 0, st>>>(deg, flag, pos, ids, n, k, keys);
+    HDB_CHECK_LAUNCH();
+    radix_sort_u64(ctx, keys, nullptr, at, 0, 64);
+    k_mark_selected_ties<<<grid_for(ctx, missing, 256), 256, 0, st>>>(keys, missing, is_ah);
+    HDB_CHECK_LAUNCH();
+  }
+  ensure_capacity(ctx, (void **)&ctx->g_antihubs, &ctx->g_antihubs_cap,
+                  (size_t)(P > 0 ? P : 1) * sizeof(int32_t));
+  scan_exclusive_i32_i64(ctx, is_ah, pos, n, pos.get() + n);
+  k_compact_flags<<<ge, 256, 0, st>>>(is_ah, pos, n, ctx->g_antihubs);
+  HDB_CHECK_LAUNCH();
+  if (times) HDB_CUDA(cudaEventRecord(times->after_antihubs, st));
+
+  // 3. mutual flags and reverse counts
+  Buf<uint32_t> mutual(ctx, n);
+  Buf<int32_t> revcnt(ctx, n), nonmutual(ctx, n);
+  HDB_CUDA(cudaMemsetAsync(revcnt, 0, n * sizeof(int32_t), st));
+  k_mutual<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, mutual, revcnt, nonmutual);
+  HDB_CHECK_LAUNCH();
+
+  // 4. row sizes -> nindex
+  ensure_capacity(ctx, (void **)&ctx->g_nindex, &ctx->g_nindex_cap, (n + 1) * sizeof(int64_t));
+  {
+    Buf<int32_t> sizes(ctx, n);
+    k_row_sizes<<<ge, 256, 0, st>>>(revcnt, is_ah, n, k, P, sizes);
+    HDB_CHECK_LAUNCH();
+    scan_exclusive_i32_i64(ctx, sizes, ctx->g_nindex, n, ctx->g_nindex + n);
+  }
+  // 5. reverse entries (v, i) in i order, stable-sorted by v
+  Buf<int64_t> roff(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, nonmutual, roff, n, roff.get() + n);
+  int64_t hv[2];
+  HDB_CUDA(cudaMemcpyAsync(h, roff.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  HDB_CUDA(cudaMemcpyAsync(h + 1, ctx->g_nindex + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  hv[0] = h[0];
+  hv[1] = h[1];
+  const int64_t R = hv[0], E = hv[1];
+  HDB_REQUIRE(E < (int64_t(1) << 32), HDB_ERR_ARG,
+              "enhanced kNN graph has 2^32 or more edges (edge indices are 32-bit)");
+  Buf<uint32_t> rkeys(ctx, R), rvals(ctx, R);
+  k_emit_reverse<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, mutual, roff, n, k, rkeys, rvals);
+  HDB_CHECK_LAUNCH();
+  radix_sort_u32(ctx, rkeys, rvals, R, 0, bits_for(n));
+  Buf<int64_t> rev_off(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, revcnt, rev_off, n, nullptr);
+
+  // 6. fill rows + MRD weights
+  ensure_capacity(ctx, (void **)&ctx->g_nlist, &ctx->g_nlist_cap, (size_t)E * sizeof(int32_t));
+  ensure_capacity(ctx, (void **)&ctx->g_eweight, &ctx->g_eweight_cap, (size_t)E * sizeof(float));
+  k_fill<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, core, ctx->g_nindex, revcnt, rev_off, rvals, n,
+                                             k, ctx->g_nlist, ctx->g_eweight);
+  HDB_CHECK_LAUNCH();
+  if (P > 1) {
+    Buf<float> Xah(ctx, (size_t)P * d);
+    k_gather_rows<<<grid_for(ctx, (int64_t)P * d, 256), 256, 0, st>>>(X, ctx->g_antihubs, P, d,
+                                                                        Xah);
+    HDB_CHECK_LAUNCH();
+    k_clique<<<P, 256, d * sizeof(float), st>>>(ctx->g_antihubs, P, Xah, d, core, ctx->g_nindex,
+                                                revcnt, k, ctx->g_nlist, ctx->g_eweight);
+    HDB_CHECK_LAUNCH();
+  }
+  ctx->sync();
+  out->nodes = (int32_t)n;
+  out->edges = E;
+  out->nindex = ctx->g_nindex;
+  out->nlist = ctx->g_nlist;
+  out->eweight = ctx->g_eweight;
+  out->num_antihubs = P;
+  out->antihubs = ctx->g_antihubs;
+}
+
+}  // namespace hdb

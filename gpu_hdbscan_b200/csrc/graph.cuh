@@ -1,0 +1,20 @@
+// Enhanced kNN graph stage (graph.cu).
+#pragma once
+#include "hdb_internal.cuh"
+
+namespace hdb {
+
+struct GraphTimes {
+  cudaEvent_t after_antihubs;
+};
+
+// core[i]: distance to the k-th neighbour (calculateCoreDistance with index
+// k-1, HDBSCAN/graphs/graph.cu:77).  mode HDB_DIST_SQRT recomputes it with
+// fix_distances' sqrt-L2 rounding; HDB_DIST_SQUARED reads dist[i, k-1].
+void core_distances(Context *ctx, const float *dist, const float *X, const int32_t *ids,
+                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core);
+
+void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, const float *X,
+                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times);
+
+}  // namespace hdb

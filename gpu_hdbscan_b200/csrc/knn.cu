@@ -1,0 +1,510 @@
+// NN-Descent kNN graph (gpuknn::NNDescent, gpuknn/nndescent.cu:2088-2199).
+//
+// Same algorithm as the reference -- hash-seeded random init, per iteration a
+// sample of S new / S old neighbours plus reverse samples, a local join in
+// which every new neighbour is offered its closest other new neighbour and
+// its closest old neighbour and every old neighbour its closest new one --
+// laid out for one B200:
+//  * no per-row spin locks (InsertToGlobalGraph, nndescent.cu:969-1028): the
+//    join appends candidates to a fixed per-row inbox (one atomicAdd each,
+//    pre-filtered against the row's current k-th distance), and the next
+//    pass merges each row's inbox in one warp (sort, de-duplicate, merge);
+//  * the three sampling kernels, MarkAllToOld and the merge are one kernel
+//    (k_sample), so an iteration is two launches;
+//  * distances are the reference's sequential FP32 difference sum
+//    (nndescent.cu:1086-1093, fmaf per element), so every pair has one exact
+//    value wherever it is computed.
+#include "hdb_internal.cuh"
+#include "knn.cuh"
+
+namespace hdb {
+
+namespace {
+
+constexpr int kMaxK = 32;
+constexpr int kInboxCap = 127;  // + 1 overflow slot = 128 sorted candidates per merge
+constexpr int kMergeSlots = 128;
+
+__host__ __device__ __forceinline__ uint64_t xorshift64star(uint64_t x) {
+  // gpuknn/knncuda_tools.cu:126-132
+  x += 42;
+  x ^= x >> 12;
+  x ^= x << 25;
+  x ^= x >> 27;
+  return x * 0x2545F4914F6CDD1DULL;
+}
+
+__device__ __forceinline__ uint64_t pack(float d, int32_t id) {
+  return ((uint64_t)__float_as_uint(d) << 32) | (uint32_t)id;
+}
+__device__ __forceinline__ float pk_dist(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
+__device__ __forceinline__ int32_t pk_id(uint64_t k) { return (int32_t)(uint32_t)k; }
+
+__device__ __forceinline__ int32_t decode(int32_t label) { return label >= 0 ? label : -label - 1; }
+
+// Sequential FP32 difference sum (nndescent.cu:1086-1093).
+__device__ __forceinline__ float diffsum(const float *a, const float *b, int d) {
+  float s = 0.0f;
+  for (int j = 0; j < d; j++) {
+    float df = __fsub_rn(a[j], b[j]);
+    s = __fmaf_rn(df, df, s);
+  }
+  return s;
+}
+
+// Ascending bitonic sort of one u64 per lane across the warp.
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      uint64_t o = __shfl_xor_sync(0xffffffffu, v, stride);
+      bool up = ((lane & size) == 0);
+      bool lower = (lane & stride) == 0;
+      uint64_t mn = v < o ? v : o, mx = v < o ? o : v;
+      v = (lower == up) ? mn : mx;
+    }
+  }
+  return v;
+}
+
+// Ascending bitonic sort of kMergeSlots u64 in shared memory by one warp.
+__device__ __forceinline__ void warp_sort_smem128(uint64_t *s) {
+  const int lane = lane_id();
+  for (int size = 2; size <= kMergeSlots; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+      for (int q = 0; q < kMergeSlots / 64; q++) {
+        int t = lane + 32 * q;                       // pair index 0..63
+        int i = (t / stride) * (2 * stride) + (t % stride);
+        int j = i + stride;
+        bool up = (i & size) == 0;
+        uint64_t a = s[i], b = s[j];
+        if ((a > b) == up) { s[i] = b; s[j] = a; }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
+                       int32_t *__restrict__ gid, float *__restrict__ gdist,
+                       float *__restrict__ worst) {
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    // InitKNNGraphIndexKernel (nndescent.cu:1673-1692): xorshift64star(pos) % n,
+    // advanced past the row itself -- and here also past ids already taken.
+    int64_t label = (int64_t)(xorshift64star((uint64_t)(row * k + lane)) % (uint64_t)n);
+    for (int t = 0; t < k; t++) {
+      while (true) {
+        int64_t c = __shfl_sync(0xffffffffu, label, t);
+        bool dup = (lane < t) && (label == c);
+        if (c != row && __ballot_sync(0xffffffffu, dup) == 0) break;
+        if (lane == t) label = (label + 1) % n;
+      }
+    }
+    uint64_t key = ~0ull;
+    if (lane < k) key = pack(diffsum(X + row * d, X + label * d, d), (int32_t)label);
+    key = warp_sort32(key);
+    if (lane < k) {
+      gid[row * k + lane] = pk_id(key);  // all "new"
+      gdist[row * k + lane] = pk_dist(key);
+    }
+    float w = __shfl_sync(0xffffffffu, pk_dist(key), k - 1);
+    if (lane == 0) worst[row] = w;
+  }
+}
+
+// Per-warp shared memory of a merge: 128 sorted candidates, then the k output
+// keys and labels.
+constexpr int kMergeSmemU64 = kMergeSlots + kMaxK + kMaxK / 2;
+
+// Merge of a row's inbox into its sorted list (one warp).  On return, lane j
+// (< k) holds the j-th entry of the merged row: flagged label and distance.
+// Candidates of one pair always carry the same distance, so duplicates are
+// adjacent after the sort.
+__device__ __forceinline__ void merge_inbox(int64_t row, int k, int32_t &lab, float &dist,
+                                            int32_t *__restrict__ inbox_cnt,
+                                            const uint64_t *__restrict__ inbox,
+                                            unsigned long long *__restrict__ ovf, uint64_t *sk) {
+  const int lane = lane_id();
+  int cnt = inbox_cnt[row];
+  const uint64_t ov = ovf[row];
+  if (cnt == 0 && ov == ~0ull) return;
+  if (cnt > kInboxCap) cnt = kInboxCap;
+  __syncwarp();
+  if (lane == 0) {
+    inbox_cnt[row] = 0;
+    if (ov != ~0ull) ovf[row] = ~0ull;
+  }
+  for (int i = lane; i < kMergeSlots; i += 32)
+    sk[i] = i < cnt ? inbox[row * kInboxCap + i] : (i == kInboxCap ? ov : ~0ull);
+  __syncwarp();
+  warp_sort_smem128(sk);
+  const bool have = lane < k;
+  const uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
+  const int32_t rid = have ? decode(lab) : -1;
+  uint64_t c[kMergeSlots / 32];
+  bool ok[kMergeSlots / 32];
+#pragma unroll
+  for (int q = 0; q < kMergeSlots / 32; q++) {
+    int i = lane + 32 * q;
+    c[q] = sk[i];
+    uint64_t prev = i > 0 ? sk[i - 1] : ~0ull;
+    ok[q] = c[q] != ~0ull && c[q] != prev;
+  }
+  for (int t = 0; t < k; t++) {
+    int32_t r = __shfl_sync(0xffffffffu, rid, t);
+#pragma unroll
+    for (int q = 0; q < kMergeSlots / 32; q++)
+      if (pk_id(c[q]) == r) ok[q] = false;
+  }
+  __syncwarp();
+  int ns = 0;
+#pragma unroll
+  for (int q = 0; q < kMergeSlots / 32; q++) {
+    uint32_t bal = __ballot_sync(0xffffffffu, ok[q]);
+    if (ok[q]) sk[ns + __popc(bal & lanemask_lt())] = c[q];
+    ns += __popc(bal);
+  }
+  __syncwarp();
+  if (ns == 0) return;
+  uint64_t *out_key = sk + kMergeSlots;
+  int32_t *out_lab = reinterpret_cast<int32_t *>(out_key + kMaxK);
+  // row entry of this lane: rank = lane + #(survivors below it)
+  int lo = 0, hi = ns;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (sk[mid] < rkey) lo = mid + 1; else hi = mid;
+  }
+  if (have && lane + lo < k) {
+    out_key[lane + lo] = rkey;
+    out_lab[lane + lo] = lab;
+  }
+  // survivor i: rank = i + #(row entries below it)
+#pragma unroll
+  for (int q = 0; q < kMergeSlots / 32; q++) {
+    int i = lane + 32 * q;
+    uint64_t cc = i < ns ? sk[i] : ~0ull;
+    int below = 0;
+    for (int t = 0; t < k; t++) below += __shfl_sync(0xffffffffu, rkey, t) < cc;
+    if (i < ns && i + below < k) {
+      out_key[i + below] = cc;
+      out_lab[i + below] = pk_id(cc);  // inserted as "new"
+    }
+  }
+  __syncwarp();
+  if (have) {
+    lab = out_lab[lane];
+    dist = pk_dist(out_key[lane]);
+  }
+  __syncwarp();
+}
+
+// Merge (iterations >= 1), sample (PrepareGraph :44-98 and reverse samples
+// PrepareReverseGraph :293-346) and MarkAllToOld (:1398), one warp per row.
+__global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restrict__ gid,
+                         float *__restrict__ gdist, float *__restrict__ worst,
+                         int32_t *__restrict__ inbox_cnt, const uint64_t *__restrict__ inbox,
+                         unsigned long long *__restrict__ ovf, int32_t *__restrict__ newS,
+                         int32_t *__restrict__ oldS, int8_t *__restrict__ nf, int8_t *__restrict__ of,
+                         int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
+  extern __shared__ uint64_t smem_sample[];
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  uint64_t *sk = smem_sample + (threadIdx.x >> 5) * kMergeSmemU64;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const bool have = lane < k;
+    int32_t lab = have ? gid[row * k + lane] : 0;
+    float dist = have ? gdist[row * k + lane] : 0.0f;
+    if (do_merge) merge_inbox(row, k, lab, dist, inbox_cnt, inbox, ovf, sk);
+    const bool isnew = have && lab >= 0;
+    const bool isold = have && lab < 0;
+    const int32_t id = decode(lab);
+    uint32_t nm = __ballot_sync(0xffffffffu, isnew), om = __ballot_sync(0xffffffffu, isold);
+    int rn = __popc(nm & lanemask_lt()), ro = __popc(om & lanemask_lt());
+    const int64_t sb = row * (2 * S);
+    if (isnew && rn < S) {
+      newS[sb + rn] = id;
+      int p = atomicAdd(&nrev[id], 1);
+      if (p < S) newS[(int64_t)id * (2 * S) + S + p] = (int32_t)row;
+    }
+    if (isold && ro < S) {
+      oldS[sb + ro] = id;
+      int p = atomicAdd(&orev[id], 1);
+      if (p < S) oldS[(int64_t)id * (2 * S) + S + p] = (int32_t)row;
+    }
+    if (lane == 0) {
+      nf[row] = (int8_t)min(__popc(nm), S);
+      of[row] = (int8_t)min(__popc(om), S);
+    }
+    if (have) {
+      gid[row * k + lane] = isnew ? -id - 1 : lab;  // MarkAllToOld
+      gdist[row * k + lane] = dist;
+    }
+    float w = __shfl_sync(0xffffffffu, dist, k - 1);
+    if (lane == 0) worst[row] = w;
+  }
+}
+
+// Final merge after the last join; writes NNDElement rows with their flags.
+__global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
+                           const float *__restrict__ gdist, int32_t *__restrict__ inbox_cnt,
+                           const uint64_t *__restrict__ inbox, unsigned long long *__restrict__ ovf,
+                           hdb_nnd_element *__restrict__ out) {
+  extern __shared__ uint64_t smem_fin[];
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  uint64_t *sk = smem_fin + (threadIdx.x >> 5) * kMergeSmemU64;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const bool have = lane < k;
+    int32_t lab = have ? gid[row * k + lane] : 0;
+    float dist = have ? gdist[row * k + lane] : 0.0f;
+    merge_inbox(row, k, lab, dist, inbox_cnt, inbox, ovf, sk);
+    if (have) {
+      hdb_nnd_element e;
+      e.distance_ = dist;
+      e.label_ = lab;
+      out[row * k + lane] = e;
+    }
+  }
+}
+
+struct JoinSmem {
+  // layout per warp: ids[64] | Dnn[32*33] | Dno[32*33] | X rows [64 * dp]
+  static constexpr int kIds = 64;
+  static constexpr int kMat = 32 * 33;
+  __host__ __device__ static int floats(int dp) { return kIds + 2 * kMat + 64 * dp; }
+};
+
+__device__ __forceinline__ void push_candidate(int32_t target, int32_t id, float d,
+                                               const float *__restrict__ worst,
+                                               int32_t *__restrict__ inbox_cnt,
+                                               uint64_t *__restrict__ inbox,
+                                               unsigned long long *__restrict__ ovf,
+                                               unsigned long long *__restrict__ dropped) {
+  if (!(d < worst[target])) return;  // cannot enter the target's list
+  int slot = atomicAdd(&inbox_cnt[target], 1);
+  uint64_t key = pack(d, id);
+  if (slot < kInboxCap) {
+    inbox[(int64_t)target * kInboxCap + slot] = key;
+  } else {
+    atomicMin(&ovf[target], (unsigned long long)key);
+    atomicAdd(dropped, 1ull);
+  }
+}
+
+// Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).
+__global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
+                       const int32_t *__restrict__ newS, const int32_t *__restrict__ oldS,
+                       const int8_t *__restrict__ nf, const int8_t *__restrict__ of,
+                       int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
+                       const float *__restrict__ worst, int32_t *__restrict__ inbox_cnt,
+                       uint64_t *__restrict__ inbox, unsigned long long *__restrict__ ovf,
+                       unsigned long long *__restrict__ dropped) {
+  extern __shared__ float smem_join[];
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  const int dp = (d & 1) ? d : d + 1;
+  float *base = smem_join + (threadIdx.x >> 5) * JoinSmem::floats(dp);
+  int32_t *ids = reinterpret_cast<int32_t *>(base);
+  float *Dnn = base + JoinSmem::kIds;
+  float *Dno = Dnn + JoinSmem::kMat;
+  float *Xs = Dno + JoinSmem::kMat;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const int cnf = nf[row], cof = of[row];
+    const int cnr = min(nrev[row], S), cor = min(orev[row], S);
+    __syncwarp();
+    if (lane == 0) { nrev[row] = 0; orev[row] = 0; }
+    const int64_t sb = row * (2 * S);
+    // slot t < S: forward sample t; slot S + t: reverse sample t
+    bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
+    bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
+    int32_t nid = vn ? newS[sb + lane] : -1 - lane;
+    int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    // de-duplicate (ShrinkGraph RemoveDuplicates, :285-291)
+    uint32_t pn = __match_any_sync(0xffffffffu, nid);
+    vn = vn && (__ffs(pn) - 1 == lane);
+    uint32_t po = __match_any_sync(0xffffffffu, oid);
+    vo = vo && (__ffs(po) - 1 == lane);
+    // new \ old (:468-486)
+    for (int t = 0; t < 32; t++) {
+      int32_t o = __shfl_sync(0xffffffffu, oid, t);
+      bool ov = __shfl_sync(0xffffffffu, vo, t);
+      if (ov && o == nid) vn = false;
+    }
+    uint32_t bn = __ballot_sync(0xffffffffu, vn), bo = __ballot_sync(0xffffffffu, vo);
+    const int nn = __popc(bn), no = __popc(bo);
+    if (vn) ids[__popc(bn & lanemask_lt())] = nid;
+    if (vo) ids[nn + __popc(bo & lanemask_lt())] = oid;
+    __syncwarp();
+    const int T = nn + no;
+    if (nn == 0 || T < 2) continue;
+    for (int idx = lane; idx < T * d; idx += 32) {
+      int r = idx / d, c = idx - r * d;
+      Xs[r * dp + c] = __ldg(X + (int64_t)ids[r] * d + c);
+    }
+    __syncwarp();
+    // new x new (upper triangle) and new x old distances
+    const int p1 = nn * (nn - 1) / 2, p2 = nn * no;
+    for (int p = lane; p < p1 + p2; p += 32) {
+      int a, b;
+      if (p < p1) {
+        // p -> (a, b), a < b, row-major over the upper triangle
+        a = 0;
+        int rem = p;
+        while (rem >= nn - 1 - a) { rem -= nn - 1 - a; a++; }
+        b = a + 1 + rem;
+        float dd = diffsum(Xs + a * dp, Xs + b * dp, d);
+        Dnn[a * 33 + b] = dd;
+        Dnn[b * 33 + a] = dd;
+      } else {
+        int q = p - p1;
+        a = q / no;
+        b = q - a * no;
+        Dno[a * 33 + b] = diffsum(Xs + a * dp, Xs + (nn + b) * dp, d);
+      }
+    }
+    __syncwarp();
+    if (lane < nn) {
+      uint64_t best1 = ~0ull, best2 = ~0ull;
+      for (int b = 0; b < nn; b++)
+        if (b != lane) {
+          uint64_t c = pack(Dnn[lane * 33 + b], ids[b]);
+          best1 = c < best1 ? c : best1;
+        }
+      for (int b = 0; b < no; b++) {
+        uint64_t c = pack(Dno[lane * 33 + b], ids[nn + b]);
+        best2 = c < best2 ? c : best2;
+      }
+      const int32_t x = ids[lane];
+      if (best1 != ~0ull)
+        push_candidate(x, pk_id(best1), pk_dist(best1), worst, inbox_cnt, inbox, ovf, dropped);
+      if (best2 != ~0ull)
+        push_candidate(x, pk_id(best2), pk_dist(best2), worst, inbox_cnt, inbox, ovf, dropped);
+    }
+    if (lane < no) {
+      uint64_t best = ~0ull;
+      for (int a = 0; a < nn; a++) {
+        uint64_t c = pack(Dno[a * 33 + lane], ids[a]);
+        best = c < best ? c : best;
+      }
+      if (best != ~0ull)
+        push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, inbox_cnt, inbox, ovf,
+                       dropped);
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void k_split(const hdb_nnd_element *__restrict__ G, int64_t total, int32_t *__restrict__ ids,
+                        float *__restrict__ dist) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    hdb_nnd_element e = G[i];
+    if (ids) ids[i] = decode(e.label_);
+    if (dist) dist[i] = e.distance_;
+  }
+}
+
+__device__ __forceinline__ float euclid_ref(const float *__restrict__ a, const float *__restrict__ b,
+                                           int d) {
+  float soma = 0.0f;
+  for (int i = 0; i < d; i++) {
+    float diff = __fsub_rn(a[i], b[i]);
+    double sq = __dmul_rn((double)diff, (double)diff);
+    soma = __double2float_rn(__dadd_rn((double)soma, sq));
+  }
+  return __fsqrt_rn(soma);
+}
+
+__global__ void k_fix_distances(const float *__restrict__ X, int64_t n, int d,
+                                const int32_t *__restrict__ ids, int k, float *__restrict__ dist) {
+  const int64_t total = n * k;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row = i / k;
+    dist[i] = euclid_ref(X + row * d, X + (int64_t)ids[i] * d, d);
+  }
+}
+
+}  // namespace
+
+void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
+               hdb_nnd_element *G, int64_t *dropped_out) {
+  const int k = p.k, S = p.sample_num;
+  HDB_REQUIRE(k >= 1 && k <= kMaxK, HDB_ERR_ARG, "NN-Descent: k must be in [1, 32]");
+  HDB_REQUIRE(S >= 1 && 2 * S <= k, HDB_ERR_ARG,
+              "NN-Descent: SAMPLE_NUM must satisfy 1 <= SAMPLE_NUM and 2*SAMPLE_NUM <= k");
+  HDB_REQUIRE(n > k && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "NN-Descent: need k < n < 2^31");
+  HDB_REQUIRE(d >= 1 && d <= 4096, HDB_ERR_ARG, "NN-Descent: d must be in [1, 4096]");
+  HDB_REQUIRE(p.iterations >= 0, HDB_ERR_ARG, "NN-Descent: negative iteration count");
+  HDB_REQUIRE(p.precision == HDB_PREC_FP32, HDB_ERR_ARG,
+              "NN-Descent: only HDB_PREC_FP32 is available in this build");
+  cudaStream_t st = ctx->stream;
+  Buf<int32_t> gid(ctx, n * k);
+  Buf<float> gdist(ctx, n * k), worst(ctx, n);
+  Buf<int32_t> newS(ctx, n * 2 * S), oldS(ctx, n * 2 * S), nrev(ctx, n), orev(ctx, n),
+      inbox_cnt(ctx, n);
+  Buf<int8_t> nf(ctx, n), of(ctx, n);
+  Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
+  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 1);
+  HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
+  HDB_CUDA(cudaMemsetAsync(dropped, 0, 8, st));
+
+  const int wpb = 8;
+  const int grid_rows = grid_for(ctx, n, wpb, 16);
+  k_init<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, gid, gdist, worst);
+  HDB_CHECK_LAUNCH();
+  const size_t smem_sample = (size_t)wpb * kMergeSmemU64 * sizeof(uint64_t);
+  const int dp = (d & 1) ? d : d + 1;
+  const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
+  int jw = (int)((200 * 1024) / per_warp);
+  jw = jw < 1 ? 1 : (jw > 8 ? 8 : jw);
+  const size_t smem_join = per_warp * jw;
+  HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "NN-Descent: d too large for the join tile");
+  HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
+  const int grid_join = grid_for(ctx, n, jw, 64);
+  for (int it = 0; it < p.iterations; it++) {
+    k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst,
+                                                       inbox_cnt, inbox, ovf, newS, oldS, nf, of,
+                                                       nrev, orev);
+    HDB_CHECK_LAUNCH();
+    k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
+                                                  inbox_cnt, inbox, ovf, dropped);
+    HDB_CHECK_LAUNCH();
+  }
+  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, inbox_cnt, inbox, ovf, G);
+  HDB_CHECK_LAUNCH();
+  if (dropped_out) {
+    HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 8, cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    *dropped_out = *static_cast<int64_t *>(ctx->pinned);
+  } else {
+    ctx->sync();
+  }
+}
+
+void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,
+               float *dist) {
+  k_split<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(G, n * k, ids, dist);
+  HDB_CHECK_LAUNCH();
+}
+
+void fix_distances(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
+                   int32_t k, float *dist) {
+  k_fix_distances<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(X, n, d, ids, k, dist);
+  HDB_CHECK_LAUNCH();
+}
+
+}  // namespace hdb

@@ -1,0 +1,14 @@
+// kNN graph stage (knn.cu).
+#pragma once
+#include "hdb_internal.cuh"
+
+namespace hdb {
+
+void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
+               hdb_nnd_element *G, int64_t *dropped_out);
+void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,
+               float *dist);
+void fix_distances(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
+                   int32_t k, float *dist);
+
+}  // namespace hdb

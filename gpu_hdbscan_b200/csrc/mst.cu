@@ -1,0 +1,330 @@
+// Minimum spanning tree of the enhanced kNN graph and the MST edge sort.
+//
+// Reference: cpuMST (HDBSCAN/mst/mst.cu:34-78) runs Kruskal over the entries
+// (weight, CSR edge index, row, target) whose target exceeds their row, and
+// buildMST (mst.cu:291-336) + sort_edges (merge_sort/merge_sort.cu:226-279)
+// list the chosen edges stably sorted by weight -- i.e. in (weight, edge
+// index) order.  Under that strict total order the MST is unique, so a
+// Boruvka MST that compares packed 64-bit keys (order-preserving weight bits
+// << 32 | edge index) selects exactly Kruskal's edge set.  Each round:
+// atomicMin of the key at both component representatives, hooking of every
+// component to its chosen neighbour (a mutual pair keeps the smaller id as
+// root), pointer jumping, and compaction of the edges that still cross
+// components.  The chosen keys, radix-sorted, give the reference's sorted
+// MSTedge list directly.
+#include "hdb_internal.cuh"
+#include "mst.cuh"
+
+namespace hdb {
+
+namespace {
+
+constexpr int kWarps = 8;
+
+struct alignas(16) CEdge {
+  int32_t a, b;  // current component representatives of the endpoints
+  uint64_t key;  // float_key(weight) << 32 | CSR edge index
+};
+
+__device__ __forceinline__ uint32_t weight_key(float w) {
+  // -0.0 and +0.0 compare equal in the reference (std::sort / merge on <)
+  return float_key(w == 0.0f ? 0.0f : w);
+}
+
+__global__ void k_count_canon(const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
+                              int64_t n, int32_t *__restrict__ cnt, uint32_t *err) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  for (; row < n; row += (int64_t)gridDim.x * kWarps) {
+    int64_t b = nindex[row], e = nindex[row + 1];
+    int c = 0;
+    for (int64_t j = b + lane; j < e; j += 32) {
+      int32_t v = nlist[j];
+      if (v < 0 || v >= n) { atomicOr(err, DEVERR_ID_RANGE); continue; }
+      c += v > row;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[row] = c;
+  }
+}
+
+__global__ void k_emit_canon(const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
+                             const float *__restrict__ ew, const int64_t *__restrict__ off,
+                             int64_t n, CEdge *__restrict__ el) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  for (; row < n; row += (int64_t)gridDim.x * kWarps) {
+    int64_t b = nindex[row], e = nindex[row + 1];
+    int64_t p = off[row];
+    for (int64_t j0 = b; j0 < e; j0 += 32) {
+      int64_t j = j0 + lane;
+      bool take = j < e && nlist[j] > row;
+      uint32_t m = __ballot_sync(0xffffffffu, take);
+      if (take) {
+        CEdge c;
+        c.a = (int32_t)row;
+        c.b = nlist[j];
+        c.key = ((uint64_t)weight_key(ew[j]) << 32) | (uint64_t)(uint32_t)j;
+        el[p + __popc(m & lanemask_lt())] = c;
+      }
+      p += __popc(m);
+    }
+  }
+}
+
+__global__ void k_iota(int32_t *__restrict__ v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (int32_t)i;
+}
+
+__global__ void k_min_edge(const CEdge *__restrict__ el, int64_t m,
+                           unsigned long long *__restrict__ minkey) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    CEdge c = el[i];
+    unsigned long long k = c.key;
+    if (k < minkey[c.a]) atomicMin(&minkey[c.a], k);
+    if (k < minkey[c.b]) atomicMin(&minkey[c.b], k);
+  }
+}
+
+__global__ void k_winner(const CEdge *__restrict__ el, int64_t m,
+                         const unsigned long long *__restrict__ minkey, int32_t *__restrict__ other) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    CEdge c = el[i];
+    if (minkey[c.a] == c.key) other[c.a] = c.b;
+    if (minkey[c.b] == c.key) other[c.b] = c.a;
+  }
+}
+
+// Hook every representative to the component across its minimum edge.
+__global__ void k_hook(const int32_t *__restrict__ reps, int64_t nr,
+                       unsigned long long *__restrict__ minkey, const int32_t *__restrict__ other,
+                       int32_t *__restrict__ parent, uint64_t *__restrict__ mst_keys,
+                       unsigned long long *__restrict__ mst_count, int64_t cap) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nr;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int32_t v = reps[t];
+    unsigned long long mk = minkey[v];
+    if (mk == ~0ull) continue;
+    int32_t o = other[v];
+    bool mutual = other[o] == v;
+    parent[v] = (mutual && v < o) ? v : o;
+    if (!(mutual && v > o)) {
+      unsigned long long idx = atomicAdd(mst_count, 1ull);
+      if ((int64_t)idx < cap) mst_keys[idx] = mk;
+    }
+  }
+}
+
+__global__ void k_reset_minkey(const int32_t *__restrict__ reps, int64_t nr,
+                               unsigned long long *__restrict__ minkey) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nr;
+       t += (int64_t)gridDim.x * blockDim.x)
+    minkey[reps[t]] = ~0ull;
+}
+
+// Pointer jumping to the roots (concurrent halving: every write moves a
+// pointer up its own tree, so each thread's walk ends at its root).
+__global__ void k_jump(const int32_t *__restrict__ reps, int64_t nr, int32_t *parent,
+                       uint32_t *err) {
+  volatile int32_t *vp = parent;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nr;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int32_t v = reps[t];
+    int32_t p = vp[v];
+    int64_t steps = 0;
+    while (true) {
+      int32_t gp = vp[p];
+      if (gp == p) break;
+      vp[v] = gp;
+      p = gp;
+      if (++steps > nr) {  // a forest path is shorter than the node count
+        atomicOr(err, DEVERR_TIMEOUT);
+        break;
+      }
+    }
+  }
+}
+
+// Relabel both endpoints to their new roots and keep the edges that still
+// join two components (warp-aggregated append; order does not matter).
+__global__ void k_relabel_filter(const CEdge *__restrict__ el, int64_t m,
+                                 const int32_t *__restrict__ parent, CEdge *__restrict__ out,
+                                 unsigned long long *__restrict__ out_count) {
+  const int lane = lane_id();
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < m; i0 += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = i0 + threadIdx.x;
+    CEdge c;
+    bool keep = false;
+    if (i < m) {
+      c = el[i];
+      c.a = parent[c.a];
+      c.b = parent[c.b];
+      keep = c.a != c.b;
+    }
+    uint32_t bal = __ballot_sync(0xffffffffu, keep);
+    unsigned long long base = 0;
+    if (lane == 0 && bal) base = atomicAdd(out_count, (unsigned long long)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (keep) out[base + __popc(bal & lanemask_lt())] = c;
+  }
+}
+
+__global__ void k_roots(const int32_t *__restrict__ reps, int64_t nr,
+                        const int32_t *__restrict__ parent, int32_t *__restrict__ out,
+                        unsigned long long *__restrict__ count) {
+  const int lane = lane_id();
+  for (int64_t t0 = (int64_t)blockIdx.x * blockDim.x; t0 < nr; t0 += (int64_t)gridDim.x * blockDim.x) {
+    int64_t t = t0 + threadIdx.x;
+    int32_t v = 0;
+    bool keep = false;
+    if (t < nr) {
+      v = reps[t];
+      keep = parent[v] == v;
+    }
+    uint32_t bal = __ballot_sync(0xffffffffu, keep);
+    unsigned long long base = 0;
+    if (lane == 0 && bal) base = atomicAdd(count, (unsigned long long)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (keep) out[base + __popc(bal & lanemask_lt())] = v;
+  }
+}
+
+__device__ __forceinline__ int32_t row_of(const int64_t *__restrict__ nindex, int64_t n, int64_t j) {
+  int64_t lo = 0, hi = n - 1;  // largest r with nindex[r] <= j
+  while (lo < hi) {
+    int64_t mid = (lo + hi + 1) >> 1;
+    if (nindex[mid] <= j) lo = mid; else hi = mid - 1;
+  }
+  return (int32_t)lo;
+}
+
+__global__ void k_gather_mst(const uint64_t *__restrict__ keys, int64_t m,
+                             const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
+                             const float *__restrict__ ew, int64_t n, hdb_mst_edge *__restrict__ out,
+                             uint8_t *__restrict__ in_mst) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = (uint32_t)keys[t];
+    hdb_mst_edge e;
+    e.from_node = row_of(nindex, n, j);
+    e.to_node = nlist[j];
+    e.weight = ew[j];
+    out[t] = e;
+    if (in_mst) in_mst[j] = 1;
+  }
+}
+
+__global__ void k_edge_keys(const hdb_mst_edge *__restrict__ e, int64_t m, uint32_t *__restrict__ keys,
+                            uint32_t *__restrict__ vals) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    keys[t] = weight_key(e[t].weight);
+    vals[t] = (uint32_t)t;
+  }
+}
+
+__global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint32_t *__restrict__ idx,
+                                int64_t m, hdb_mst_edge *__restrict__ out) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = in[idx[t]];
+}
+
+}  // namespace
+
+void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
+                 int32_t *rounds_out) {
+  const int64_t n = g->nodes;
+  HDB_REQUIRE(n >= 2, HDB_ERR_ARG, "MST: need at least 2 nodes");
+  HDB_REQUIRE(g->edges < (int64_t(1) << 32), HDB_ERR_ARG, "MST: 2^32 or more edges");
+  cudaStream_t st = ctx->stream;
+  const int gw = grid_for(ctx, n, kWarps);
+  Buf<int32_t> cnt(ctx, n);
+  Buf<int64_t> off(ctx, n + 1);
+  k_count_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, n, cnt, ctx->dev_err);
+  HDB_CHECK_LAUNCH();
+  HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
+              "MST: graph has a neighbour id outside [0, nodes)");
+  scan_exclusive_i32_i64(ctx, cnt, off, n, off.get() + n);
+  int64_t *h = static_cast<int64_t *>(ctx->pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, off.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  int64_t m = h[0];
+  Buf<CEdge> el(ctx, m > 0 ? m : 1), el2(ctx, m > 0 ? m : 1);
+  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, el);
+  HDB_CHECK_LAUNCH();
+
+  Buf<unsigned long long> minkey(ctx, n);
+  Buf<int32_t> other(ctx, n), parent(ctx, n), reps(ctx, n), reps2(ctx, n);
+  Buf<uint64_t> keys(ctx, n);
+  Buf<unsigned long long> counters(ctx, 4);  // [0] mst edges, [1] live edges, [2] reps
+  HDB_CUDA(cudaMemsetAsync(minkey, 0xff, n * sizeof(unsigned long long), st));
+  HDB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+  const int gn = grid_for(ctx, n, 256);
+  k_iota<<<gn, 256, 0, st>>>(parent, n);
+  k_iota<<<gn, 256, 0, st>>>(reps, n);
+  HDB_CHECK_LAUNCH();
+  int64_t nr = n;
+  int rounds = 0;
+  int32_t *rp = reps, *rp2 = reps2;
+  CEdge *ep = el, *ep2 = el2;
+  while (m > 0) {
+    HDB_REQUIRE(rounds < 64, HDB_ERR_INTERNAL, "MST: Boruvka did not converge");
+    rounds++;
+    const int ge = grid_for(ctx, m, 256);
+    const int gr = grid_for(ctx, nr, 256);
+    k_min_edge<<<ge, 256, 0, st>>>(ep, m, minkey);
+    k_winner<<<ge, 256, 0, st>>>(ep, m, minkey, other);
+    k_hook<<<gr, 256, 0, st>>>(rp, nr, minkey, other, parent, keys, counters, n - 1);
+    k_reset_minkey<<<gr, 256, 0, st>>>(rp, nr, minkey);
+    k_jump<<<gr, 256, 0, st>>>(rp, nr, parent, ctx->dev_err);
+    HDB_CUDA(cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(unsigned long long), st));
+    k_relabel_filter<<<ge, 256, 0, st>>>(ep, m, parent, ep2, counters.get() + 1);
+    k_roots<<<gr, 256, 0, st>>>(rp, nr, parent, rp2, counters.get() + 2);
+    HDB_CHECK_LAUNCH();
+    HDB_CUDA(cudaMemcpyAsync(h, counters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    m = h[1];
+    nr = h[2];
+    HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_TIMEOUT), HDB_ERR_INTERNAL,
+                "MST: pointer jumping exceeded its bound");
+    std::swap(ep, ep2);
+    std::swap(rp, rp2);
+  }
+  const int64_t chosen = h[0];
+  if (rounds == 0) {
+    HDB_CUDA(cudaMemcpyAsync(h, counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+  }
+  HDB_REQUIRE((rounds == 0 ? h[0] : chosen) == n - 1, HDB_ERR_DISCONNECTED,
+              "MST does not have n-1 edges: the enhanced kNN graph is disconnected");
+  radix_sort_u64(ctx, keys, nullptr, n - 1, 0, 64);
+  if (in_mst) HDB_CUDA(cudaMemsetAsync(in_mst, 0, g->edges, st));
+  k_gather_mst<<<grid_for(ctx, n - 1, 256), 256, 0, st>>>(keys, n - 1, g->nindex, g->nlist,
+                                                          g->eweight, n, mst, in_mst);
+  HDB_CHECK_LAUNCH();
+  ctx->sync();
+  if (rounds_out) *rounds_out = rounds;
+}
+
+void sort_mst_edges(Context *ctx, hdb_mst_edge *edges, int64_t m) {
+  if (m <= 1) return;
+  cudaStream_t st = ctx->stream;
+  Buf<uint32_t> keys(ctx, m), idx(ctx, m);
+  Buf<hdb_mst_edge> tmp(ctx, m);
+  const int g = grid_for(ctx, m, 256);
+  k_edge_keys<<<g, 256, 0, st>>>(edges, m, keys, idx);
+  HDB_CHECK_LAUNCH();
+  radix_sort_u32(ctx, keys, idx, m, 0, 32);
+  HDB_CUDA(cudaMemcpyAsync(tmp, edges, m * sizeof(hdb_mst_edge), cudaMemcpyDeviceToDevice, st));
+  k_permute_edges<<<g, 256, 0, st>>>(tmp, idx, m, edges);
+  HDB_CHECK_LAUNCH();
+  ctx->sync();
+}
+
+}  // namespace hdb

@@ -1,0 +1,11 @@
+// MST stage (mst.cu).
+#pragma once
+#include "hdb_internal.cuh"
+
+namespace hdb {
+
+void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
+                 int32_t *rounds_out);
+void sort_mst_edges(Context *ctx, hdb_mst_edge *edges, int64_t m);
+
+}  // namespace hdb

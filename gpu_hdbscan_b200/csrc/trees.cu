@@ -1,0 +1,838 @@
+// Single-linkage tree, condensed tree, stability, excess-of-mass selection
+// and labels -- all on the device.
+//
+// Reference: build_Linkage_tree, build_Condensed_tree, compute_stability,
+// get_clusters and do_labelling (HDBSCAN/trees/tree.cu:171-746), which run as
+// serial host loops (union-find replay, BFS, per-cluster scans).
+//
+// Linkage tree.  Node N+r merges the two components joined by sorted MST edge
+// r; its children are the components' current roots, i.e. the largest edge
+// rank inside each endpoint's component among edges < r (or the vertex itself).
+// Edge ranks are processed as a binary divide and conquer: at every level each
+// block of ranks [s, s+S) unions its lower half with a lock-free union-find,
+// tags each component with its largest rank, and relabels the endpoints of its
+// upper half by those tags.  Endpoint labels seen by different blocks of one
+// level are disjoint, so all blocks share one union-find array.  After log2(N)
+// levels every edge's endpoint labels are exactly its two children.
+//
+// Condensed tree.  A node is visited by the reference's BFS iff it is the root
+// or holds >= mpts points.  Chains of "one big child" nodes share a cluster; a
+// node whose children are both big starts two clusters, numbered in BFS order
+// (depth, then left-to-right = preorder).  Depth, preorder and chain heads come
+// from pointer jumping; each point falls out at the lowest visited ancestor.
+// Stability is summed per cluster in the reference's row order (chain nodes
+// top-down, identical terms for the points of each small side), in FP32 with
+// separate multiply/add roundings, or in FP64 when asked.
+#include "hdb_internal.cuh"
+#include "trees.cuh"
+
+namespace hdb {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Linkage tree
+// ---------------------------------------------------------------------------
+// Union-find over labels [0, 2n-1); hooks always point to a smaller label, so
+// every path ends at a root.  The step bounds only guard against corrupted
+// state and report through the device error word.
+constexpr int64_t kUfBound = int64_t(1) << 31;
+
+__device__ __forceinline__ int32_t uf_find(volatile int32_t *p, int32_t x) {
+  for (int64_t s = 0; s < kUfBound; s++) {
+    int32_t px = p[x];
+    if (px == x) return x;
+    int32_t ppx = p[px];
+    if (ppx != px) p[x] = ppx;
+    x = px;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_union(int32_t *p, int32_t a, int32_t b, uint32_t *err) {
+  volatile int32_t *vp = p;
+  for (int64_t s = 0; s < kUfBound; s++) {
+    a = uf_find(vp, a);
+    b = uf_find(vp, b);
+    if (a == b) return;
+    if (a > b) { int32_t t = a; a = b; b = t; }
+    if (atomicCAS(&p[b], b, a) == b) return;
+  }
+  atomicOr(err, DEVERR_TIMEOUT);
+}
+
+// Lower-half edge of a block that has an upper half at block size S.
+__device__ __forceinline__ bool active_lower(int64_t r, int64_t S, int64_t m) {
+  int64_t pos = r & (S - 1);
+  int64_t half = S >> 1;
+  return pos < half && (r - pos) + half < m;
+}
+
+__global__ void k_link_init(const hdb_mst_edge *__restrict__ mst, int64_t m,
+                            int32_t *__restrict__ la, int32_t *__restrict__ lb) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    la[r] = mst[r].from_node;
+    lb[r] = mst[r].to_node;
+  }
+}
+
+__global__ void k_uf_init(int64_t total, int64_t n, int32_t *__restrict__ ufp,
+                          int32_t *__restrict__ maxr, int32_t *__restrict__ seen,
+                          int32_t *__restrict__ acc, int32_t *__restrict__ size) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    ufp[i] = (int32_t)i;
+    maxr[i] = -1;
+    seen[i] = 0;
+    acc[i] = 0;
+    size[i] = i < n ? 1 : 0;
+  }
+}
+
+__global__ void k_level_union(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
+                              int64_t m, int64_t S, int32_t *ufp, uint32_t *err) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x)
+    if (active_lower(r, S, m)) uf_union(ufp, la[r], lb[r], err);
+}
+
+// MST input check: endpoints in [0, n).
+__global__ void k_validate_mst(const hdb_mst_edge *__restrict__ mst, int64_t m, int64_t n,
+                               uint32_t *err) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    hdb_mst_edge e = mst[r];
+    if (e.from_node < 0 || e.from_node >= n || e.to_node < 0 || e.to_node >= n)
+      atomicOr(err, DEVERR_ID_RANGE);
+  }
+}
+
+__global__ void k_level_tag(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
+                            int64_t m, int64_t S, int64_t n, int32_t *ufp, int32_t *maxr,
+                            int32_t *seen, int32_t *acc, const int32_t *__restrict__ size) {
+  volatile int32_t *vp = ufp;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!active_lower(r, S, m)) continue;
+    int32_t a = la[r], b = lb[r];
+    int32_t root = uf_find(vp, a);
+    atomicMax(&maxr[root], (int32_t)r);
+    if (atomicExch(&seen[a], 1) == 0) atomicAdd(&acc[root], a < n ? 1 : size[a]);
+    if (atomicExch(&seen[b], 1) == 0) atomicAdd(&acc[root], b < n ? 1 : size[b]);
+  }
+}
+
+__global__ void k_level_produce(const int32_t *__restrict__ la, int64_t m, int64_t S, int64_t n,
+                                int32_t *ufp, const int32_t *__restrict__ maxr,
+                                const int32_t *__restrict__ acc, int32_t *__restrict__ size) {
+  volatile int32_t *vp = ufp;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!active_lower(r, S, m)) continue;
+    int32_t root = uf_find(vp, la[r]);
+    if (maxr[root] == (int32_t)r) size[n + r] = acc[root];
+  }
+}
+
+__global__ void k_level_relabel(int32_t *__restrict__ la, int32_t *__restrict__ lb, int64_t m,
+                                int64_t S, int64_t n, int32_t *ufp,
+                                const int32_t *__restrict__ maxr) {
+  volatile int32_t *vp = ufp;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if ((r & (S - 1)) < (S >> 1)) continue;
+    int32_t a = la[r], b = lb[r];
+    int32_t ra = uf_find(vp, a), rb = uf_find(vp, b);
+    int32_t ma = maxr[ra], mb = maxr[rb];
+    if (ma >= 0) la[r] = (int32_t)(n + ma);
+    if (mb >= 0) lb[r] = (int32_t)(n + mb);
+  }
+}
+
+__global__ void k_level_reset(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
+                              int64_t m, int64_t S, int32_t *__restrict__ ufp,
+                              int32_t *__restrict__ maxr, int32_t *__restrict__ seen,
+                              int32_t *__restrict__ acc) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!active_lower(r, S, m)) continue;
+    int32_t a = la[r], b = lb[r];
+    ufp[a] = a; maxr[a] = -1; seen[a] = 0; acc[a] = 0;
+    ufp[b] = b; maxr[b] = -1; seen[b] = 0; acc[b] = 0;
+  }
+}
+
+__global__ void k_link_out(const hdb_mst_edge *__restrict__ mst, const int32_t *__restrict__ la,
+                           const int32_t *__restrict__ lb, const int32_t *__restrict__ size,
+                           int64_t m, int64_t n, hdb_linkage_node *__restrict__ out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t a = la[r], b = lb[r];
+    hdb_linkage_node o;
+    o.left_node = a;
+    o.right_node = b;
+    o.weight = mst[r].weight;
+    o.node_size = (a < n ? 1 : size[a]) + (b < n ? 1 : size[b]);
+    out[r] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Condensed tree, stability, EOM, labels
+// ---------------------------------------------------------------------------
+enum : int8_t { KIND_SPLIT = 0, KIND_BOTHSMALL = 1, KIND_LEFTBIG = 2, KIND_RIGHTBIG = 3 };
+
+struct TreeView {
+  const hdb_linkage_node *h;
+  int64_t n;  // points
+  int32_t mpts;
+  __device__ __forceinline__ int32_t sz(int64_t x) const {
+    return x < n ? 1 : h[x - n].node_size;
+  }
+};
+
+__device__ __forceinline__ float lambda_of(float w) {
+  // tree.cu:308-313: INFINITE = INT_MAX, else 1.0 / weight in double
+  return w > 0.0f ? __double2float_rn(__drcp_rn((double)w)) : 2147483648.0f;
+}
+
+// Hierarchy input check: children are earlier nodes and sizes add up, so
+// parent pointers always go to larger ids (every upward walk ends at the root).
+__global__ void k_validate_hier(TreeView t, uint32_t *err) {
+  const int64_t m = t.n - 1;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    hdb_linkage_node h = t.h[r];
+    int64_t lim = t.n + r;
+    bool ok = h.left_node >= 0 && h.left_node < lim && h.right_node >= 0 &&
+              h.right_node < lim && h.left_node != h.right_node;
+    if (ok) ok = (int64_t)t.sz(h.left_node) + t.sz(h.right_node) == h.node_size;
+    if (!ok) atomicOr(err, DEVERR_ID_RANGE);
+  }
+}
+
+// Per internal node: parent pointers, side, kind, visited flag, lambda.
+__global__ void k_nodes(TreeView t, int32_t *__restrict__ par, int8_t *__restrict__ side,
+                        int8_t *__restrict__ kind, int8_t *__restrict__ visited,
+                        float *__restrict__ lam) {
+  const int64_t m = t.n - 1;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    hdb_linkage_node h = t.h[r];
+    int64_t x = t.n + r;
+    par[h.left_node] = (int32_t)x;
+    par[h.right_node] = (int32_t)x;
+    side[h.left_node] = 0;
+    side[h.right_node] = 1;
+    bool lb = t.sz(h.left_node) >= t.mpts, rb = t.sz(h.right_node) >= t.mpts;
+    kind[r] = (lb && rb) ? KIND_SPLIT : (!lb && !rb) ? KIND_BOTHSMALL : lb ? KIND_LEFTBIG : KIND_RIGHTBIG;
+    visited[r] = (r == m - 1) || h.node_size >= t.mpts;
+    lam[r] = lambda_of(h.weight);
+  }
+}
+
+// Doubling state for visited nodes: jump pointer, depth and preorder sums,
+// and the chain-head pointer.
+__global__ void k_path_init(TreeView t, const int32_t *__restrict__ par, const int8_t *__restrict__ side,
+                            const int8_t *__restrict__ kind, const int8_t *__restrict__ visited,
+                            int32_t *__restrict__ jmp, int64_t *__restrict__ dep,
+                            int64_t *__restrict__ pre, int32_t *__restrict__ head) {
+  const int64_t m = t.n - 1;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!visited[r]) { jmp[r] = -1; head[r] = -1; continue; }
+    int64_t x = t.n + r;
+    if (r == m - 1) {  // root
+      jmp[r] = -1; dep[r] = 0; pre[r] = 0; head[r] = (int32_t)r;
+      continue;
+    }
+    int32_t p = par[x];
+    int64_t pr = p - t.n;
+    jmp[r] = (int32_t)pr;
+    dep[r] = 1;
+    int64_t d = 1;
+    if (side[x] == 1) {
+      int32_t sib = t.h[pr].left_node;
+      d += 2 * (int64_t)t.sz(sib) - 1;
+    }
+    pre[r] = d;
+    int8_t pk = kind[pr];
+    bool inherit = (pk == KIND_LEFTBIG && side[x] == 0) || (pk == KIND_RIGHTBIG && side[x] == 1);
+    head[r] = inherit ? (int32_t)pr : (int32_t)r;
+  }
+}
+
+__global__ void k_path_jump(int64_t m, const int32_t *__restrict__ jmp, const int64_t *__restrict__ dep,
+                            const int64_t *__restrict__ pre, int32_t *__restrict__ jmp2,
+                            int64_t *__restrict__ dep2, int64_t *__restrict__ pre2,
+                            int32_t *changed) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = jmp[r];
+    if (j < 0) { jmp2[r] = j; dep2[r] = dep[r]; pre2[r] = pre[r]; continue; }
+    dep2[r] = dep[r] + dep[j];
+    pre2[r] = pre[r] + pre[j];
+    jmp2[r] = jmp[j];
+    *changed = 1;
+  }
+}
+
+__global__ void k_head_jump(int64_t m, int32_t *head, int32_t *changed) {
+  volatile int32_t *vh = head;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t h = vh[r];
+    if (h < 0) continue;
+    int32_t hh = vh[h];
+    if (hh != h) {
+      vh[r] = hh;
+      *changed = 1;
+    }
+  }
+}
+
+__global__ void k_split_keys(int64_t m, const int8_t *__restrict__ kind,
+                             const int8_t *__restrict__ visited, const int64_t *__restrict__ dep,
+                             const int64_t *__restrict__ pre, int32_t *__restrict__ flag) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x)
+    flag[r] = visited[r] && kind[r] == KIND_SPLIT;
+}
+
+__global__ void k_split_emit(int64_t m, const int32_t *__restrict__ flag, const int64_t *__restrict__ pos,
+                             const int64_t *__restrict__ dep, const int64_t *__restrict__ pre,
+                             uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[r]) continue;
+    keys[pos[r]] = ((uint64_t)dep[r] << 32) | (uint64_t)pre[r];
+    vals[pos[r]] = (uint32_t)r;
+  }
+}
+
+// Cluster ids: root = n; the t-th split node in BFS order gives n+1+2t (left)
+// and n+2+2t (right).  cid is indexed by internal-node rank r (-1 otherwise).
+__global__ void k_assign_cids(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
+                              int32_t *__restrict__ cid, int32_t *__restrict__ split_rank) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ns;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = split_nodes[q];
+    hdb_linkage_node h = t.h[r];
+    cid[h.left_node - t.n] = (int32_t)(t.n + 1 + 2 * q);
+    cid[h.right_node - t.n] = (int32_t)(t.n + 2 + 2 * q);
+    split_rank[r] = (int32_t)q;
+  }
+}
+
+// Cluster of every visited node; per-cluster info (index c - n).
+__global__ void k_node_cluster(int64_t m, int64_t n, const int8_t *__restrict__ visited,
+                               const int32_t *__restrict__ head, const int32_t *__restrict__ cid,
+                               int32_t *__restrict__ ncl) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x)
+    ncl[r] = visited[r] ? cid[head[r]] : -1;
+}
+
+__global__ void k_cluster_info(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
+                               const int32_t *__restrict__ ncl, const float *__restrict__ lam,
+                               float *__restrict__ birth, int32_t *__restrict__ cparent,
+                               int32_t *__restrict__ ckid0) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ns;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = split_nodes[q];
+    int32_t pc = ncl[r];  // cluster whose chain ends at this split
+    int32_t c0 = (int32_t)(1 + 2 * q), c1 = (int32_t)(2 + 2 * q);
+    birth[c0] = lam[r];
+    birth[c1] = lam[r];
+    cparent[c0] = pc - (int32_t)t.n;
+    cparent[c1] = pc - (int32_t)t.n;
+    ckid0[pc - t.n] = c0;
+  }
+}
+
+// Chain nodes grouped by cluster, top-down: key (cluster index << 32) | depth.
+__global__ void k_chain_keys(int64_t m, int64_t n, const int32_t *__restrict__ ncl,
+                             const int64_t *__restrict__ dep, const int64_t *__restrict__ pos,
+                             uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (ncl[r] < 0) continue;
+    keys[pos[r]] = ((uint64_t)(ncl[r] - n) << 32) | (uint64_t)dep[r];
+    vals[pos[r]] = (uint32_t)r;
+  }
+}
+
+// One thread per cluster: stability in the reference's row order.
+__global__ void k_stability(TreeView t, int64_t C, const int64_t *__restrict__ seg_start,
+                            const int64_t *__restrict__ seg_end, const uint32_t *__restrict__ chain,
+                            const int8_t *__restrict__ kind, const float *__restrict__ lam,
+                            const float *__restrict__ birth, float *__restrict__ stab,
+                            double *__restrict__ stab64) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const float b = birth[c];
+    float s = 0.0f;
+    double s64 = 0.0;
+    for (int64_t i = seg_start[c]; i < seg_end[c]; i++) {
+      const uint32_t r = chain[i];
+      const hdb_linkage_node h = t.h[r];
+      const float v = __fsub_rn(lam[r], b);
+      const double v64 = __dsub_rn((double)lam[r], (double)b);
+      const int8_t kd = kind[r];
+      if (kd == KIND_SPLIT) {
+        int32_t sl = t.sz(h.left_node), sr = t.sz(h.right_node);
+        s = __fadd_rn(s, __fmul_rn(v, (float)sl));
+        s = __fadd_rn(s, __fmul_rn(v, (float)sr));
+        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)sl));
+        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)sr));
+      } else {
+        int64_t cnt = kd == KIND_LEFTBIG ? t.sz(h.right_node)
+                      : kd == KIND_RIGHTBIG ? t.sz(h.left_node)
+                                            : (int64_t)t.sz(h.left_node) + t.sz(h.right_node);
+        for (int64_t q = 0; q < cnt; q++) {  // one row per point, in row order
+          s = __fadd_rn(s, v);
+          s64 = __dadd_rn(s64, v64);
+        }
+      }
+    }
+    stab[c] = s;
+    stab64[c] = s64;
+  }
+}
+
+// Excess of mass, bottom-up: the last of two siblings to finish continues
+// with their parent (get_clusters, tree.cu:692-725).  Index 0 is the root,
+// which the reference never evaluates.
+__global__ void k_eom(int64_t C, const int32_t *__restrict__ ckid0, const int32_t *__restrict__ cparent,
+                      const float *__restrict__ stab, const double *__restrict__ stab64, int fp64,
+                      float *sub, double *sub64, int8_t *self_sel, int32_t *arrive) {
+  for (int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < C;
+       c0 += (int64_t)gridDim.x * blockDim.x) {
+    if (c0 == 0 || ckid0[c0] >= 0) continue;  // start from leaf clusters
+    int64_t c = c0;
+    // leaf: no children -> subtree stability 0, never above its own
+    volatile float *vsub = sub;
+    volatile double *vsub64 = sub64;
+    vsub[c] = stab[c];
+    vsub64[c] = stab64[c];
+    self_sel[c] = 1;
+    for (int64_t guard = 0; guard < C; guard++) {
+      int64_t p = cparent[c];
+      if (p <= 0) break;  // parent is the root
+      __threadfence();
+      if (atomicAdd(&arrive[p], 1) == 0) break;  // sibling not done yet
+      __threadfence();
+      int32_t k0 = ckid0[p];
+      bool over;
+      if (fp64) {
+        double ssum = vsub64[k0] + vsub64[k0 + 1];
+        over = ssum > stab64[p];
+        vsub64[p] = over ? ssum : stab64[p];
+        vsub[p] = over ? (float)ssum : stab[p];
+      } else {
+        float ssum = __fadd_rn(__fadd_rn(0.0f, vsub[k0]), vsub[k0 + 1]);
+        over = ssum > stab[p];
+        vsub[p] = over ? ssum : stab[p];
+        vsub64[p] = vsub[p];
+      }
+      self_sel[p] = over ? 0 : 1;
+      c = p;
+    }
+  }
+}
+
+// Nearest self-selected proper ancestor (root excluded) by doubling.
+__global__ void k_sel_init(int64_t C, const int32_t *__restrict__ cparent, const int8_t *__restrict__ self_sel,
+                           int32_t *__restrict__ jmp, int8_t *__restrict__ anc) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t p = c == 0 ? -1 : cparent[c];
+    if (p <= 0) { jmp[c] = -1; anc[c] = 0; }
+    else { jmp[c] = p; anc[c] = self_sel[p]; }
+  }
+}
+
+__global__ void k_sel_jump(int64_t C, const int32_t *__restrict__ jmp, const int8_t *__restrict__ anc,
+                           int32_t *__restrict__ jmp2, int8_t *__restrict__ anc2, int32_t *changed) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = jmp[c];
+    if (j < 0) { jmp2[c] = -1; anc2[c] = anc[c]; continue; }
+    anc2[c] = anc[c] | anc[j];
+    jmp2[c] = jmp[j];
+    *changed = 1;
+  }
+}
+
+__global__ void k_selected(int64_t C, const int8_t *__restrict__ self_sel, const int8_t *__restrict__ anc,
+                           int32_t *__restrict__ sel) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x)
+    sel[c] = (c > 0 && self_sel[c] && !anc[c]) ? 1 : 0;
+}
+
+// Selected cluster covering each cluster (itself or nearest selected ancestor).
+__global__ void k_cover_init(int64_t C, const int32_t *__restrict__ cparent, const int32_t *__restrict__ sel,
+                             int32_t *__restrict__ jmp, int32_t *__restrict__ cover) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (sel[c]) { cover[c] = (int32_t)c; jmp[c] = -1; continue; }
+    cover[c] = -1;
+    int32_t p = c == 0 ? -1 : cparent[c];
+    jmp[c] = p > 0 ? p : -1;
+  }
+}
+
+__global__ void k_cover_jump(int64_t C, const int32_t *__restrict__ jmp, const int32_t *__restrict__ cover,
+                             int32_t *__restrict__ jmp2, int32_t *__restrict__ cover2, int32_t *changed) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = jmp[c];
+    if (cover[c] >= 0 || j < 0) { cover2[c] = cover[c]; jmp2[c] = -1; continue; }
+    cover2[c] = cover[j];
+    jmp2[c] = cover[j] >= 0 ? -1 : jmp[j];
+    *changed = 1;
+  }
+}
+
+// Points: fall-out node = parent of the highest ancestor holding < mpts points.
+__global__ void k_points(TreeView t, const int32_t *__restrict__ par, const int32_t *__restrict__ ncl,
+                         const float *__restrict__ lam, const int32_t *__restrict__ cover,
+                         const float *__restrict__ birth, const int32_t *__restrict__ label_of,
+                         int32_t *__restrict__ labels, int32_t *__restrict__ pcl,
+                         float *__restrict__ plam) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < t.n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = p;
+    while (true) {
+      int32_t up = par[a];
+      if (up < 0 || t.sz(up) >= t.mpts) break;
+      a = up;
+    }
+    int64_t f = par[a] < 0 ? a : par[a];  // a is the root only if n < mpts
+    int64_t fr = f - t.n;
+    int32_t c = ncl[fr];
+    float lp = lam[fr];
+    int32_t s = cover[c - t.n];
+    int32_t lab = -1;
+    if (s >= 0 && lp > birth[s]) lab = label_of[s];
+    labels[p] = lab;
+    if (pcl) { pcl[p] = c; plam[p] = lp; }
+  }
+}
+
+__global__ void k_label_map(int64_t C, const int32_t *__restrict__ sel, const int32_t *__restrict__ pos,
+                            int32_t *__restrict__ label_of) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x)
+    label_of[c] = sel[c] ? pos[c] : -1;
+}
+
+__global__ void k_condensed_rows(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
+                                 const int32_t *__restrict__ ncl, const float *__restrict__ lam,
+                                 const int32_t *__restrict__ pcl, const float *__restrict__ plam,
+                                 hdb_condensed_node *__restrict__ rows, uint64_t *__restrict__ keys,
+                                 uint32_t *__restrict__ vals) {
+  const int64_t total = t.n + 2 * ns;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    hdb_condensed_node row;
+    if (i < t.n) {
+      row.parent = pcl[i];
+      row.child = (int32_t)i;
+      row.lambda_val = plam[i];
+      row.child_size = 1;
+    } else {
+      int64_t q = (i - t.n) >> 1;
+      int side = (int)((i - t.n) & 1);
+      int64_t r = split_nodes[q];
+      hdb_linkage_node h = t.h[r];
+      row.parent = ncl[r];
+      row.child = (int32_t)(t.n + 1 + 2 * q + side);
+      row.lambda_val = lam[r];
+      row.child_size = t.sz(side ? h.right_node : h.left_node);
+    }
+    rows[i] = row;
+    keys[i] = ((uint64_t)(uint32_t)row.parent << 32) | (uint32_t)row.child;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+__global__ void k_permute_rows(const hdb_condensed_node *__restrict__ in, const uint32_t *__restrict__ idx,
+                               int64_t cnt, hdb_condensed_node *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[idx[i]];
+}
+
+__global__ void k_stab_out(int64_t C, int64_t n, const float *__restrict__ stab,
+                           hdb_stability *__restrict__ out) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    hdb_stability s;
+    s.cluster_id = (int32_t)(n + c);
+    s.lambda = stab[c];
+    out[c] = s;
+  }
+}
+
+__global__ void k_seg_bounds(const uint64_t *__restrict__ keys, int64_t cnt, int64_t *__restrict__ s0,
+                             int64_t *__restrict__ s1) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t c = (uint32_t)(keys[i] >> 32);
+    if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != c) s0[c] = i;
+    if (i == cnt - 1 || (uint32_t)(keys[i + 1] >> 32) != c) s1[c] = i + 1;
+  }
+}
+
+__global__ void k_flag_nonneg(const int32_t *__restrict__ v, int64_t m, int32_t *__restrict__ flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = v[i] >= 0;
+}
+
+int bits_for(int64_t v) {
+  int b = 0;
+  while (b < 63 && (int64_t(1) << b) <= v) b++;
+  return b < 1 ? 1 : b;
+}
+
+}  // namespace
+
+void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_node *out) {
+  HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 30), HDB_ERR_ARG, "linkage tree: bad n");
+  cudaStream_t st = ctx->stream;
+  const int64_t m = n - 1, total = 2 * n - 1;
+  Buf<int32_t> la(ctx, m), lb(ctx, m), ufp(ctx, total), maxr(ctx, total), seen(ctx, total),
+      acc(ctx, total), size(ctx, total);
+  const int gm = grid_for(ctx, m, 256), gt = grid_for(ctx, total, 256);
+  k_validate_mst<<<gm, 256, 0, st>>>(mst, m, n, ctx->dev_err);
+  HDB_CHECK_LAUNCH();
+  HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
+              "linkage tree: MST edge endpoint outside [0, n)");
+  k_link_init<<<gm, 256, 0, st>>>(mst, m, la, lb);
+  k_uf_init<<<gt, 256, 0, st>>>(total, n, ufp, maxr, seen, acc, size);
+  HDB_CHECK_LAUNCH();
+  int64_t S = 1;
+  while (S < m) S <<= 1;
+  for (; S >= 2; S >>= 1) {
+    k_level_union<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, ctx->dev_err);
+    k_level_tag<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr, seen, acc, size);
+    k_level_produce<<<gm, 256, 0, st>>>(la, m, S, n, ufp, maxr, acc, size);
+    k_level_relabel<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr);
+    k_level_reset<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, maxr, seen, acc);
+    HDB_CHECK_LAUNCH();
+  }
+  k_link_out<<<gm, 256, 0, st>>>(mst, la, lb, size, m, n, out);
+  HDB_CHECK_LAUNCH();
+  HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_TIMEOUT), HDB_ERR_INTERNAL,
+              "linkage tree: union-find exceeded its step bound");
+}
+
+void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t mpts,
+                     int32_t stab_mode, int32_t *labels, int32_t *num_clusters,
+                     hdb_condensed_node *condensed, int64_t *condensed_size,
+                     hdb_stability *stability, int64_t *num_stability) {
+  HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 30), HDB_ERR_ARG, "condensed tree: bad n");
+  HDB_REQUIRE(mpts >= 2, HDB_ERR_ARG, "condensed tree: mpts (min cluster size) must be >= 2");
+  cudaStream_t st = ctx->stream;
+  const int64_t m = n - 1, total = 2 * n - 1;
+  TreeView t{h, n, mpts};
+  const int gm = grid_for(ctx, m, 256), gn = grid_for(ctx, n, 256);
+  int64_t *hp = static_cast<int64_t *>(ctx->pinned);
+  int32_t *hflag = reinterpret_cast<int32_t *>(hp + 8);
+
+  Buf<int32_t> par(ctx, total);
+  Buf<int8_t> side(ctx, total), kind(ctx, m), visited(ctx, m);
+  Buf<float> lam(ctx, m);
+  HDB_CUDA(cudaMemsetAsync(par, 0xff, total * sizeof(int32_t), st));
+  k_validate_hier<<<gm, 256, 0, st>>>(t, ctx->dev_err);
+  HDB_CHECK_LAUNCH();
+  HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
+              "condensed tree: hierarchy is not a valid single-linkage tree");
+  k_nodes<<<gm, 256, 0, st>>>(t, par, side, kind, visited, lam);
+  HDB_CHECK_LAUNCH();
+
+  // depth / preorder / chain heads by pointer jumping
+  Buf<int32_t> jmp(ctx, m), jmp2(ctx, m), head(ctx, m);
+  Buf<int64_t> dep(ctx, m), dep2(ctx, m), pre(ctx, m), pre2(ctx, m);
+  Buf<int32_t> changed(ctx, 2);
+  k_path_init<<<gm, 256, 0, st>>>(t, par, side, kind, visited, jmp, dep, pre, head);
+  HDB_CHECK_LAUNCH();
+  int32_t *j0 = jmp, *j1 = jmp2;
+  int64_t *d0 = dep, *d1 = dep2, *p0 = pre, *p1 = pre2;
+  for (int it = 0; it < 64; it++) {
+    HDB_CUDA(cudaMemsetAsync(changed, 0, 2 * sizeof(int32_t), st));
+    k_path_jump<<<gm, 256, 0, st>>>(m, j0, d0, p0, j1, d1, p1, changed);
+    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed.get() + 1);
+    HDB_CHECK_LAUNCH();
+    HDB_CUDA(cudaMemcpyAsync(hflag, changed, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    std::swap(j0, j1);
+    std::swap(d0, d1);
+    std::swap(p0, p1);
+    if (!hflag[0] && !hflag[1]) break;
+    HDB_REQUIRE(it < 63, HDB_ERR_INTERNAL, "condensed tree: pointer jumping did not converge");
+  }
+  // head pointers may need extra rounds beyond the path sums
+  for (int it = 0; it < 64; it++) {
+    HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
+    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed);
+    HDB_CHECK_LAUNCH();
+    HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    if (!hflag[0]) break;
+  }
+
+  // split nodes in BFS order -> cluster ids
+  Buf<int32_t> flag(ctx, m);
+  Buf<int64_t> pos(ctx, m + 1);
+  k_split_keys<<<gm, 256, 0, st>>>(m, kind, visited, d0, p0, flag);
+  HDB_CHECK_LAUNCH();
+  scan_exclusive_i32_i64(ctx, flag, pos, m, pos.get() + m);
+  HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  const int64_t ns = hp[0];
+  const int64_t C = 1 + 2 * ns;
+  Buf<uint64_t> skeys(ctx, ns > 0 ? ns : 1);
+  Buf<uint32_t> snodes(ctx, ns > 0 ? ns : 1);
+  Buf<int32_t> cid(ctx, m), split_rank(ctx, m);
+  HDB_CUDA(cudaMemsetAsync(cid, 0xff, m * sizeof(int32_t), st));
+  if (ns > 0) {
+    k_split_emit<<<gm, 256, 0, st>>>(m, flag, pos, d0, p0, skeys, snodes);
+    HDB_CHECK_LAUNCH();
+    radix_sort_u64(ctx, skeys, snodes, ns, 0, 64);
+    k_assign_cids<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, cid, split_rank);
+    HDB_CHECK_LAUNCH();
+  }
+  // root cluster id
+  {
+    int32_t root_cid = (int32_t)n;
+    HDB_CUDA(cudaMemcpyAsync(cid.get() + (m - 1), &root_cid, sizeof(int32_t),
+                             cudaMemcpyHostToDevice, st));
+    ctx->sync();
+  }
+  Buf<int32_t> ncl(ctx, m);
+  k_node_cluster<<<gm, 256, 0, st>>>(m, n, visited, head, cid, ncl);
+  HDB_CHECK_LAUNCH();
+
+  // per-cluster info
+  Buf<float> birth(ctx, C), stab(ctx, C), sub(ctx, C);
+  Buf<double> stab64(ctx, C), sub64(ctx, C);
+  Buf<int32_t> cparent(ctx, C), ckid0(ctx, C), arrive(ctx, C);
+  Buf<int8_t> self_sel(ctx, C);
+  HDB_CUDA(cudaMemsetAsync(birth, 0, C * sizeof(float), st));
+  HDB_CUDA(cudaMemsetAsync(cparent, 0xff, C * sizeof(int32_t), st));
+  HDB_CUDA(cudaMemsetAsync(ckid0, 0xff, C * sizeof(int32_t), st));
+  HDB_CUDA(cudaMemsetAsync(arrive, 0, C * sizeof(int32_t), st));
+  HDB_CUDA(cudaMemsetAsync(self_sel, 0, C, st));
+  if (ns > 0) {
+    k_cluster_info<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, ncl, lam, birth,
+                                                            cparent, ckid0);
+    HDB_CHECK_LAUNCH();
+  }
+
+  // chain segments (cluster, depth), then stability per cluster
+  Buf<int64_t> s0(ctx, C), s1(ctx, C);
+  HDB_CUDA(cudaMemsetAsync(s0, 0, C * sizeof(int64_t), st));
+  HDB_CUDA(cudaMemsetAsync(s1, 0, C * sizeof(int64_t), st));
+  Buf<uint32_t> chain(ctx, m);
+  {
+    k_flag_nonneg<<<gm, 256, 0, st>>>(ncl, m, flag);
+    HDB_CHECK_LAUNCH();
+    scan_exclusive_i32_i64(ctx, flag, pos, m, pos.get() + m);
+    HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    const int64_t nv = hp[0];
+    Buf<uint64_t> ckeys(ctx, nv);
+    k_chain_keys<<<gm, 256, 0, st>>>(m, n, ncl, d0, pos, ckeys, chain);
+    HDB_CHECK_LAUNCH();
+    radix_sort_u64(ctx, ckeys, chain, nv, 0, 32 + bits_for(C));
+    k_seg_bounds<<<grid_for(ctx, nv, 256), 256, 0, st>>>(ckeys, nv, s0, s1);
+    HDB_CHECK_LAUNCH();
+  }
+  const int gc = grid_for(ctx, C, 128);
+  k_stability<<<gc, 128, 0, st>>>(t, C, s0, s1, chain, kind, lam, birth, stab, stab64);
+  HDB_CHECK_LAUNCH();
+
+  // excess of mass
+  const int fp64 = stab_mode == HDB_STAB_FP64;
+  k_eom<<<gc, 128, 0, st>>>(C, ckid0, cparent, stab, stab64, fp64, sub, sub64, self_sel, arrive);
+  HDB_CHECK_LAUNCH();
+  Buf<int32_t> cj(ctx, C), cj2(ctx, C), sel(ctx, C), cover(ctx, C), cover2(ctx, C);
+  Buf<int8_t> anc(ctx, C), anc2(ctx, C);
+  k_sel_init<<<gc, 128, 0, st>>>(C, cparent, self_sel, cj, anc);
+  HDB_CHECK_LAUNCH();
+  {
+    int32_t *ja = cj, *jb = cj2;
+    int8_t *aa = anc, *ab = anc2;
+    for (int it = 0; it < 64; it++) {
+      HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
+      k_sel_jump<<<gc, 128, 0, st>>>(C, ja, aa, jb, ab, changed);
+      HDB_CHECK_LAUNCH();
+      HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      ctx->sync();
+      std::swap(ja, jb);
+      std::swap(aa, ab);
+      if (!hflag[0]) break;
+    }
+    k_selected<<<gc, 128, 0, st>>>(C, self_sel, aa, sel);
+    HDB_CHECK_LAUNCH();
+  }
+  Buf<int32_t> selpos(ctx, C + 1), label_of(ctx, C);
+  scan_exclusive_i32_i32(ctx, sel, selpos, C, selpos.get() + C);
+  k_label_map<<<gc, 128, 0, st>>>(C, sel, selpos, label_of);
+  k_cover_init<<<gc, 128, 0, st>>>(C, cparent, sel, cj, cover);
+  HDB_CHECK_LAUNCH();
+  int32_t *cov_final = cover;
+  {
+    int32_t *ja = cj, *jb = cj2, *ca = cover, *cb = cover2;
+    for (int it = 0; it < 64; it++) {
+      HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
+      k_cover_jump<<<gc, 128, 0, st>>>(C, ja, ca, jb, cb, changed);
+      HDB_CHECK_LAUNCH();
+      HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      ctx->sync();
+      std::swap(ja, jb);
+      std::swap(ca, cb);
+      if (!hflag[0]) break;
+    }
+    cov_final = ca;
+  }
+
+  // labels (and the per-point condensed rows when asked)
+  Buf<int32_t> pcl;
+  Buf<float> plam;
+  if (condensed) {
+    pcl = Buf<int32_t>(ctx, n);
+    plam = Buf<float>(ctx, n);
+  }
+  k_points<<<gn, 256, 0, st>>>(t, par, ncl, lam, cov_final, birth, label_of, labels,
+                               condensed ? pcl.get() : nullptr, condensed ? plam.get() : nullptr);
+  HDB_CHECK_LAUNCH();
+  HDB_CUDA(cudaMemcpyAsync(hflag, selpos.get() + C, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  if (condensed) {
+    const int64_t rows = n + 2 * ns;
+    Buf<hdb_condensed_node> tmp(ctx, rows);
+    Buf<uint64_t> rkeys(ctx, rows);
+    Buf<uint32_t> ridx(ctx, rows);
+    k_condensed_rows<<<grid_for(ctx, rows, 256), 256, 0, st>>>(t, snodes, ns, ncl, lam, pcl, plam,
+                                                                tmp, rkeys, ridx);
+    HDB_CHECK_LAUNCH();
+    radix_sort_u64(ctx, rkeys, ridx, rows, 0, 64);
+    k_permute_rows<<<grid_for(ctx, rows, 256), 256, 0, st>>>(tmp, ridx, rows, condensed);
+    HDB_CHECK_LAUNCH();
+    if (condensed_size) *condensed_size = rows;
+  }
+  if (stability) {
+    k_stab_out<<<gc, 128, 0, st>>>(C, n, stab, stability);
+    HDB_CHECK_LAUNCH();
+  }
+  if (num_stability) *num_stability = C;
+  ctx->sync();
+  if (num_clusters) *num_clusters = hflag[0];
+}
+
+}  // namespace hdb

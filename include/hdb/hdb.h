@@ -1,0 +1,177 @@
+/*
+ * hdb.h -- C ABI of the B200-native HDBSCAN path (libhdb_b200.so).
+ *
+ * The reference (gorlando04/GPU_HDBSCAN) has no library API: its operator
+ * surface is a set of C++ functions called in the order of HDBSCAN/_new.cu
+ * (kNN graph -> enhanced kNN graph -> MST -> edge sort -> linkage tree ->
+ * condensed tree -> stability -> clusters), plus the compile-time parameters
+ * VEC_DIM, NEIGHB_NUM_PER_LIST (k), SAMPLE_NUM and NND_ITERATION.  Every entry
+ * point below replaces one of those functions; the comment above each one
+ * names the reference interface (file:line) it stands in for.  Record layouts
+ * are byte-identical to the reference structs so buffers can be exchanged.
+ *
+ * Conventions
+ *  - Every call returns an hdb_status; on failure hdb_last_error() (thread
+ *    local) holds a one-line message.  Nothing exits the process.
+ *  - Array arguments are DEVICE pointers (cudaMalloc'd, on the context's
+ *    device) unless the argument's comment says otherwise.  hdb_run also takes
+ *    host pointers when hdb_params.host_io is 1.
+ *  - Work is enqueued on the context's stream; every call returns after the
+ *    stream has finished the call's work.
+ *  - A context is single-stream and not thread safe; separate contexts are
+ *    independent.  Scratch memory comes from a per-context pool that grows on
+ *    demand and is released by hdb_destroy.
+ */
+#ifndef HDB_HDB_H
+#define HDB_HDB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HDB_API __attribute__((visibility("default")))
+
+typedef enum {
+  HDB_OK = 0,
+  HDB_ERR_ARG = 1,          /* invalid argument or input (the reference exit(1)s / asserts) */
+  HDB_ERR_ALLOC = 2,        /* device or host allocation failed */
+  HDB_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  HDB_ERR_IO = 4,           /* file read/write failed */
+  HDB_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  HDB_ERR_DISCONNECTED = 6, /* the MST does not have n-1 edges ("MST montada incorretamente") */
+  HDB_ERR_INTERNAL = 7
+} hdb_status;
+
+/* NNDElement, tools/nndescent_element.cuh:9-57: label_ < 0 encodes an "old"
+ * neighbour as -label-1; label() decodes it.  8 bytes. */
+typedef struct { float distance_; int32_t label_; } hdb_nnd_element;
+/* MSTedge, HDBSCAN/structs/hdbscan_elements.cuh:40-45.  12 bytes. */
+typedef struct { int32_t from_node, to_node; float weight; } hdb_mst_edge;
+/* SingleLinkageNode, hdbscan_elements.cuh:50-56.  16 bytes. */
+typedef struct { int32_t left_node, right_node; float weight; int32_t node_size; } hdb_linkage_node;
+/* CondensedTreeNode, hdbscan_elements.cuh:59-65.  16 bytes. */
+typedef struct { int32_t parent, child; float lambda_val; int32_t child_size; } hdb_condensed_node;
+/* Stability, hdbscan_elements.cuh:80-84.  8 bytes. */
+typedef struct { int32_t cluster_id; float lambda; } hdb_stability;
+
+/* ECLgraph, HDBSCAN/structs/ECLgraph.h:41-47, plus the antihub list.  The
+ * arrays are device memory owned by the context; they stay valid until the
+ * next hdb_enhanced_knng call on the same context or hdb_destroy. */
+typedef struct {
+  int32_t nodes;
+  int64_t edges;
+  int64_t *nindex;   /* [nodes + 1] */
+  int32_t *nlist;    /* [edges] */
+  float *eweight;    /* [edges] mutual-reachability weights */
+  int32_t num_antihubs;
+  int32_t *antihubs; /* [num_antihubs], ascending */
+} hdb_graph;
+
+enum { HDB_PREC_FP32 = 0, HDB_PREC_BF16 = 1 };
+enum { HDB_DIST_SQRT = 0, HDB_DIST_SQUARED = 1 };
+enum { HDB_STAB_FP32 = 0, HDB_STAB_FP64 = 1 };
+
+/* The compile-time parameters of gpuknn/nndescent.cuh:9-15 as run-time ones. */
+typedef struct {
+  int32_t k;           /* NEIGHB_NUM_PER_LIST, 1..32 (reference: 32) */
+  int32_t sample_num;  /* SAMPLE_NUM, 1..k/2 (reference: 16; 2*SAMPLE_NUM <= k) */
+  int32_t iterations;  /* NND_ITERATION (reference: 6) */
+  int32_t precision;   /* HDB_PREC_FP32: reference difference-sum distances;
+                          HDB_PREC_BF16: tensor-core candidate distances, FP32 re-rank */
+} hdb_knn_params;
+
+typedef struct {
+  hdb_knn_params knn;
+  int32_t mpts;        /* min cluster size (mpts, HDBSCAN/_new.cu:163); k >= mpts >= 2 */
+  int32_t distance;    /* HDB_DIST_SQRT: fix_distances applied (build_kNNG.cu:131-174);
+                          HDB_DIST_SQUARED: NN-Descent's squared distances kept */
+  int32_t stability;   /* HDB_STAB_FP32 (tree.cu:494-511 order) or HDB_STAB_FP64 */
+  int32_t host_io;     /* hdb_run only: 1 = X and labels are host pointers */
+} hdb_params;
+
+typedef struct {
+  int64_t edges;          /* enhanced kNN graph edges (CSR entries) */
+  int32_t num_antihubs;
+  int32_t num_clusters;
+  int64_t condensed_size;
+  int32_t mst_rounds;     /* Boruvka rounds */
+  int64_t knn_dropped;    /* NN-Descent candidates lost to a full inbox (normally 0) */
+  float ms_knn, ms_graph, ms_mst, ms_tree, ms_total; /* device time per stage */
+} hdb_run_stats;
+
+typedef struct hdb_ctx hdb_ctx;
+
+HDB_API const char *hdb_version(void);
+HDB_API const char *hdb_last_error(void);
+/* Creates a context on `device` with its own non-blocking stream. */
+HDB_API hdb_status hdb_create(hdb_ctx **ctx, int32_t device);
+HDB_API hdb_status hdb_destroy(hdb_ctx *ctx);
+/* Run the context's work on a caller stream (cudaStream_t); NULL restores the
+ * context's own stream. */
+HDB_API hdb_status hdb_set_stream(hdb_ctx *ctx, void *stream);
+
+/* gpuknn::NNDescent, gpuknn/nndescent.cuh:40-42 (nndescent.cu:2088-2199):
+ * X [n, d] float32 row-major -> G [n, k] NNDElement rows sorted by ascending
+ * squared L2, old/new flag sign-encoded as in the reference. */
+HDB_API hdb_status hdb_nndescent(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
+                                 const hdb_knn_params *params, hdb_nnd_element *G);
+
+/* The NNDElement -> (int ids, float distances) split of HDBSCAN/_new.cu:204-229. */
+HDB_API hdb_status hdb_knn_split(hdb_ctx *ctx, const hdb_nnd_element *G, int64_t n, int32_t k,
+                                 int32_t *ids, float *dist);
+
+/* fix_distances, build_kNNG.cu:131-174 (calculate_euclidean_distance_fix :4-13):
+ * dist[i, j] = sqrt-L2(X[i], X[ids[i, j]]) with the reference's rounding. */
+HDB_API hdb_status hdb_fix_distances(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
+                                     const int32_t *ids, int32_t k, float *dist);
+
+/* buildEnhancedKNNG, HDBSCAN/graphs/graph.cuh:24 (graph.cu:108-176 and
+ * buildECLgraph graph.cu:16-103): in-degrees, floor(sqrt(n)) antihubs, the
+ * symmetric CSR with the antihub clique, core distances (distance to the k-th
+ * neighbour) and mutual-reachability weights.  ids must be in [0, n), without
+ * self ids or repeated ids in a row (HDB_ERR_ARG otherwise). */
+HDB_API hdb_status hdb_enhanced_knng(hdb_ctx *ctx, const int32_t *ids, const float *dist,
+                                     const float *X, int64_t n, int32_t d, int32_t k,
+                                     hdb_graph *graph);
+
+/* cpuMST + buildMST, HDBSCAN/mst/mst.cuh:64,91 (mst.cu:34-78, 291-336): the
+ * minimum spanning tree under the order (weight, CSR edge index) of the
+ * entries whose target exceeds their row, written as MSTedge[n-1] already
+ * sorted the way sort_edges leaves it.  in_mst [edges] (optional, may be NULL)
+ * receives the reference's bool-per-edge result.  HDB_ERR_DISCONNECTED if the
+ * graph is not connected. */
+HDB_API hdb_status hdb_mst(hdb_ctx *ctx, const hdb_graph *graph, uint8_t *in_mst,
+                           hdb_mst_edge *mst, int32_t *rounds);
+
+/* sort_edges, HDBSCAN/merge_sort/merge_sort.cuh:30: stable ascending sort by
+ * weight, in place. */
+HDB_API hdb_status hdb_sort_edges(hdb_ctx *ctx, hdb_mst_edge *edges, int64_t m);
+
+/* build_Linkage_tree, HDBSCAN/trees/tree.cuh:33 (tree.cu:171-202): the
+ * single-linkage tree of n points from n-1 sorted MST edges. */
+HDB_API hdb_status hdb_linkage_tree(hdb_ctx *ctx, const hdb_mst_edge *sorted, int64_t n,
+                                    hdb_linkage_node *hierarchy);
+
+/* build_Condensed_tree + compute_stability + get_clusters, tree.cuh:39-45
+ * (tree.cu:255-746): labels [n] (-1 = noise, clusters 0.. in ascending
+ * cluster id).  Optional outputs (NULL to skip): condensed [n + 2*(n/mpts) + 2]
+ * rows sorted by (parent, child) with *condensed_size set; stability
+ * [n/mpts*2 + 2] indexed by cluster id - n with *num_stability set. */
+HDB_API hdb_status hdb_condense_select(hdb_ctx *ctx, const hdb_linkage_node *hierarchy,
+                                       int64_t n, int32_t mpts, int32_t stability_mode,
+                                       int32_t *labels, int32_t *num_clusters,
+                                       hdb_condensed_node *condensed, int64_t *condensed_size,
+                                       hdb_stability *stability, int64_t *num_stability);
+
+/* The whole path in the HDBSCAN/_new.cu:149-358 order (hdbscan_ binary):
+ * X [n, d] -> labels [n].  With params->host_io = 1 both are host pointers and
+ * the copies run inside the call. */
+HDB_API hdb_status hdb_run(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
+                           const hdb_params *params, int32_t *labels, hdb_run_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HDB_HDB_H */

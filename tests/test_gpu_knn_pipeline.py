@@ -1,0 +1,132 @@
+"""NN-Descent quality and the end-to-end pipeline on the GPU."""
+import numpy as np
+import pytest
+
+from conftest import blobs
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x):
+    return x.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize("n,d,k", [(5000, 12, 32), (4000, 32, 16), (3000, 3, 8)])
+def test_nndescent_graph_is_valid_and_exact(ctx, oracle, n, d, k):
+    X = blobs(n, d, seed=n + d)
+    G = ctx.NNDescent(X, k=k, sample_num=k // 2, iterations=6)
+    ids, dist = (_t(a) for a in ctx.knn_split(G))
+    assert oracle.validate_knn(ids)
+    # rows sorted by (distance, id) and every distance is the reference's
+    # FP32 difference sum of the pair, bit for bit
+    key = dist.view(np.uint32).astype(np.uint64) << np.uint64(32) | ids.astype(np.uint64)
+    assert (np.diff(key, axis=1) > 0).all()
+    rng = np.random.default_rng(0)
+    for i in rng.choice(n, 200, replace=False):
+        for j in range(k):
+            ref = oracle.diffsum(X[i], X[ids[i, j]])
+            assert np.float32(ref).view(np.uint32) == dist[i, j].view(np.uint32)
+
+
+@pytest.mark.parametrize("n,d,k", [(20000, 12, 32), (8000, 64, 32)])
+def test_nndescent_recall_matches_reference_algorithm(ctx, oracle, n, d, k):
+    """Recall@k against the FP64 exact kNN within 0.5 pt of the oracle's
+    restatement of the reference NN-Descent (same S, iterations)."""
+    X = blobs(n, d, seed=7 + d, blobs=20)
+    G = ctx.NNDescent(X, k=k, sample_num=16, iterations=6)
+    ids, _ = ctx.knn_split(G)
+    ids = _t(ids)
+    q = np.arange(0, n, 7)
+    gt, _ = oracle.bruteforce_knn(X, k, q)
+    r_gpu = oracle.recall(ids[q], gt, k)
+    oids, _ = oracle.nndescent(X, k, 16, 6)
+    r_orc = oracle.recall(oids[q], gt, k)
+    assert r_gpu >= r_orc - 0.005, (r_gpu, r_orc)
+
+
+@pytest.mark.parametrize("distance", ["sqrt", "squared"])
+def test_pipeline_labels_identical_on_shared_graph(ctx, oracle, distance):
+    """hdb_run's labels equal the oracle's labels computed from the kNN graph
+    the GPU built (bit-identical labels on the shared graph)."""
+    from gpu_hdbscan_b200 import HDB_DIST_SQRT, HDB_DIST_SQUARED
+    X = blobs(6000, 12, seed=21, blobs=8)
+    mode = HDB_DIST_SQRT if distance == "sqrt" else HDB_DIST_SQUARED
+    labels, stats = ctx.hdbscan(X, k=32, mpts=32, distance=mode)
+    G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6)
+    ids, dist = (_t(a) for a in ctx.knn_split(G))
+    if distance == "sqrt":
+        dist = oracle.fix_distances(X, ids)
+    _, ref_labels, ncl = oracle.hdbscan_from_knn(ids, dist, X, 32)
+    np.testing.assert_array_equal(_t(labels) if hasattr(labels, "cpu") else labels, ref_labels)
+    assert stats["num_clusters"] == ncl
+    assert ncl >= 2
+
+
+def test_pipeline_device_and_host_io_agree(ctx):
+    import torch
+    X = blobs(4000, 12, seed=3)
+    lh, _ = ctx.hdbscan(X)
+    ld, _ = ctx.hdbscan(torch.from_numpy(X).cuda())
+    np.testing.assert_array_equal(lh.numpy(), _t(ld))
+
+
+def test_invalid_knn_graphs_are_rejected(ctx):
+    from gpu_hdbscan_b200 import HdbError
+    rng = np.random.default_rng(1)
+    n, k = 200, 8
+    X = rng.normal(size=(n, 3)).astype(np.float32)
+    ids = np.stack([rng.choice(np.delete(np.arange(n), i), k, replace=False) for i in range(n)])
+    dist = np.ones((n, k), np.float32)
+    bad = ids.copy(); bad[3, 2] = bad[3, 1]
+    with pytest.raises(HdbError, match="repeats"):
+        ctx.buildEnhancedKNNG(bad, dist, X)
+    bad = ids.copy(); bad[5, 0] = 5
+    with pytest.raises(HdbError, match="own id"):
+        ctx.buildEnhancedKNNG(bad, dist, X)
+    bad = ids.copy(); bad[7, 3] = n
+    with pytest.raises(HdbError, match="outside"):
+        ctx.buildEnhancedKNNG(bad, dist, X)
+    g = ctx.buildEnhancedKNNG(ids, dist, X)  # the context still works
+    assert g.edges > 0
+
+
+def test_disconnected_graph_is_reported(ctx):
+    """Two groups whose kNN lists stay inside the group; every antihub falls in
+    the first group (ties broken by index), so the second is unreachable --
+    the reference exits with "MST montada incorretamente" (mst.cu:317-323)."""
+    from gpu_hdbscan_b200 import HdbError, _lib
+    n, k = 100, 4
+    ids = np.zeros((n, k), np.int32)
+    for g0 in (0, 50):
+        for i in range(50):
+            ids[g0 + i] = [g0 + (i + s) % 50 for s in (1, 2, 3, 4)]
+    X = np.random.default_rng(0).normal(size=(n, 2)).astype(np.float32)
+    dist = np.ones((n, k), np.float32)
+    g = ctx.buildEnhancedKNNG(ids, dist, X)
+    assert (g.antihubs.cpu().numpy() < 50).all()
+    with pytest.raises(HdbError) as e:
+        ctx.buildMST(g)
+    assert e.value.status == _lib.HDB_ERR_DISCONNECTED
+
+
+def test_small_and_edge_sizes(ctx, oracle):
+    # n just above k, and mpts larger than every cluster (all noise)
+    for n, k, mpts in [(40, 32, 32), (100, 8, 64 if False else 8), (33, 32, 2)]:
+        X = blobs(n, 3, seed=n)
+        labels, stats = ctx.hdbscan(X, k=k, mpts=min(mpts, k), sample_num=k // 2)
+        G = ctx.NNDescent(X, k=k, sample_num=k // 2)
+        ids = _t(ctx.knn_split(G)[0])
+        fd = oracle.fix_distances(X, ids)
+        _, ref, _ = oracle.hdbscan_from_knn(ids, fd, X, min(mpts, k))
+        np.testing.assert_array_equal(labels.numpy(), ref)
+
+
+def test_argument_errors(ctx):
+    from gpu_hdbscan_b200 import HdbError
+    X = blobs(500, 4, seed=1)
+    with pytest.raises(HdbError, match="mpts"):
+        ctx.hdbscan(X, k=16, mpts=1)
+    with pytest.raises(HdbError, match="SAMPLE_NUM"):
+        ctx.hdbscan(X, k=16, sample_num=9)
+    with pytest.raises(HdbError, match="k"):
+        ctx.hdbscan(X, k=64)
