@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""End-to-end HDBSCAN points/s on B200 (libhdb_b200.so).
+
+One step = one full run of the path (NN-Descent kNN graph -> enhanced kNN
+graph -> MST -> linkage tree -> condensed tree / EOM -> labels) over the whole
+synthetic workload.  `value` is measured with the input already resident in
+HBM; `e2e` is the same metric through the C ABI with host buffers (H2D copy of
+X and D2H copy of the labels inside every timed step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload blobs_10m_d12]
+
+N > 1 runs N independent replicas (one process per GPU, torchrun); the path
+has no cross-GPU exchange, so only the timing is reduced (max over ranks).
+`--impl reference` times the reference algorithm's CPU restatement (the
+oracle port, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "end-to-end HDBSCAN points/s on 1 B200: BF16-TC vs plain FP32, equal recall@k"
+UNIT = "points/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="blobs_10m_d12")
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="points in the CPU baseline sample (0: sized per workload)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """Per-row DRAM bytes of `kernel` from the committed ncu summary (profiles/),
+    or None.  Line format: TRAFFIC <kernel> bytes_per_row=<float> ..."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for name in sorted(os.listdir(pdir)):
+        if not name.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(pdir, name)) as f:
+            for line in f:
+                m = re.match(rf"TRAFFIC {re.escape(kernel)} bytes_per_row=([0-9.eE+]+)", line.strip())
+                if m:
+                    return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_run(workload, n_sample, steps):
+    """The reference algorithm on the host cores (oracle port, OpenMP over all
+    available threads): NN-Descent + the _new.cu stages on a sample."""
+    from gpu_hdbscan_b200 import synth
+    from oracle import oracle as O
+
+    w = synth.scaled(workload.name, n_sample, seed=workload.seed)
+    X = synth.generate(w)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ids, _ = O.nndescent(X, w.k, w.sample_num, w.iterations)
+        fd = O.fix_distances(X, ids)
+        O.hdbscan_from_knn(ids, fd, X, w.mpts)
+        times.append(time.perf_counter() - t0)
+    return {"value": n_sample * len(times) / sum(times), "unit": UNIT,
+            "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n_sample} points of the {workload.name} distribution "
+                      f"(d={w.d}, k={w.k}, mpts={w.mpts}), {len(times)} run(s), oracle port "
+                      f"(NN-Descent + enhanced kNNG + Kruskal + trees)"}
+
+
+def default_cpu_sample(w):
+    return 100_000 if w.d <= 16 else 20_000
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n_s = args.cpu_sample or default_cpu_sample(w)
+    for _ in range(args.warmup):
+        pass  # the CPU port has no warm-up state; warm-up steps are not repeated work
+    cb = cpu_baseline_run(w, n_s, max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": w.name, "n": w.n, "d": w.d, "k": w.k,
+                                             "mpts": w.mpts, "sample_points": n_s},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, w):
+    import torch
+    import torch.distributed as dist
+
+    import gpu_hdbscan_b200 as g
+    from gpu_hdbscan_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
+    # each replica clusters its own seeded copy of the workload
+    wr = synth.Workload(**{**w.__dict__, "seed": w.seed + 1000 * rank})
+    X = synth.generate_torch(wr, device=dev)
+    ctx = g.Context(local)
+    kw = dict(k=w.k, mpts=w.mpts, sample_num=w.sample_num, iterations=w.iterations,
+              precision=prec)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ctx.hdbscan(X, **kw)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        _, st = ctx.hdbscan(X, **kw)
+        stats.append(st)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = w.n * args.steps * world / (ms_max / 1e3)
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        Xh = X.cpu().pin_memory()
+        lab = torch.empty(w.n, dtype=torch.int32).pin_memory()
+        ctx.hdbscan(Xh, labels_out=lab, **kw)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.hdbscan(Xh, labels_out=lab, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": w.n * args.steps * world / (float(te.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(w.n * w.d * 4), "d2h_bytes_per_step": int(w.n * 4)}
+
+    if rank == 0:
+        hbm, _, peak_kind = measured_peaks()
+        last = stats[-1]
+        S = w.sample_num
+        launches = max(1, last["join_launches"])
+        # algorithmic bytes of the local join (per launch): staged sample rows,
+        # the sample lists and counters, and each pushed candidate (inbox entry,
+        # counter atomic, k-th distance read)
+        join_bytes = (last["join_rows_gathered"] * w.d * 4
+                      + launches * w.n * (2 * 2 * S * 4 + 2 * 4 + 2 * 1)
+                      + last["join_candidates"] * (8 + 4 + 4)) / launches
+        join_ms = last["join_ms"] / launches
+        achieved = join_bytes / (join_ms / 1e3) / 1e9
+        tpr = profiled_traffic("k_join")
+        roofline = {"kernel": "k_join (NN-Descent local join)", "bound": "hbm",
+                    "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(achieved / hbm, 4),
+                    "traffic": None if tpr is None else round(tpr * w.n),
+                    "peak_kind": peak_kind,
+                    "algorithmic_bytes_per_launch": round(join_bytes),
+                    "avg_launch_ms": round(join_ms, 4),
+                    "mean_rows_gathered_per_point": round(last["join_rows_gathered"] / launches / w.n, 2)}
+        cb = None
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline_run(w, args.cpu_sample or default_cpu_sample(w), 1)
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if prec == g.HDB_PREC_FP32 else "bf16",
+                "data": "synthetic",
+                "config": {"workload": w.name, "n": w.n, "d": w.d, "k": w.k, "mpts": w.mpts,
+                           "sample_num": w.sample_num, "iterations": w.iterations,
+                           "form": args.precision, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (X alone is "
+                                 f"{w.n * w.d * 4 / 1e6:.0f} MB)",
+                           "stage_ms": {s: round(last[f"ms_{s}"], 3) for s in
+                                        ("knn", "graph", "mst", "tree", "total")},
+                           "num_clusters": last["num_clusters"], "edges": last["edges"],
+                           "mst_rounds": last["mst_rounds"], "knn_dropped": last["knn_dropped"]},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+                "gpu_launches": int(sum(s["gpu_launches"] for s in stats))}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    from gpu_hdbscan_b200 import synth
+    w = synth.WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_ours(args, w)
+
+
+if __name__ == "__main__":
+    main()

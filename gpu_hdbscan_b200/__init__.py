@@ -201,6 +201,29 @@ class Context:
         _lib.check(self.L.hdb_run(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels), C.byref(st)))
         return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
 
+    def hdbscan_from_knn(self, G, X, k=32, mpts=32, distance=HDB_DIST_SQRT,
+                         stability=HDB_STAB_FP32):
+        """The stages after the kNN graph (hdb_run_knn): G [n, k, 2] NNDElement rows,
+        X [n, d].  Device tensors -> device labels; host arrays -> host labels
+        (host_io: copies inside the call)."""
+        torch = self._torch
+        host = not (isinstance(X, torch.Tensor) and X.is_cuda)
+        if host:
+            X = torch.as_tensor(X, dtype=torch.float32).contiguous()
+            G = torch.as_tensor(G).cpu().contiguous()
+            labels = torch.empty(X.shape[0], dtype=torch.int32)
+        else:
+            X = X.to(torch.float32).contiguous()
+            G = G.to(self.device).contiguous()
+            labels = torch.empty(X.shape[0], dtype=torch.int32, device=self.device)
+        n, d = X.shape
+        p = _lib.Params(_lib.KnnParams(k, max(1, k // 2), 0, HDB_PREC_FP32), mpts, distance,
+                        stability, 1 if host else 0)
+        st = _lib.RunStats()
+        _lib.check(self.L.hdb_run_knn(self.h, _ptr(G), _ptr(X), n, d, C.byref(p), _ptr(labels),
+                                      C.byref(st)))
+        return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
+
 
 _CUDART = None
 

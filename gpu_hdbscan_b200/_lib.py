@@ -23,7 +23,8 @@ HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 # Every symbol include/hdb/hdb.h declares.
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
-           "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run")
+           "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
+           "hdb_run_knn")
 
 
 class HdbError(RuntimeError):
@@ -52,7 +53,10 @@ class RunStats(C.Structure):
     _fields_ = [("edges", C.c_int64), ("num_antihubs", C.c_int32), ("num_clusters", C.c_int32),
                 ("condensed_size", C.c_int64), ("mst_rounds", C.c_int32),
                 ("knn_dropped", C.c_int64), ("ms_knn", C.c_float), ("ms_graph", C.c_float),
-                ("ms_mst", C.c_float), ("ms_tree", C.c_float), ("ms_total", C.c_float)]
+                ("ms_mst", C.c_float), ("ms_tree", C.c_float), ("ms_total", C.c_float),
+                ("join_ms", C.c_float), ("join_launches", C.c_int32),
+                ("join_rows_gathered", C.c_int64), ("join_candidates", C.c_int64),
+                ("gpu_launches", C.c_int64)]
 
 
 _L = None
@@ -84,6 +88,8 @@ def load(path: str = LIB_PATH):
         "hdb_condense_select": (C.c_int, [_P, _P, _I64, _I32, _I32, _P, C.POINTER(_I32), _P,
                                           C.POINTER(_I64), _P, C.POINTER(_I64)]),
         "hdb_run": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(Params), _P, C.POINTER(RunStats)]),
+        "hdb_run_knn": (C.c_int, [_P, _P, _P, _I64, _I32, C.POINTER(Params), _P,
+                                  C.POINTER(RunStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -139,6 +139,59 @@ HDB_API hdb_status hdb_condense_select(hdb_ctx *h, const hdb_linkage_node *hiera
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+void check_run_params(const hdb_params &p) {
+  check_knn_params(&p.knn);
+  const int32_t k = p.knn.k;
+  HDB_REQUIRE(p.mpts >= 2 && p.mpts <= k, HDB_ERR_ARG, "mpts must satisfy 2 <= mpts <= k");
+  HDB_REQUIRE(p.distance == HDB_DIST_SQRT || p.distance == HDB_DIST_SQUARED, HDB_ERR_ARG,
+              "unknown distance mode");
+  HDB_REQUIRE(p.stability == HDB_STAB_FP32 || p.stability == HDB_STAB_FP64, HDB_ERR_ARG,
+              "unknown stability mode");
+}
+
+// The stages after the kNN graph (HDBSCAN/_new.cu:243-347) on device arrays:
+// ids [n, k] decoded, core [n], X [n, d] -> labels [n].  Records ev[3..5].
+void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X, int64_t n,
+                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st) {
+  cudaStream_t s = ctx->stream;
+  hdb_graph g;
+  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr);
+  HDB_CUDA(cudaEventRecord(ctx->ev[3], s));
+  int32_t rounds = 0;
+  Buf<hdb_mst_edge> mst(ctx, n - 1);
+  boruvka_mst(ctx, &g, nullptr, mst, &rounds);
+  HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
+  int32_t ncl = 0;
+  {
+    Buf<hdb_linkage_node> hier(ctx, n - 1);
+    linkage_tree(ctx, mst, n, hier);
+    condense_select(ctx, hier, n, p.mpts, p.stability, labels, &ncl, nullptr, nullptr, nullptr,
+                    nullptr);
+  }
+  HDB_CUDA(cudaEventRecord(ctx->ev[5], s));
+  st->edges = g.edges;
+  st->num_antihubs = g.num_antihubs;
+  st->num_clusters = ncl;
+  st->mst_rounds = rounds;
+}
+
+void fill_times(Context *ctx, hdb_run_stats *st, bool with_knn) {
+  cudaEvent_t *ev = ctx->ev;
+  st->ms_knn = with_knn ? elapsed(ev[1], ev[2]) : 0.0f;
+  st->ms_graph = elapsed(ev[2], ev[3]);
+  st->ms_mst = elapsed(ev[3], ev[4]);
+  st->ms_tree = elapsed(ev[4], ev[5]);
+  st->ms_total = elapsed(ev[0], ev[6]);
+}
+
+}  // namespace
+
+extern "C" {
+
 HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
                            const hdb_params *params, int32_t *labels, hdb_run_stats *stats) {
   return guard([&] {
@@ -146,17 +199,15 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
     require_ptr(X, "X");
     require_ptr(labels, "labels");
     require_ptr(params, "params");
-    check_knn_params(&params->knn);
     const hdb_params &p = *params;
+    check_run_params(p);
     const int32_t k = p.knn.k;
-    HDB_REQUIRE(p.mpts >= 2 && p.mpts <= k, HDB_ERR_ARG, "mpts must satisfy 2 <= mpts <= k");
-    HDB_REQUIRE(p.distance == HDB_DIST_SQRT || p.distance == HDB_DIST_SQUARED, HDB_ERR_ARG,
-                "unknown distance mode");
-    HDB_REQUIRE(p.stability == HDB_STAB_FP32 || p.stability == HDB_STAB_FP64, HDB_ERR_ARG,
-                "unknown stability mode");
     HDB_REQUIRE(n > k && d >= 1, HDB_ERR_ARG, "need n > k and d >= 1");
     cudaStream_t st = ctx->stream;
     cudaEvent_t *ev = ctx->ev;
+    const int64_t launches0 = ctx->launches;
+    hdb_run_stats rs = {};
+    JoinStats js;
     HDB_CUDA(cudaEventRecord(ev[0], st));
     Buf<float> Xd;
     Buf<int32_t> Ld;
@@ -175,44 +226,85 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
     Buf<float> core(ctx, n);
     {
       Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
-      nndescent(ctx, Xuse, n, d, p.knn, G, &dropped);
+      nndescent(ctx, Xuse, n, d, p.knn, G, &dropped, &js);
       HDB_CUDA(cudaEventRecord(ev[2], st));
       Buf<float> dist;
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
       core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
     }
-    hdb_graph g;
-    build_enhanced_knng(ctx, ids, core, Xuse, n, d, k, &g, nullptr);
-    HDB_CUDA(cudaEventRecord(ev[3], st));
-    int32_t rounds = 0;
-    Buf<hdb_mst_edge> mst(ctx, n - 1);
-    boruvka_mst(ctx, &g, nullptr, mst, &rounds);
-    HDB_CUDA(cudaEventRecord(ev[4], st));
-    int32_t ncl = 0;
-    {
-      Buf<hdb_linkage_node> hier(ctx, n - 1);
-      linkage_tree(ctx, mst, n, hier);
-      condense_select(ctx, hier, n, p.mpts, p.stability, Luse, &ncl, nullptr, nullptr, nullptr,
-                      nullptr);
-    }
-    HDB_CUDA(cudaEventRecord(ev[5], st));
+    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs);
     if (p.host_io)
       HDB_CUDA(cudaMemcpyAsync(labels, Luse, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     HDB_CUDA(cudaEventRecord(ev[6], st));
     ctx->sync();
     if (stats) {
-      stats->edges = g.edges;
-      stats->num_antihubs = g.num_antihubs;
-      stats->num_clusters = ncl;
-      stats->condensed_size = 0;
-      stats->mst_rounds = rounds;
-      stats->knn_dropped = dropped;
-      stats->ms_knn = elapsed(ev[1], ev[2]);
-      stats->ms_graph = elapsed(ev[2], ev[3]);
-      stats->ms_mst = elapsed(ev[3], ev[4]);
-      stats->ms_tree = elapsed(ev[4], ev[5]);
-      stats->ms_total = elapsed(ev[0], ev[6]);
+      rs.knn_dropped = dropped;
+      fill_times(ctx, &rs, true);
+      rs.join_ms = (float)js.ms;
+      rs.join_launches = (int32_t)js.launches;
+      rs.join_rows_gathered = js.rows_gathered;
+      rs.join_candidates = js.candidates;
+      rs.gpu_launches = ctx->launches - launches0;
+      *stats = rs;
+    }
+  });
+}
+
+HDB_API hdb_status hdb_run_knn(hdb_ctx *h, const hdb_nnd_element *G, const float *X, int64_t n,
+                               int32_t d, const hdb_params *params, int32_t *labels,
+                               hdb_run_stats *stats) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(G, "G");
+    require_ptr(X, "X");
+    require_ptr(labels, "labels");
+    require_ptr(params, "params");
+    const hdb_params &p = *params;
+    check_run_params(p);
+    const int32_t k = p.knn.k;
+    HDB_REQUIRE(n > k && d >= 1, HDB_ERR_ARG, "need n > k and d >= 1");
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t *ev = ctx->ev;
+    const int64_t launches0 = ctx->launches;
+    hdb_run_stats rs = {};
+    HDB_CUDA(cudaEventRecord(ev[0], st));
+    Buf<float> Xd;
+    Buf<int32_t> Ld;
+    Buf<hdb_nnd_element> Gd;
+    const float *Xuse = X;
+    const hdb_nnd_element *Guse = G;
+    int32_t *Luse = labels;
+    if (p.host_io) {
+      Xd = Buf<float>(ctx, (size_t)n * d);
+      Gd = Buf<hdb_nnd_element>(ctx, (size_t)n * k);
+      Ld = Buf<int32_t>(ctx, n);
+      HDB_CUDA(cudaMemcpyAsync(Xd, X, (size_t)n * d * sizeof(float), cudaMemcpyHostToDevice, st));
+      HDB_CUDA(cudaMemcpyAsync(Gd, G, (size_t)n * k * sizeof(hdb_nnd_element),
+                               cudaMemcpyHostToDevice, st));
+      Xuse = Xd;
+      Guse = Gd;
+      Luse = Ld;
+    }
+    HDB_CUDA(cudaEventRecord(ev[1], st));
+    HDB_CUDA(cudaEventRecord(ev[2], st));
+    Buf<int32_t> ids(ctx, (size_t)n * k);
+    Buf<float> core(ctx, n);
+    {
+      Buf<float> dist;
+      if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
+      knn_split(ctx, Guse, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
+      core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
+    }
+    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs);
+    if (p.host_io)
+      HDB_CUDA(cudaMemcpyAsync(labels, Luse, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    HDB_CUDA(cudaEventRecord(ev[6], st));
+    ctx->sync();
+    if (stats) {
+      fill_times(ctx, &rs, false);
+      rs.gpu_launches = ctx->launches - launches0;
+      *stats = rs;
     }
   });
 }

@@ -48,7 +48,8 @@ Scratch::~Scratch() {
 void Context::sync() { HDB_CUDA(cudaStreamSynchronize(stream)); }
 
 uint32_t Context::take_dev_err() {
-  uint32_t *h = static_cast<uint32_t *>(pinned);
+  // its own slot: callers keep other values staged at the start of `pinned`
+  uint32_t *h = reinterpret_cast<uint32_t *>(static_cast<char *>(pinned) + kPinnedErrOffset);
   HDB_CUDA(cudaMemcpyAsync(h, dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
   HDB_CUDA(cudaMemsetAsync(dev_err, 0, sizeof(uint32_t), stream));
   sync();
@@ -98,7 +99,7 @@ HDB_API hdb_status hdb_create(hdb_ctx **out, int32_t device) {
       c.stream = c.own_stream;
       HDB_CUDA(cudaMalloc(&c.dev_err, 4 * sizeof(uint32_t)));
       HDB_CUDA(cudaMemset(c.dev_err, 0, 4 * sizeof(uint32_t)));
-      HDB_CUDA(cudaMallocHost(&c.pinned, 4096));
+      HDB_CUDA(cudaMallocHost(&c.pinned, kPinnedBytes));
       for (auto &e : c.ev) HDB_CUDA(cudaEventCreate(&e));
       // Keep freed scratch cached in the stream-ordered pool between calls.
       cudaMemPool_t pool;

@@ -293,6 +293,7 @@ void core_distances(Context *ctx, const float *dist, const float *X, const int32
     k_core_sqrt<<<g, 256, 0, ctx->stream>>>(X, ids, n, d, k, core);
   else
     k_core_from_dist<<<g, 256, 0, ctx->stream>>>(dist, n, k, core);
+  ctx->launches++;
   HDB_CHECK_LAUNCH();
 }
 
@@ -308,7 +309,7 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   // 1. in-degrees + validation
   Buf<int32_t> deg(ctx, n);
   HDB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(int32_t), st));
-  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err);
+  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   uint32_t err = ctx->take_dev_err();
   HDB_REQUIRE(!(err & DEVERR_ID_RANGE), HDB_ERR_ARG, "kNN graph: neighbour id outside [0, n)");
@@ -321,9 +322,9 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   Buf<uint32_t> hist(ctx, kDegHistBins);
   Buf<int64_t> thr(ctx, 4);
   HDB_CUDA(cudaMemsetAsync(hist, 0, kDegHistBins * sizeof(uint32_t), st));
-  k_degree_hist<<<ge, 256, 0, st>>>(deg, n, hist);
+  k_degree_hist<<<ge, 256, 0, st>>>(deg, n, hist); ctx->launches++;
   HDB_CHECK_LAUNCH();
-  k_find_threshold<<<1, 1024, 0, st>>>(hist, P, thr);
+  k_find_threshold<<<1, 1024, 0, st>>>(hist, P, thr); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int64_t *h = static_cast<int64_t *>(ctx->pinned);
   HDB_CUDA(cudaMemcpyAsync(h, thr, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -335,23 +336,23 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   Buf<int32_t> is_ah(ctx, n);
   Buf<int64_t> pos(ctx, n + 1);
   Buf<int32_t> flag(ctx, n);
-  k_flag_below<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, is_ah, at == missing ? 1 : 0);
+  k_flag_below<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, is_ah, at == missing ? 1 : 0); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (at > missing) {
-    k_flag_eq<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, flag);
+    k_flag_eq<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, flag); ctx->launches++;
     HDB_CHECK_LAUNCH();
     scan_exclusive_i32_i64(ctx, flag, pos, n, nullptr);
     Buf<uint64_t> keys(ctx, at);
-    k_tie_keys<<<ge, 256, 0, st>>>(deg, flag, pos, ids, n, k, keys);
+    k_tie_keys<<<ge, 256, 0, st>>>(deg, flag, pos, ids, n, k, keys); ctx->launches++;
     HDB_CHECK_LAUNCH();
     radix_sort_u64(ctx, keys, nullptr, at, 0, 64);
-    k_mark_selected_ties<<<grid_for(ctx, missing, 256), 256, 0, st>>>(keys, missing, is_ah);
+    k_mark_selected_ties<<<grid_for(ctx, missing, 256), 256, 0, st>>>(keys, missing, is_ah); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   ensure_capacity(ctx, (void **)&ctx->g_antihubs, &ctx->g_antihubs_cap,
                   (size_t)(P > 0 ? P : 1) * sizeof(int32_t));
   scan_exclusive_i32_i64(ctx, is_ah, pos, n, pos.get() + n);
-  k_compact_flags<<<ge, 256, 0, st>>>(is_ah, pos, n, ctx->g_antihubs);
+  k_compact_flags<<<ge, 256, 0, st>>>(is_ah, pos, n, ctx->g_antihubs); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (times) HDB_CUDA(cudaEventRecord(times->after_antihubs, st));
 
@@ -359,14 +360,14 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   Buf<uint32_t> mutual(ctx, n);
   Buf<int32_t> revcnt(ctx, n), nonmutual(ctx, n);
   HDB_CUDA(cudaMemsetAsync(revcnt, 0, n * sizeof(int32_t), st));
-  k_mutual<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, mutual, revcnt, nonmutual);
+  k_mutual<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, mutual, revcnt, nonmutual); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   // 4. row sizes -> nindex
   ensure_capacity(ctx, (void **)&ctx->g_nindex, &ctx->g_nindex_cap, (n + 1) * sizeof(int64_t));
   {
     Buf<int32_t> sizes(ctx, n);
-    k_row_sizes<<<ge, 256, 0, st>>>(revcnt, is_ah, n, k, P, sizes);
+    k_row_sizes<<<ge, 256, 0, st>>>(revcnt, is_ah, n, k, P, sizes); ctx->launches++;
     HDB_CHECK_LAUNCH();
     scan_exclusive_i32_i64(ctx, sizes, ctx->g_nindex, n, ctx->g_nindex + n);
   }
@@ -383,7 +384,7 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   HDB_REQUIRE(E < (int64_t(1) << 32), HDB_ERR_ARG,
               "enhanced kNN graph has 2^32 or more edges (edge indices are 32-bit)");
   Buf<uint32_t> rkeys(ctx, R), rvals(ctx, R);
-  k_emit_reverse<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, mutual, roff, n, k, rkeys, rvals);
+  k_emit_reverse<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, mutual, roff, n, k, rkeys, rvals); ctx->launches++;
   HDB_CHECK_LAUNCH();
   radix_sort_u32(ctx, rkeys, rvals, R, 0, bits_for(n));
   Buf<int64_t> rev_off(ctx, n + 1);
@@ -393,15 +394,15 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   ensure_capacity(ctx, (void **)&ctx->g_nlist, &ctx->g_nlist_cap, (size_t)E * sizeof(int32_t));
   ensure_capacity(ctx, (void **)&ctx->g_eweight, &ctx->g_eweight_cap, (size_t)E * sizeof(float));
   k_fill<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, core, ctx->g_nindex, revcnt, rev_off, rvals, n,
-                                             k, ctx->g_nlist, ctx->g_eweight);
+                                             k, ctx->g_nlist, ctx->g_eweight); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (P > 1) {
     Buf<float> Xah(ctx, (size_t)P * d);
     k_gather_rows<<<grid_for(ctx, (int64_t)P * d, 256), 256, 0, st>>>(X, ctx->g_antihubs, P, d,
-                                                                        Xah);
+                                                                        Xah); ctx->launches++;
     HDB_CHECK_LAUNCH();
     k_clique<<<P, 256, d * sizeof(float), st>>>(ctx->g_antihubs, P, Xah, d, core, ctx->g_nindex,
-                                                revcnt, k, ctx->g_nlist, ctx->g_eweight);
+                                                revcnt, k, ctx->g_nlist, ctx->g_eweight); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   ctx->sync();

@@ -101,6 +101,11 @@ struct Buf {
   operator T *() const { return s.as<T>(); }
 };
 
+// Pinned host staging area: bytes [0, kPinnedErrOffset) are free for callers,
+// the device error word is read back at kPinnedErrOffset.
+constexpr size_t kPinnedBytes = 4096;
+constexpr size_t kPinnedErrOffset = 3072;
+
 struct Context {
   int device = 0;
   int num_sms = 148;
@@ -115,6 +120,12 @@ struct Context {
   int32_t *g_antihubs = nullptr;
   size_t g_nindex_cap = 0, g_nlist_cap = 0, g_eweight_cap = 0, g_antihubs_cap = 0;
   cudaEvent_t ev[8] = {};
+  // Kernel launches issued by this context (all stages count them).
+  int64_t launches = 0;
+  // Live timing of the NN-Descent local join (hdb_run_stats.join_*).
+  cudaEvent_t join_ev[2] = {};
+  double join_ms = 0.0;
+  int64_t join_launches = 0;
 
   void sync();
   // Reads and clears the device error word.

@@ -14,6 +14,8 @@
 //  * distances are the reference's sequential FP32 difference sum
 //    (nndescent.cu:1086-1093, fmaf per element), so every pair has one exact
 //    value wherever it is computed.
+#include <vector>
+
 #include "hdb_internal.cuh"
 #include "knn.cuh"
 
@@ -283,13 +285,13 @@ struct JoinSmem {
   __host__ __device__ static int floats(int dp) { return kIds + 2 * kMat + 64 * dp; }
 };
 
-__device__ __forceinline__ void push_candidate(int32_t target, int32_t id, float d,
+__device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
                                                const float *__restrict__ worst,
                                                int32_t *__restrict__ inbox_cnt,
                                                uint64_t *__restrict__ inbox,
                                                unsigned long long *__restrict__ ovf,
                                                unsigned long long *__restrict__ dropped) {
-  if (!(d < worst[target])) return;  // cannot enter the target's list
+  if (!(d < worst[target])) return 0;  // cannot enter the target's list
   int slot = atomicAdd(&inbox_cnt[target], 1);
   uint64_t key = pack(d, id);
   if (slot < kInboxCap) {
@@ -298,6 +300,7 @@ __device__ __forceinline__ void push_candidate(int32_t target, int32_t id, float
     atomicMin(&ovf[target], (unsigned long long)key);
     atomicAdd(dropped, 1ull);
   }
+  return 1;
 }
 
 // Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).
@@ -307,8 +310,12 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
                        int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
                        const float *__restrict__ worst, int32_t *__restrict__ inbox_cnt,
                        uint64_t *__restrict__ inbox, unsigned long long *__restrict__ ovf,
-                       unsigned long long *__restrict__ dropped) {
+                       unsigned long long *__restrict__ dropped,
+                       unsigned long long *__restrict__ jstats) {
   extern __shared__ float smem_join[];
+  __shared__ unsigned long long blk_rows, blk_cands;
+  if (threadIdx.x == 0) { blk_rows = 0; blk_cands = 0; }
+  __syncthreads();
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
   const int dp = (d & 1) ? d : d + 1;
@@ -347,6 +354,7 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
     __syncwarp();
     const int T = nn + no;
     if (nn == 0 || T < 2) continue;
+    if (lane == 0) atomicAdd(&blk_rows, (unsigned long long)T);
     for (int idx = lane; idx < T * d; idx += 32) {
       int r = idx / d, c = idx - r * d;
       Xs[r * dp + c] = __ldg(X + (int64_t)ids[r] * d + c);
@@ -385,10 +393,14 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
         best2 = c < best2 ? c : best2;
       }
       const int32_t x = ids[lane];
+      int pushed = 0;
       if (best1 != ~0ull)
-        push_candidate(x, pk_id(best1), pk_dist(best1), worst, inbox_cnt, inbox, ovf, dropped);
+        pushed += push_candidate(x, pk_id(best1), pk_dist(best1), worst, inbox_cnt, inbox, ovf,
+                                 dropped);
       if (best2 != ~0ull)
-        push_candidate(x, pk_id(best2), pk_dist(best2), worst, inbox_cnt, inbox, ovf, dropped);
+        pushed += push_candidate(x, pk_id(best2), pk_dist(best2), worst, inbox_cnt, inbox, ovf,
+                                 dropped);
+      if (pushed) atomicAdd(&blk_cands, (unsigned long long)pushed);
     }
     if (lane < no) {
       uint64_t best = ~0ull;
@@ -396,11 +408,17 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
         uint64_t c = pack(Dno[a * 33 + lane], ids[a]);
         best = c < best ? c : best;
       }
-      if (best != ~0ull)
-        push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, inbox_cnt, inbox, ovf,
-                       dropped);
+      if (best != ~0ull &&
+          push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, inbox_cnt, inbox, ovf,
+                         dropped))
+        atomicAdd(&blk_cands, 1ull);
     }
     __syncwarp();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && jstats) {
+    atomicAdd(&jstats[0], blk_rows);
+    atomicAdd(&jstats[1], blk_cands);
   }
 }
 
@@ -438,7 +456,7 @@ __global__ void k_fix_distances(const float *__restrict__ X, int64_t n, int d,
 }  // namespace
 
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
-               hdb_nnd_element *G, int64_t *dropped_out) {
+               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js) {
   const int k = p.k, S = p.sample_num;
   HDB_REQUIRE(k >= 1 && k <= kMaxK, HDB_ERR_ARG, "NN-Descent: k must be in [1, 32]");
   HDB_REQUIRE(S >= 1 && 2 * S <= k, HDB_ERR_ARG,
@@ -455,16 +473,21 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
       inbox_cnt(ctx, n);
   Buf<int8_t> nf(ctx, n), of(ctx, n);
   Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
-  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 1);
+  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
   HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
-  HDB_CUDA(cudaMemsetAsync(dropped, 0, 8, st));
+  HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+  std::vector<cudaEvent_t> jev;
+  if (js) {
+    jev.resize(2 * (size_t)p.iterations);
+    for (auto &e : jev) HDB_CUDA(cudaEventCreate(&e));
+  }
 
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
-  k_init<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, gid, gdist, worst);
+  k_init<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, gid, gdist, worst); ctx->launches++;
   HDB_CHECK_LAUNCH();
   const size_t smem_sample = (size_t)wpb * kMergeSmemU64 * sizeof(uint64_t);
   const int dp = (d & 1) ? d : d + 1;
@@ -478,32 +501,45 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   for (int it = 0; it < p.iterations; it++) {
     k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst,
                                                        inbox_cnt, inbox, ovf, newS, oldS, nf, of,
-                                                       nrev, orev);
+                                                       nrev, orev); ctx->launches++;
     HDB_CHECK_LAUNCH();
+    if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
     k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
-                                                  inbox_cnt, inbox, ovf, dropped);
+                                                  inbox_cnt, inbox, ovf, dropped,
+                                                  dropped.get() + 1); ctx->launches++;
+    if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
     HDB_CHECK_LAUNCH();
   }
-  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, inbox_cnt, inbox, ovf, G);
+  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, inbox_cnt, inbox, ovf, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
-  if (dropped_out) {
-    HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 8, cudaMemcpyDeviceToHost, st));
-    ctx->sync();
-    *dropped_out = *static_cast<int64_t *>(ctx->pinned);
-  } else {
-    ctx->sync();
+  HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  const int64_t *hs = static_cast<const int64_t *>(ctx->pinned);
+  if (dropped_out) *dropped_out = hs[0];
+  if (js) {
+    js->rows_gathered = hs[1];
+    js->candidates = hs[2];
+    js->launches = p.iterations;
+    js->ms = 0.0;
+    for (int it = 0; it < p.iterations; it++) {
+      float ms = 0.0f;
+      HDB_CUDA(cudaEventElapsedTime(&ms, jev[2 * it], jev[2 * it + 1]));
+      js->ms += ms;
+    }
+    for (auto &e : jev) cudaEventDestroy(e);
   }
 }
 
 void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,
                float *dist) {
-  k_split<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(G, n * k, ids, dist);
+  k_split<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(G, n * k, ids, dist); ctx->launches++;
   HDB_CHECK_LAUNCH();
 }
 
 void fix_distances(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
                    int32_t k, float *dist) {
-  k_fix_distances<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(X, n, d, ids, k, dist);
+  k_fix_distances<<<grid_for(ctx, n * k, 256), 256, 0, ctx->stream>>>(X, n, d, ids, k, dist); ctx->launches++;
   HDB_CHECK_LAUNCH();
 }
 

@@ -4,8 +4,15 @@
 
 namespace hdb {
 
+// Live measurement of the local-join kernel: summed CUDA-event time over
+// its launches, rows staged in shared memory and candidates pushed.
+struct JoinStats {
+  double ms = 0.0;
+  int64_t launches = 0, rows_gathered = 0, candidates = 0;
+};
+
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
-               hdb_nnd_element *G, int64_t *dropped_out);
+               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr);
 void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,
                float *dist);
 void fix_distances(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,

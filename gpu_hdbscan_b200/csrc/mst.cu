@@ -246,7 +246,7 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
   const int gw = grid_for(ctx, n, kWarps);
   Buf<int32_t> cnt(ctx, n);
   Buf<int64_t> off(ctx, n + 1);
-  k_count_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, n, cnt, ctx->dev_err);
+  k_count_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, n, cnt, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
               "MST: graph has a neighbour id outside [0, nodes)");
@@ -256,7 +256,7 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
   ctx->sync();
   int64_t m = h[0];
   Buf<CEdge> el(ctx, m > 0 ? m : 1), el2(ctx, m > 0 ? m : 1);
-  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, el);
+  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, el); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   Buf<unsigned long long> minkey(ctx, n);
@@ -266,8 +266,8 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
   HDB_CUDA(cudaMemsetAsync(minkey, 0xff, n * sizeof(unsigned long long), st));
   HDB_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
   const int gn = grid_for(ctx, n, 256);
-  k_iota<<<gn, 256, 0, st>>>(parent, n);
-  k_iota<<<gn, 256, 0, st>>>(reps, n);
+  k_iota<<<gn, 256, 0, st>>>(parent, n); ctx->launches++;
+  k_iota<<<gn, 256, 0, st>>>(reps, n); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int64_t nr = n;
   int rounds = 0;
@@ -278,14 +278,14 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
     rounds++;
     const int ge = grid_for(ctx, m, 256);
     const int gr = grid_for(ctx, nr, 256);
-    k_min_edge<<<ge, 256, 0, st>>>(ep, m, minkey);
-    k_winner<<<ge, 256, 0, st>>>(ep, m, minkey, other);
-    k_hook<<<gr, 256, 0, st>>>(rp, nr, minkey, other, parent, keys, counters, n - 1);
-    k_reset_minkey<<<gr, 256, 0, st>>>(rp, nr, minkey);
-    k_jump<<<gr, 256, 0, st>>>(rp, nr, parent, ctx->dev_err);
+    k_min_edge<<<ge, 256, 0, st>>>(ep, m, minkey); ctx->launches++;
+    k_winner<<<ge, 256, 0, st>>>(ep, m, minkey, other); ctx->launches++;
+    k_hook<<<gr, 256, 0, st>>>(rp, nr, minkey, other, parent, keys, counters, n - 1); ctx->launches++;
+    k_reset_minkey<<<gr, 256, 0, st>>>(rp, nr, minkey); ctx->launches++;
+    k_jump<<<gr, 256, 0, st>>>(rp, nr, parent, ctx->dev_err); ctx->launches++;
     HDB_CUDA(cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(unsigned long long), st));
-    k_relabel_filter<<<ge, 256, 0, st>>>(ep, m, parent, ep2, counters.get() + 1);
-    k_roots<<<gr, 256, 0, st>>>(rp, nr, parent, rp2, counters.get() + 2);
+    k_relabel_filter<<<ge, 256, 0, st>>>(ep, m, parent, ep2, counters.get() + 1); ctx->launches++;
+    k_roots<<<gr, 256, 0, st>>>(rp, nr, parent, rp2, counters.get() + 2); ctx->launches++;
     HDB_CHECK_LAUNCH();
     HDB_CUDA(cudaMemcpyAsync(h, counters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ctx->sync();
@@ -306,7 +306,7 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
   radix_sort_u64(ctx, keys, nullptr, n - 1, 0, 64);
   if (in_mst) HDB_CUDA(cudaMemsetAsync(in_mst, 0, g->edges, st));
   k_gather_mst<<<grid_for(ctx, n - 1, 256), 256, 0, st>>>(keys, n - 1, g->nindex, g->nlist,
-                                                          g->eweight, n, mst, in_mst);
+                                                          g->eweight, n, mst, in_mst); ctx->launches++;
   HDB_CHECK_LAUNCH();
   ctx->sync();
   if (rounds_out) *rounds_out = rounds;
@@ -318,11 +318,11 @@ void sort_mst_edges(Context *ctx, hdb_mst_edge *edges, int64_t m) {
   Buf<uint32_t> keys(ctx, m), idx(ctx, m);
   Buf<hdb_mst_edge> tmp(ctx, m);
   const int g = grid_for(ctx, m, 256);
-  k_edge_keys<<<g, 256, 0, st>>>(edges, m, keys, idx);
+  k_edge_keys<<<g, 256, 0, st>>>(edges, m, keys, idx); ctx->launches++;
   HDB_CHECK_LAUNCH();
   radix_sort_u32(ctx, keys, idx, m, 0, 32);
   HDB_CUDA(cudaMemcpyAsync(tmp, edges, m * sizeof(hdb_mst_edge), cudaMemcpyDeviceToDevice, st));
-  k_permute_edges<<<g, 256, 0, st>>>(tmp, idx, m, edges);
+  k_permute_edges<<<g, 256, 0, st>>>(tmp, idx, m, edges); ctx->launches++;
   HDB_CHECK_LAUNCH();
   ctx->sync();
 }

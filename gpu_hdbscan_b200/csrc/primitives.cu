@@ -106,16 +106,16 @@ void scan_impl(Context *ctx, const In *in, Out *out, int64_t n, Out *total) {
   }
   int64_t nb = ceil_div(n, kScanTile);
   if (nb == 1) {
-    scan_tile_apply<In, Out><<<1, kScanThreads, 0, ctx->stream>>>(in, out, nullptr, n, total);
+    scan_tile_apply<In, Out><<<1, kScanThreads, 0, ctx->stream>>>(in, out, nullptr, n, total); ctx->launches++;
     HDB_CHECK_LAUNCH();
     return;
   }
   Buf<Out> sums(ctx, nb), offs(ctx, nb);
-  scan_tile_sums<In, Out><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, sums, n);
+  scan_tile_sums<In, Out><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, sums, n); ctx->launches++;
   HDB_CHECK_LAUNCH();
   scan_impl<Out, Out>(ctx, sums, offs, nb, (Out *)nullptr);
   scan_tile_apply<In, Out><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, out, offs, n,
-                                                                            total);
+                                                                            total); ctx->launches++;
   HDB_CHECK_LAUNCH();
 }
 
@@ -213,7 +213,7 @@ void radix_sort_impl(Context *ctx, K *keys, uint32_t *vals, int64_t n, int begin
   uint32_t *vin = vals, *vout = vals ? vtmp.get() : nullptr;
   int passes = 0;
   for (int shift = begin_bit; shift < end_bit; shift += 8, passes++) {
-    radix_hist<K><<<nb, kSortThreads, 0, ctx->stream>>>(kin, counts, n, shift, nb);
+    radix_hist<K><<<nb, kSortThreads, 0, ctx->stream>>>(kin, counts, n, shift, nb); ctx->launches++;
     HDB_CHECK_LAUNCH();
     scan_exclusive_u32_u32(ctx, counts, offs, (int64_t)nb * 256, nullptr);
     if (vals)
@@ -222,6 +222,7 @@ void radix_sort_impl(Context *ctx, K *keys, uint32_t *vals, int64_t n, int begin
     else
       radix_scatter<K, false><<<nb, kSortThreads, 0, ctx->stream>>>(kin, nullptr, kout, nullptr,
                                                                     offs, n, shift, nb);
+    ctx->launches++;
     HDB_CHECK_LAUNCH();
     K *t = kin; kin = kout; kout = t;
     uint32_t *tv = vin; vin = vout; vout = tv;

@@ -608,24 +608,24 @@ void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_
   Buf<int32_t> la(ctx, m), lb(ctx, m), ufp(ctx, total), maxr(ctx, total), seen(ctx, total),
       acc(ctx, total), size(ctx, total);
   const int gm = grid_for(ctx, m, 256), gt = grid_for(ctx, total, 256);
-  k_validate_mst<<<gm, 256, 0, st>>>(mst, m, n, ctx->dev_err);
+  k_validate_mst<<<gm, 256, 0, st>>>(mst, m, n, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
               "linkage tree: MST edge endpoint outside [0, n)");
-  k_link_init<<<gm, 256, 0, st>>>(mst, m, la, lb);
-  k_uf_init<<<gt, 256, 0, st>>>(total, n, ufp, maxr, seen, acc, size);
+  k_link_init<<<gm, 256, 0, st>>>(mst, m, la, lb); ctx->launches++;
+  k_uf_init<<<gt, 256, 0, st>>>(total, n, ufp, maxr, seen, acc, size); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int64_t S = 1;
   while (S < m) S <<= 1;
   for (; S >= 2; S >>= 1) {
-    k_level_union<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, ctx->dev_err);
-    k_level_tag<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr, seen, acc, size);
-    k_level_produce<<<gm, 256, 0, st>>>(la, m, S, n, ufp, maxr, acc, size);
-    k_level_relabel<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr);
-    k_level_reset<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, maxr, seen, acc);
+    k_level_union<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, ctx->dev_err); ctx->launches++;
+    k_level_tag<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr, seen, acc, size); ctx->launches++;
+    k_level_produce<<<gm, 256, 0, st>>>(la, m, S, n, ufp, maxr, acc, size); ctx->launches++;
+    k_level_relabel<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr); ctx->launches++;
+    k_level_reset<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, maxr, seen, acc); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
-  k_link_out<<<gm, 256, 0, st>>>(mst, la, lb, size, m, n, out);
+  k_link_out<<<gm, 256, 0, st>>>(mst, la, lb, size, m, n, out); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_TIMEOUT), HDB_ERR_INTERNAL,
               "linkage tree: union-find exceeded its step bound");
@@ -648,25 +648,25 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   Buf<int8_t> side(ctx, total), kind(ctx, m), visited(ctx, m);
   Buf<float> lam(ctx, m);
   HDB_CUDA(cudaMemsetAsync(par, 0xff, total * sizeof(int32_t), st));
-  k_validate_hier<<<gm, 256, 0, st>>>(t, ctx->dev_err);
+  k_validate_hier<<<gm, 256, 0, st>>>(t, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
               "condensed tree: hierarchy is not a valid single-linkage tree");
-  k_nodes<<<gm, 256, 0, st>>>(t, par, side, kind, visited, lam);
+  k_nodes<<<gm, 256, 0, st>>>(t, par, side, kind, visited, lam); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   // depth / preorder / chain heads by pointer jumping
   Buf<int32_t> jmp(ctx, m), jmp2(ctx, m), head(ctx, m);
   Buf<int64_t> dep(ctx, m), dep2(ctx, m), pre(ctx, m), pre2(ctx, m);
   Buf<int32_t> changed(ctx, 2);
-  k_path_init<<<gm, 256, 0, st>>>(t, par, side, kind, visited, jmp, dep, pre, head);
+  k_path_init<<<gm, 256, 0, st>>>(t, par, side, kind, visited, jmp, dep, pre, head); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int32_t *j0 = jmp, *j1 = jmp2;
   int64_t *d0 = dep, *d1 = dep2, *p0 = pre, *p1 = pre2;
   for (int it = 0; it < 64; it++) {
     HDB_CUDA(cudaMemsetAsync(changed, 0, 2 * sizeof(int32_t), st));
-    k_path_jump<<<gm, 256, 0, st>>>(m, j0, d0, p0, j1, d1, p1, changed);
-    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed.get() + 1);
+    k_path_jump<<<gm, 256, 0, st>>>(m, j0, d0, p0, j1, d1, p1, changed); ctx->launches++;
+    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed.get() + 1); ctx->launches++;
     HDB_CHECK_LAUNCH();
     HDB_CUDA(cudaMemcpyAsync(hflag, changed, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     ctx->sync();
@@ -679,7 +679,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   // head pointers may need extra rounds beyond the path sums
   for (int it = 0; it < 64; it++) {
     HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
-    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed);
+    k_head_jump<<<gm, 256, 0, st>>>(m, head, changed); ctx->launches++;
     HDB_CHECK_LAUNCH();
     HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     ctx->sync();
@@ -689,7 +689,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   // split nodes in BFS order -> cluster ids
   Buf<int32_t> flag(ctx, m);
   Buf<int64_t> pos(ctx, m + 1);
-  k_split_keys<<<gm, 256, 0, st>>>(m, kind, visited, d0, p0, flag);
+  k_split_keys<<<gm, 256, 0, st>>>(m, kind, visited, d0, p0, flag); ctx->launches++;
   HDB_CHECK_LAUNCH();
   scan_exclusive_i32_i64(ctx, flag, pos, m, pos.get() + m);
   HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -701,10 +701,10 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   Buf<int32_t> cid(ctx, m), split_rank(ctx, m);
   HDB_CUDA(cudaMemsetAsync(cid, 0xff, m * sizeof(int32_t), st));
   if (ns > 0) {
-    k_split_emit<<<gm, 256, 0, st>>>(m, flag, pos, d0, p0, skeys, snodes);
+    k_split_emit<<<gm, 256, 0, st>>>(m, flag, pos, d0, p0, skeys, snodes); ctx->launches++;
     HDB_CHECK_LAUNCH();
     radix_sort_u64(ctx, skeys, snodes, ns, 0, 64);
-    k_assign_cids<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, cid, split_rank);
+    k_assign_cids<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, cid, split_rank); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   // root cluster id
@@ -715,7 +715,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     ctx->sync();
   }
   Buf<int32_t> ncl(ctx, m);
-  k_node_cluster<<<gm, 256, 0, st>>>(m, n, visited, head, cid, ncl);
+  k_node_cluster<<<gm, 256, 0, st>>>(m, n, visited, head, cid, ncl); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   // per-cluster info
@@ -730,7 +730,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   HDB_CUDA(cudaMemsetAsync(self_sel, 0, C, st));
   if (ns > 0) {
     k_cluster_info<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, ncl, lam, birth,
-                                                            cparent, ckid0);
+                                                            cparent, ckid0); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
 
@@ -740,37 +740,37 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   HDB_CUDA(cudaMemsetAsync(s1, 0, C * sizeof(int64_t), st));
   Buf<uint32_t> chain(ctx, m);
   {
-    k_flag_nonneg<<<gm, 256, 0, st>>>(ncl, m, flag);
+    k_flag_nonneg<<<gm, 256, 0, st>>>(ncl, m, flag); ctx->launches++;
     HDB_CHECK_LAUNCH();
     scan_exclusive_i32_i64(ctx, flag, pos, m, pos.get() + m);
     HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     ctx->sync();
     const int64_t nv = hp[0];
     Buf<uint64_t> ckeys(ctx, nv);
-    k_chain_keys<<<gm, 256, 0, st>>>(m, n, ncl, d0, pos, ckeys, chain);
+    k_chain_keys<<<gm, 256, 0, st>>>(m, n, ncl, d0, pos, ckeys, chain); ctx->launches++;
     HDB_CHECK_LAUNCH();
     radix_sort_u64(ctx, ckeys, chain, nv, 0, 32 + bits_for(C));
-    k_seg_bounds<<<grid_for(ctx, nv, 256), 256, 0, st>>>(ckeys, nv, s0, s1);
+    k_seg_bounds<<<grid_for(ctx, nv, 256), 256, 0, st>>>(ckeys, nv, s0, s1); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   const int gc = grid_for(ctx, C, 128);
-  k_stability<<<gc, 128, 0, st>>>(t, C, s0, s1, chain, kind, lam, birth, stab, stab64);
+  k_stability<<<gc, 128, 0, st>>>(t, C, s0, s1, chain, kind, lam, birth, stab, stab64); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   // excess of mass
   const int fp64 = stab_mode == HDB_STAB_FP64;
-  k_eom<<<gc, 128, 0, st>>>(C, ckid0, cparent, stab, stab64, fp64, sub, sub64, self_sel, arrive);
+  k_eom<<<gc, 128, 0, st>>>(C, ckid0, cparent, stab, stab64, fp64, sub, sub64, self_sel, arrive); ctx->launches++;
   HDB_CHECK_LAUNCH();
   Buf<int32_t> cj(ctx, C), cj2(ctx, C), sel(ctx, C), cover(ctx, C), cover2(ctx, C);
   Buf<int8_t> anc(ctx, C), anc2(ctx, C);
-  k_sel_init<<<gc, 128, 0, st>>>(C, cparent, self_sel, cj, anc);
+  k_sel_init<<<gc, 128, 0, st>>>(C, cparent, self_sel, cj, anc); ctx->launches++;
   HDB_CHECK_LAUNCH();
   {
     int32_t *ja = cj, *jb = cj2;
     int8_t *aa = anc, *ab = anc2;
     for (int it = 0; it < 64; it++) {
       HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
-      k_sel_jump<<<gc, 128, 0, st>>>(C, ja, aa, jb, ab, changed);
+      k_sel_jump<<<gc, 128, 0, st>>>(C, ja, aa, jb, ab, changed); ctx->launches++;
       HDB_CHECK_LAUNCH();
       HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
       ctx->sync();
@@ -778,20 +778,20 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
       std::swap(aa, ab);
       if (!hflag[0]) break;
     }
-    k_selected<<<gc, 128, 0, st>>>(C, self_sel, aa, sel);
+    k_selected<<<gc, 128, 0, st>>>(C, self_sel, aa, sel); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   Buf<int32_t> selpos(ctx, C + 1), label_of(ctx, C);
   scan_exclusive_i32_i32(ctx, sel, selpos, C, selpos.get() + C);
-  k_label_map<<<gc, 128, 0, st>>>(C, sel, selpos, label_of);
-  k_cover_init<<<gc, 128, 0, st>>>(C, cparent, sel, cj, cover);
+  k_label_map<<<gc, 128, 0, st>>>(C, sel, selpos, label_of); ctx->launches++;
+  k_cover_init<<<gc, 128, 0, st>>>(C, cparent, sel, cj, cover); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int32_t *cov_final = cover;
   {
     int32_t *ja = cj, *jb = cj2, *ca = cover, *cb = cover2;
     for (int it = 0; it < 64; it++) {
       HDB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int32_t), st));
-      k_cover_jump<<<gc, 128, 0, st>>>(C, ja, ca, jb, cb, changed);
+      k_cover_jump<<<gc, 128, 0, st>>>(C, ja, ca, jb, cb, changed); ctx->launches++;
       HDB_CHECK_LAUNCH();
       HDB_CUDA(cudaMemcpyAsync(hflag, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
       ctx->sync();
@@ -810,7 +810,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     plam = Buf<float>(ctx, n);
   }
   k_points<<<gn, 256, 0, st>>>(t, par, ncl, lam, cov_final, birth, label_of, labels,
-                               condensed ? pcl.get() : nullptr, condensed ? plam.get() : nullptr);
+                               condensed ? pcl.get() : nullptr, condensed ? plam.get() : nullptr); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemcpyAsync(hflag, selpos.get() + C, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   if (condensed) {
@@ -819,15 +819,15 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     Buf<uint64_t> rkeys(ctx, rows);
     Buf<uint32_t> ridx(ctx, rows);
     k_condensed_rows<<<grid_for(ctx, rows, 256), 256, 0, st>>>(t, snodes, ns, ncl, lam, pcl, plam,
-                                                                tmp, rkeys, ridx);
+                                                                tmp, rkeys, ridx); ctx->launches++;
     HDB_CHECK_LAUNCH();
     radix_sort_u64(ctx, rkeys, ridx, rows, 0, 64);
-    k_permute_rows<<<grid_for(ctx, rows, 256), 256, 0, st>>>(tmp, ridx, rows, condensed);
+    k_permute_rows<<<grid_for(ctx, rows, 256), 256, 0, st>>>(tmp, ridx, rows, condensed); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (condensed_size) *condensed_size = rows;
   }
   if (stability) {
-    k_stab_out<<<gc, 128, 0, st>>>(C, n, stab, stability);
+    k_stab_out<<<gc, 128, 0, st>>>(C, n, stab, stability); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   if (num_stability) *num_stability = C;

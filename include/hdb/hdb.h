@@ -99,6 +99,12 @@ typedef struct {
   int32_t mst_rounds;     /* Boruvka rounds */
   int64_t knn_dropped;    /* NN-Descent candidates lost to a full inbox (normally 0) */
   float ms_knn, ms_graph, ms_mst, ms_tree, ms_total; /* device time per stage */
+  /* NN-Descent local join, measured with CUDA events around each launch */
+  float join_ms;                /* summed over the join launches */
+  int32_t join_launches;
+  int64_t join_rows_gathered;   /* sampled rows staged in shared memory, all launches */
+  int64_t join_candidates;      /* candidates that passed the k-th distance filter */
+  int64_t gpu_launches;         /* kernel launches issued by the call */
 } hdb_run_stats;
 
 typedef struct hdb_ctx hdb_ctx;
@@ -170,6 +176,15 @@ HDB_API hdb_status hdb_condense_select(hdb_ctx *ctx, const hdb_linkage_node *hie
  * the copies run inside the call. */
 HDB_API hdb_status hdb_run(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
                            const hdb_params *params, int32_t *labels, hdb_run_stats *stats);
+
+/* The stages after the kNN graph in the HDBSCAN/_new.cu:196-347 order, which
+ * reads a finished .kgraph (ReadBinaryVecs, _new.cu:199) instead of building
+ * it: G [n, params->knn.k] NNDElement rows (flags allowed), X [n, d] ->
+ * labels [n].  params->knn.sample_num / iterations / precision are ignored.
+ * With params->host_io = 1, G, X and labels are host pointers. */
+HDB_API hdb_status hdb_run_knn(hdb_ctx *ctx, const hdb_nnd_element *G, const float *X, int64_t n,
+                               int32_t d, const hdb_params *params, int32_t *labels,
+                               hdb_run_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -45,29 +45,52 @@ def test_nndescent_recall_matches_reference_algorithm(ctx, oracle, n, d, k):
 
 
 @pytest.mark.parametrize("distance", ["sqrt", "squared"])
-def test_pipeline_labels_identical_on_shared_graph(ctx, oracle, distance):
-    """hdb_run's labels equal the oracle's labels computed from the kNN graph
-    the GPU built (bit-identical labels on the shared graph)."""
-    from gpu_hdbscan_b200 import HDB_DIST_SQRT, HDB_DIST_SQUARED
+@pytest.mark.parametrize("stab", ["fp32", "fp64"])
+def test_pipeline_labels_identical_on_shared_graph(ctx, oracle, distance, stab):
+    """Labels of the path after the kNN graph (hdb_run_knn, the HDBSCAN/_new.cu
+    flow from a finished graph) equal the oracle's on the same GPU-built graph."""
+    from gpu_hdbscan_b200 import HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_STAB_FP32, HDB_STAB_FP64
     X = blobs(6000, 12, seed=21, blobs=8)
     mode = HDB_DIST_SQRT if distance == "sqrt" else HDB_DIST_SQUARED
-    labels, stats = ctx.hdbscan(X, k=32, mpts=32, distance=mode)
+    sm = HDB_STAB_FP32 if stab == "fp32" else HDB_STAB_FP64
     G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6)
+    labels, stats = ctx.hdbscan_from_knn(G, X, k=32, mpts=32, distance=mode, stability=sm)
     ids, dist = (_t(a) for a in ctx.knn_split(G))
     if distance == "sqrt":
         dist = oracle.fix_distances(X, ids)
-    _, ref_labels, ncl = oracle.hdbscan_from_knn(ids, dist, X, 32)
-    np.testing.assert_array_equal(_t(labels) if hasattr(labels, "cpu") else labels, ref_labels)
+    _, ref_labels, ncl = oracle.hdbscan_from_knn(ids, dist, X, 32, fp64=(stab == "fp64"))
+    np.testing.assert_array_equal(_t(labels), ref_labels)
     assert stats["num_clusters"] == ncl
     assert ncl >= 2
+
+
+def test_full_run_labels_are_consistent_with_its_own_graph_quality(ctx, oracle):
+    """hdb_run end to end: clusters found on well separated blobs agree with
+    the generating blobs (ARI) -- the kNN graph inside is not shared."""
+    from sklearn.metrics import adjusted_rand_score
+    rng = np.random.default_rng(4)
+    centers = rng.uniform(-20, 20, size=(6, 12))
+    lab = rng.integers(0, 6, 8000)
+    X = (centers[lab] + rng.normal(size=(8000, 12))).astype(np.float32)
+    labels, stats = ctx.hdbscan(X, k=32, mpts=32)
+    got = labels.numpy()
+    assert stats["num_clusters"] == 6
+    keep = got >= 0
+    assert keep.mean() > 0.8
+    assert adjusted_rand_score(lab[keep], got[keep]) > 0.99
 
 
 def test_pipeline_device_and_host_io_agree(ctx):
     import torch
     X = blobs(4000, 12, seed=3)
-    lh, _ = ctx.hdbscan(X)
-    ld, _ = ctx.hdbscan(torch.from_numpy(X).cuda())
+    Xd = torch.from_numpy(X).cuda()
+    G = ctx.NNDescent(Xd, k=32, sample_num=16)
+    ld, _ = ctx.hdbscan_from_knn(G, Xd)
+    lh, _ = ctx.hdbscan_from_knn(G.cpu(), X)
+    assert not lh.is_cuda
     np.testing.assert_array_equal(lh.numpy(), _t(ld))
+    lr, st = ctx.hdbscan(X)  # full path with host buffers
+    assert not lr.is_cuda and lr.shape == (4000,) and st["num_clusters"] >= 1
 
 
 def test_invalid_knn_graphs_are_rejected(ctx):
@@ -110,22 +133,24 @@ def test_disconnected_graph_is_reported(ctx):
 
 
 def test_small_and_edge_sizes(ctx, oracle):
-    # n just above k, and mpts larger than every cluster (all noise)
-    for n, k, mpts in [(40, 32, 32), (100, 8, 64 if False else 8), (33, 32, 2)]:
+    """n just above k, k < 32, and mpts = 2."""
+    for n, k, mpts in [(40, 32, 32), (100, 8, 8), (33, 32, 2), (500, 16, 16)]:
         X = blobs(n, 3, seed=n)
-        labels, stats = ctx.hdbscan(X, k=k, mpts=min(mpts, k), sample_num=k // 2)
         G = ctx.NNDescent(X, k=k, sample_num=k // 2)
+        labels, _ = ctx.hdbscan_from_knn(G, X, k=k, mpts=mpts)
         ids = _t(ctx.knn_split(G)[0])
         fd = oracle.fix_distances(X, ids)
-        _, ref, _ = oracle.hdbscan_from_knn(ids, fd, X, min(mpts, k))
-        np.testing.assert_array_equal(labels.numpy(), ref)
+        _, ref, _ = oracle.hdbscan_from_knn(ids, fd, X, mpts)
+        np.testing.assert_array_equal(_t(labels), ref)
+        lab2, _ = ctx.hdbscan(X, k=k, mpts=mpts, sample_num=k // 2)
+        assert lab2.shape == (n,)
 
 
 def test_argument_errors(ctx):
     from gpu_hdbscan_b200 import HdbError
     X = blobs(500, 4, seed=1)
     with pytest.raises(HdbError, match="mpts"):
-        ctx.hdbscan(X, k=16, mpts=1)
+        ctx.hdbscan(X, k=16, mpts=1, sample_num=8)
     with pytest.raises(HdbError, match="SAMPLE_NUM"):
         ctx.hdbscan(X, k=16, sample_num=9)
     with pytest.raises(HdbError, match="k"):
