@@ -152,6 +152,10 @@ void radix_sort_u32(Context *ctx, uint32_t *keys, uint32_t *values, int64_t n, i
 void radix_sort_u64(Context *ctx, uint64_t *keys, uint32_t *values, int64_t n, int begin_bit,
                     int end_bit);
 
+void radix_sort_u32_buffers(cudaStream_t st, uint32_t *keys, uint32_t *vals, uint32_t *ktmp,
+                            uint32_t *vtmp, uint32_t *counts, uint32_t *offs, uint32_t *scan_sums,
+                            uint32_t *scan_offs, int64_t n, int begin_bit, int end_bit);
+
 // Fixed-point grid sizing: a multiple of the SM count, capped by the work.
 inline int grid_for(const Context *ctx, int64_t work, int per_block, int blocks_per_sm = 8) {
   int64_t need = (work + per_block - 1) / per_block;

@@ -258,4 +258,47 @@ void radix_sort_u64(Context *ctx, uint64_t *keys, uint32_t *values, int64_t n, i
   radix_sort_impl<uint64_t>(ctx, keys, values, n, begin_bit, end_bit);
 }
 
+// Stable LSD radix sort of u32 keys with u32 values in caller-provided
+// buffers (nothing is allocated): ktmp/vtmp hold n elements each, counts and
+// offs hold ceil(n / 2048) * 256 entries, scan_sums and scan_offs hold
+// ceil(counts / 2048) entries, and that count must itself fit one scan tile.
+// The result ends in keys/vals.  Used by the allocation-free entry point.
+void radix_sort_u32_buffers(cudaStream_t st, uint32_t *keys, uint32_t *vals, uint32_t *ktmp,
+                            uint32_t *vtmp, uint32_t *counts, uint32_t *offs, uint32_t *scan_sums,
+                            uint32_t *scan_offs, int64_t n, int begin_bit, int end_bit) {
+  if (n <= 1 || end_bit <= begin_bit) return;
+  const uint32_t nb = (uint32_t)ceil_div(n, kSortTile);
+  const int64_t nc = (int64_t)nb * 256;
+  const int64_t ns = ceil_div(nc, kScanTile);
+  HDB_REQUIRE(ns <= kScanTile, HDB_ERR_ARG, "radix sort buffers: too many elements");
+  uint32_t *kin = keys, *kout = ktmp, *vin = vals, *vout = vtmp;
+  int passes = 0;
+  for (int shift = begin_bit; shift < end_bit; shift += 8, passes++) {
+    radix_hist<uint32_t><<<nb, kSortThreads, 0, st>>>(kin, counts, n, shift, nb);
+    HDB_CHECK_LAUNCH();
+    if (ns == 1) {
+      scan_tile_apply<uint32_t, uint32_t><<<1, kScanThreads, 0, st>>>(counts, offs, nullptr, nc,
+                                                                      nullptr);
+    } else {
+      scan_tile_sums<uint32_t, uint32_t><<<(unsigned)ns, kScanThreads, 0, st>>>(counts, scan_sums,
+                                                                                nc);
+      scan_tile_apply<uint32_t, uint32_t><<<1, kScanThreads, 0, st>>>(scan_sums, scan_offs, nullptr,
+                                                                      ns, nullptr);
+      scan_tile_apply<uint32_t, uint32_t><<<(unsigned)ns, kScanThreads, 0, st>>>(counts, offs,
+                                                                                 scan_offs, nc,
+                                                                                 nullptr);
+    }
+    HDB_CHECK_LAUNCH();
+    radix_scatter<uint32_t, true><<<nb, kSortThreads, 0, st>>>(kin, vin, kout, vout, offs, n,
+                                                               shift, nb);
+    HDB_CHECK_LAUNCH();
+    uint32_t *t = kin; kin = kout; kout = t;
+    t = vin; vin = vout; vout = t;
+  }
+  if (passes & 1) {
+    HDB_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    HDB_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  }
+}
+
 }  // namespace hdb

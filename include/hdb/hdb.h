@@ -186,6 +186,21 @@ HDB_API hdb_status hdb_run_knn(hdb_ctx *ctx, const hdb_nnd_element *G, const flo
                                int32_t d, const hdb_params *params, int32_t *labels,
                                hdb_run_stats *stats);
 
+/* hdb_sort_edges_noalloc -- no counterpart in the reference.  The same
+ * stable ascending sort by weight as hdb_sort_edges, for callers that cannot
+ * call cudaMalloc (a host framework that owns every device byte, or a device
+ * that is already full): it allocates nothing and needs no context.  Its
+ * working memory is a fixed ~7.3 MB static device array inside the library,
+ * which every GPU that loads libhdb_b200.so keeps until the process exits, so
+ * m may be at most 262144 edges (HDB_ERR_ARG above that).  `edges` is device
+ * memory; work runs on `stream` (NULL = legacy default stream) of the current
+ * device and the call returns when it is done.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the one array: calls whose
+ * work overlaps on the GPU (for instance from different streams or threads)
+ * race and corrupt each other's result. */
+HDB_API hdb_status hdb_sort_edges_noalloc(hdb_mst_edge *edges, int64_t m, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
