@@ -125,26 +125,26 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
 // keys and labels.
 constexpr int kMergeSmemU64 = kMergeSlots + kMaxK + kMaxK / 2;
 
-// Merge of a row's inbox into its sorted list (one warp).  On return, lane j
-// (< k) holds the j-th entry of the merged row: flagged label and distance.
-// Candidates of one pair always carry the same distance, so duplicates are
-// adjacent after the sort.
-__device__ __forceinline__ void merge_inbox(int64_t row, int k, int32_t &lab, float &dist,
-                                            int32_t *__restrict__ inbox_cnt,
-                                            const uint64_t *__restrict__ inbox,
-                                            unsigned long long *__restrict__ ovf, uint64_t *sk) {
+// Where the join leaves its candidates: a fixed inbox per row, then a global
+// overflow list (radix-sorted by target row between the join and the merge).
+// Only when the overflow list is full is a candidate dropped; the best
+// dropped one per row is still kept in `best`.
+struct Inbox {
+  int32_t *cnt;                  // [n] candidates offered this iteration
+  uint64_t *slots;               // [n * kInboxCap] packed (distance, id)
+  unsigned long long *best;      // [n]
+  uint32_t *ovf_tgt;             // [ovf_cap] overflow: target row (sorted in place)
+  uint64_t *ovf_key;             // [ovf_cap] overflow: packed candidate
+  uint32_t *ovf_idx;             // [ovf_cap] overflow: permutation from the sort
+  uint32_t *ostart, *oend;       // [n] segment of each row in the sorted overflow list
+  unsigned long long *counters;  // [0] dropped [1] rows gathered [2] candidates [3] overflow
+  int64_t ovf_cap;
+};
+
+// Sorts the 128 candidates in sk, drops duplicates and ids already in the
+// row, and merges the rest into the row held one entry per lane (lane < k).
+__device__ __forceinline__ void merge_chunk(int k, int32_t &lab, float &dist, uint64_t *sk) {
   const int lane = lane_id();
-  int cnt = inbox_cnt[row];
-  const uint64_t ov = ovf[row];
-  if (cnt == 0 && ov == ~0ull) return;
-  if (cnt > kInboxCap) cnt = kInboxCap;
-  __syncwarp();
-  if (lane == 0) {
-    inbox_cnt[row] = 0;
-    if (ov != ~0ull) ovf[row] = ~0ull;
-  }
-  for (int i = lane; i < kMergeSlots; i += 32)
-    sk[i] = i < cnt ? inbox[row * kInboxCap + i] : (i == kInboxCap ? ov : ~0ull);
   __syncwarp();
   warp_sort_smem128(sk);
   const bool have = lane < k;
@@ -207,12 +207,39 @@ __device__ __forceinline__ void merge_inbox(int64_t row, int k, int32_t &lab, fl
   __syncwarp();
 }
 
+// Merge of everything offered to a row (inbox, overflow segment, best
+// dropped) into its sorted list (one warp).  On return, lane j (< k) holds the
+// j-th entry of the merged row.  Candidates of one pair always carry the same
+// distance, so duplicates are adjacent after each sort.
+__device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, float &dist,
+                                          const Inbox &ib, uint64_t *sk) {
+  const int lane = lane_id();
+  int cnt = ib.cnt[row];
+  const uint64_t ov = ib.best[row];
+  const uint32_t o0 = ib.ostart[row], o1 = ib.oend[row];
+  if (cnt == 0 && ov == ~0ull && o0 == o1) return;
+  if (cnt > kInboxCap) cnt = kInboxCap;
+  __syncwarp();
+  if (lane == 0) {
+    ib.cnt[row] = 0;
+    if (ov != ~0ull) ib.best[row] = ~0ull;
+    if (o0 != o1) { ib.ostart[row] = 0; ib.oend[row] = 0; }
+  }
+  for (int i = lane; i < kMergeSlots; i += 32)
+    sk[i] = i < cnt ? ib.slots[row * kInboxCap + i] : (i == kInboxCap ? ov : ~0ull);
+  merge_chunk(k, lab, dist, sk);
+  for (uint32_t base = o0; base < o1; base += kMergeSlots) {
+    for (int i = lane; i < kMergeSlots; i += 32)
+      sk[i] = base + i < o1 ? ib.ovf_key[ib.ovf_idx[base + i]] : ~0ull;
+    merge_chunk(k, lab, dist, sk);
+  }
+}
+
 // Merge (iterations >= 1), sample (PrepareGraph :44-98 and reverse samples
 // PrepareReverseGraph :293-346) and MarkAllToOld (:1398), one warp per row.
 __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restrict__ gid,
-                         float *__restrict__ gdist, float *__restrict__ worst,
-                         int32_t *__restrict__ inbox_cnt, const uint64_t *__restrict__ inbox,
-                         unsigned long long *__restrict__ ovf, int32_t *__restrict__ newS,
+                         float *__restrict__ gdist, float *__restrict__ worst, Inbox ib,
+                         int32_t *__restrict__ newS,
                          int32_t *__restrict__ oldS, int8_t *__restrict__ nf, int8_t *__restrict__ of,
                          int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
   extern __shared__ uint64_t smem_sample[];
@@ -224,7 +251,7 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    if (do_merge) merge_inbox(row, k, lab, dist, inbox_cnt, inbox, ovf, sk);
+    if (do_merge) merge_row(row, k, lab, dist, ib, sk);
     const bool isnew = have && lab >= 0;
     const bool isold = have && lab < 0;
     const int32_t id = decode(lab);
@@ -256,8 +283,7 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
 
 // Final merge after the last join; writes NNDElement rows with their flags.
 __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
-                           const float *__restrict__ gdist, int32_t *__restrict__ inbox_cnt,
-                           const uint64_t *__restrict__ inbox, unsigned long long *__restrict__ ovf,
+                           const float *__restrict__ gdist, Inbox ib,
                            hdb_nnd_element *__restrict__ out) {
   extern __shared__ uint64_t smem_fin[];
   const int lane = lane_id();
@@ -268,7 +294,7 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    merge_inbox(row, k, lab, dist, inbox_cnt, inbox, ovf, sk);
+    merge_row(row, k, lab, dist, ib, sk);
     if (have) {
       hdb_nnd_element e;
       e.distance_ = dist;
@@ -286,19 +312,21 @@ struct JoinSmem {
 };
 
 __device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
-                                               const float *__restrict__ worst,
-                                               int32_t *__restrict__ inbox_cnt,
-                                               uint64_t *__restrict__ inbox,
-                                               unsigned long long *__restrict__ ovf,
-                                               unsigned long long *__restrict__ dropped) {
+                                              const float *__restrict__ worst, const Inbox &ib) {
   if (!(d < worst[target])) return 0;  // cannot enter the target's list
-  int slot = atomicAdd(&inbox_cnt[target], 1);
+  int slot = atomicAdd(&ib.cnt[target], 1);
   uint64_t key = pack(d, id);
   if (slot < kInboxCap) {
-    inbox[(int64_t)target * kInboxCap + slot] = key;
+    ib.slots[(int64_t)target * kInboxCap + slot] = key;
   } else {
-    atomicMin(&ovf[target], (unsigned long long)key);
-    atomicAdd(dropped, 1ull);
+    unsigned long long pos = atomicAdd(&ib.counters[3], 1ull);
+    if ((int64_t)pos < ib.ovf_cap) {
+      ib.ovf_tgt[pos] = (uint32_t)target;
+      ib.ovf_key[pos] = key;
+    } else {
+      atomicMin(&ib.best[target], (unsigned long long)key);
+      atomicAdd(&ib.counters[0], 1ull);
+    }
   }
   return 1;
 }
@@ -308,10 +336,7 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
                        const int32_t *__restrict__ newS, const int32_t *__restrict__ oldS,
                        const int8_t *__restrict__ nf, const int8_t *__restrict__ of,
                        int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
-                       const float *__restrict__ worst, int32_t *__restrict__ inbox_cnt,
-                       uint64_t *__restrict__ inbox, unsigned long long *__restrict__ ovf,
-                       unsigned long long *__restrict__ dropped,
-                       unsigned long long *__restrict__ jstats) {
+                       const float *__restrict__ worst, Inbox ib) {
   extern __shared__ float smem_join[];
   __shared__ unsigned long long blk_rows, blk_cands;
   if (threadIdx.x == 0) { blk_rows = 0; blk_cands = 0; }
@@ -395,11 +420,9 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
       const int32_t x = ids[lane];
       int pushed = 0;
       if (best1 != ~0ull)
-        pushed += push_candidate(x, pk_id(best1), pk_dist(best1), worst, inbox_cnt, inbox, ovf,
-                                 dropped);
+        pushed += push_candidate(x, pk_id(best1), pk_dist(best1), worst, ib);
       if (best2 != ~0ull)
-        pushed += push_candidate(x, pk_id(best2), pk_dist(best2), worst, inbox_cnt, inbox, ovf,
-                                 dropped);
+        pushed += push_candidate(x, pk_id(best2), pk_dist(best2), worst, ib);
       if (pushed) atomicAdd(&blk_cands, (unsigned long long)pushed);
     }
     if (lane < no) {
@@ -409,16 +432,15 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
         best = c < best ? c : best;
       }
       if (best != ~0ull &&
-          push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, inbox_cnt, inbox, ovf,
-                         dropped))
+          push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, ib))
         atomicAdd(&blk_cands, 1ull);
     }
     __syncwarp();
   }
   __syncthreads();
-  if (threadIdx.x == 0 && jstats) {
-    atomicAdd(&jstats[0], blk_rows);
-    atomicAdd(&jstats[1], blk_cands);
+  if (threadIdx.x == 0) {
+    atomicAdd(&ib.counters[1], blk_rows);
+    atomicAdd(&ib.counters[2], blk_cands);
   }
 }
 
@@ -453,7 +475,48 @@ __global__ void k_fix_distances(const float *__restrict__ X, int64_t n, int d,
   }
 }
 
+__global__ void k_iota_u32(uint32_t *__restrict__ v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+
+// Segment [ostart, oend) of every target row in the target-sorted overflow list.
+__global__ void k_ovf_bounds(const uint32_t *__restrict__ tgt, int64_t cnt, uint32_t *__restrict__ ostart,
+                             uint32_t *__restrict__ oend) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t t = tgt[i];
+    if (i == 0 || tgt[i - 1] != t) ostart[t] = (uint32_t)i;
+    if (i == cnt - 1 || tgt[i + 1] != t) oend[t] = (uint32_t)(i + 1);
+  }
+}
+
+int bits_for_rows(int64_t n) {
+  int b = 1;
+  while (b < 40 && (int64_t(1) << b) < n) b++;
+  return b;
+}
+
 }  // namespace
+
+// Sorts the join's overflow list by target row and records each row's
+// segment for the next merge; resets the list.
+static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
+  cudaStream_t st = ctx->stream;
+  unsigned long long *h = reinterpret_cast<unsigned long long *>(ctx->pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, ib.counters + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  int64_t c = (int64_t)h[0];
+  if (c == 0) return;
+  if (c > ib.ovf_cap) c = ib.ovf_cap;
+  k_iota_u32<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_idx, c); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  radix_sort_u32(ctx, ib.ovf_tgt, ib.ovf_idx, c, 0, bits_for_rows(n));
+  k_ovf_bounds<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_tgt, c, ib.ostart, ib.oend); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  HDB_CUDA(cudaMemsetAsync(ib.counters + 3, 0, sizeof(unsigned long long), st));
+}
 
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js) {
@@ -474,6 +537,12 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   Buf<int8_t> nf(ctx, n), of(ctx, n);
   Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
+  const int64_t ovf_cap = n * 4 > (1 << 20) ? n * 4 : (1 << 20);
+  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ovf_idx(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
+  Buf<uint64_t> ovf_key(ctx, ovf_cap);
+  HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
+  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ovf_idx, ostart, oend, dropped, ovf_cap};
   HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
@@ -499,18 +568,18 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
   const int grid_join = grid_for(ctx, n, jw, 64);
   for (int it = 0; it < p.iterations; it++) {
-    k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst,
-                                                       inbox_cnt, inbox, ovf, newS, oldS, nf, of,
-                                                       nrev, orev); ctx->launches++;
+    k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
+                                                       newS, oldS, nf, of, nrev, orev); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
     k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
-                                                  inbox_cnt, inbox, ovf, dropped,
-                                                  dropped.get() + 1); ctx->launches++;
+                                                  ib); ctx->launches++;
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
     HDB_CHECK_LAUNCH();
+    sort_overflow(ctx, ib, n);
+    HDB_CHECK_LAUNCH();
   }
-  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, inbox_cnt, inbox, ovf, G); ctx->launches++;
+  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));

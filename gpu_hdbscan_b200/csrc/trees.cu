@@ -363,10 +363,113 @@ __global__ void k_chain_keys(int64_t m, int64_t n, const int32_t *__restrict__ n
   }
 }
 
+// Chain node data laid out in chain order, so the per-cluster sums stream
+// contiguous memory: lambda, and either (count of points falling out, 0) or,
+// for the split that ends the chain, (-size(left), size(right)).
+struct ChainItem {
+  float lam;
+  int32_t a, b;
+  int32_t pad;
+};
+
+__global__ void k_chain_items(TreeView t, const uint32_t *__restrict__ chain, int64_t cnt,
+                              const int8_t *__restrict__ kind, const float *__restrict__ lam,
+                              ChainItem *__restrict__ items) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = chain[i];
+    const hdb_linkage_node h = t.h[r];
+    const int8_t kd = kind[r];
+    ChainItem it;
+    it.lam = lam[r];
+    it.pad = 0;
+    if (kd == KIND_SPLIT) {
+      it.a = -t.sz(h.left_node);
+      it.b = t.sz(h.right_node);
+    } else {
+      it.a = kd == KIND_LEFTBIG ? t.sz(h.right_node)
+             : kd == KIND_RIGHTBIG ? t.sz(h.left_node)
+                                   : t.sz(h.left_node) + t.sz(h.right_node);
+      it.b = 0;
+    }
+    items[i] = it;
+  }
+}
+
+template <typename T> struct FpBits;
+template <> struct FpBits<float> {
+  static constexpr int kMant = 23;
+  __device__ static int exp_field(float x) { return (__float_as_uint(x) >> 23) & 0xff; }
+  __device__ static float pow2(int e) { return __uint_as_float((uint32_t)(e + 127) << 23); }
+  __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+  __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+  __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+  static constexpr int kBias = 127;
+};
+template <> struct FpBits<double> {
+  static constexpr int kMant = 52;
+  __device__ static int exp_field(double x) {
+    return (int)((__double_as_longlong(x) >> 52) & 0x7ff);
+  }
+  __device__ static double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+  __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+  __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+  __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+  static constexpr int kBias = 1023;
+};
+
+// s after `cnt` sequential round-to-nearest-even additions of v >= 0 --
+// exactly what one row per point gives (compute_stability, tree.cu:504-512).
+// Inside one binade of s the additions advance s by a fixed multiple of its
+// ulp; with v an odd multiple of half an ulp (a tie) the first step may differ
+// and every later one is equal.  So: take single steps until two consecutive
+// increments inside one binade agree (and v < s, which keeps s1 - s exact),
+// then jump to the last step that stays in the binade.
+template <typename T>
+__device__ T add_repeated(T s, T v, int64_t cnt) {
+  using B = FpBits<T>;
+  if (!(v > T(0))) {
+    for (; cnt > 0; cnt--) s = B::add(s, v);
+    return s;
+  }
+  T last_inc = T(-1);
+  int last_exp = -1;
+  while (cnt > 0) {
+    const T s1 = B::add(s, v);
+    cnt--;
+    const int e0 = B::exp_field(s), e1 = B::exp_field(s1);
+    if (!(v < s) || e0 == 0 || e0 != e1) {  // large step, subnormal, or binade change
+      s = s1;
+      last_inc = T(-1);
+      continue;
+    }
+    const T inc = B::sub(s1, s);  // exact: s <= s1 <= 2s
+    s = s1;
+    if (inc == T(0)) return s;  // v under half an ulp: s stays put from now on
+    if (inc == last_inc && e1 == last_exp && cnt > 0) {
+      // steady: s advances by inc = dq ulps per step while it stays in binade e1
+      const T u = B::pow2(e1 - B::kBias - B::kMant);
+      const int64_t q = (int64_t)B::mul(s, B::pow2(B::kMant - (e1 - B::kBias)));  // s / u
+      const int64_t dq = (int64_t)B::mul(inc, B::pow2(B::kMant - (e1 - B::kBias)));
+      const int64_t qmax = (int64_t(1) << (B::kMant + 1)) - 1;
+      int64_t t = (qmax - q) / dq;
+      if (t > cnt) t = cnt;
+      if (t > 0) {
+        s = B::mul((T)(q + t * dq), u);  // exact: integer significand times a power of two
+        cnt -= t;
+      }
+      last_inc = T(-1);
+      continue;
+    }
+    last_inc = inc;
+    last_exp = e1;
+  }
+  return s;
+}
+
 // One thread per cluster: stability in the reference's row order.
-__global__ void k_stability(TreeView t, int64_t C, const int64_t *__restrict__ seg_start,
-                            const int64_t *__restrict__ seg_end, const uint32_t *__restrict__ chain,
-                            const int8_t *__restrict__ kind, const float *__restrict__ lam,
+__global__ void k_stability(int64_t C, const int64_t *__restrict__ seg_start,
+                            const int64_t *__restrict__ seg_end, const ChainItem *__restrict__ items,
                             const float *__restrict__ birth, float *__restrict__ stab,
                             double *__restrict__ stab64) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
@@ -375,25 +478,17 @@ __global__ void k_stability(TreeView t, int64_t C, const int64_t *__restrict__ s
     float s = 0.0f;
     double s64 = 0.0;
     for (int64_t i = seg_start[c]; i < seg_end[c]; i++) {
-      const uint32_t r = chain[i];
-      const hdb_linkage_node h = t.h[r];
-      const float v = __fsub_rn(lam[r], b);
-      const double v64 = __dsub_rn((double)lam[r], (double)b);
-      const int8_t kd = kind[r];
-      if (kd == KIND_SPLIT) {
-        int32_t sl = t.sz(h.left_node), sr = t.sz(h.right_node);
-        s = __fadd_rn(s, __fmul_rn(v, (float)sl));
-        s = __fadd_rn(s, __fmul_rn(v, (float)sr));
-        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)sl));
-        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)sr));
-      } else {
-        int64_t cnt = kd == KIND_LEFTBIG ? t.sz(h.right_node)
-                      : kd == KIND_RIGHTBIG ? t.sz(h.left_node)
-                                            : (int64_t)t.sz(h.left_node) + t.sz(h.right_node);
-        for (int64_t q = 0; q < cnt; q++) {  // one row per point, in row order
-          s = __fadd_rn(s, v);
-          s64 = __dadd_rn(s64, v64);
-        }
+      const ChainItem it = items[i];
+      const float v = __fsub_rn(it.lam, b);
+      const double v64 = __dsub_rn((double)it.lam, (double)b);
+      if (it.a < 0) {  // split rows: (lambda - birth) * child_size, left then right
+        s = __fadd_rn(s, __fmul_rn(v, (float)(-it.a)));
+        s = __fadd_rn(s, __fmul_rn(v, (float)it.b));
+        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)(-it.a)));
+        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)it.b));
+      } else {  // one row per point falling out here
+        s = add_repeated<float>(s, v, it.a);
+        s64 = add_repeated<double>(s64, v64, it.a);
       }
     }
     stab[c] = s;
@@ -739,6 +834,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   HDB_CUDA(cudaMemsetAsync(s0, 0, C * sizeof(int64_t), st));
   HDB_CUDA(cudaMemsetAsync(s1, 0, C * sizeof(int64_t), st));
   Buf<uint32_t> chain(ctx, m);
+  int64_t nv_total = 0;
   {
     k_flag_nonneg<<<gm, 256, 0, st>>>(ncl, m, flag); ctx->launches++;
     HDB_CHECK_LAUNCH();
@@ -746,6 +842,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     ctx->sync();
     const int64_t nv = hp[0];
+    nv_total = nv;
     Buf<uint64_t> ckeys(ctx, nv);
     k_chain_keys<<<gm, 256, 0, st>>>(m, n, ncl, d0, pos, ckeys, chain); ctx->launches++;
     HDB_CHECK_LAUNCH();
@@ -754,8 +851,13 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     HDB_CHECK_LAUNCH();
   }
   const int gc = grid_for(ctx, C, 128);
-  k_stability<<<gc, 128, 0, st>>>(t, C, s0, s1, chain, kind, lam, birth, stab, stab64); ctx->launches++;
-  HDB_CHECK_LAUNCH();
+  {
+    Buf<ChainItem> items(ctx, nv_total);
+    k_chain_items<<<grid_for(ctx, nv_total, 256), 256, 0, st>>>(t, chain, nv_total, kind, lam,
+                                                                items); ctx->launches++;
+    k_stability<<<gc, 32, 0, st>>>(C, s0, s1, items, birth, stab, stab64); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
 
   // excess of mass
   const int fp64 = stab_mode == HDB_STAB_FP64;

@@ -134,3 +134,29 @@ def test_fp64_stability_labels_match_oracle(ctx, oracle, case):
 def test_fix_distances_matches_reference_rounding(ctx, oracle, case):
     got = _t(ctx.fix_distances(case["X"], case["ids"]))
     np.testing.assert_array_equal(got.view(np.uint32), case["fdist"].view(np.uint32))
+
+
+@pytest.mark.parametrize("mpts", [2, 7, 300, 4000, 20000])
+def test_stability_with_long_runs_of_equal_rows(ctx, oracle, mpts):
+    """Large mpts makes whole subtrees fall out at one lambda, so one chain
+    node contributes thousands of equal rows; the FP32 sum must still equal the
+    reference's row-by-row sum bit for bit (and FP64 mode the oracle's)."""
+    import torch
+    n = 30000
+    X = blobs(n, 5, seed=77, blobs=12, noise=0.3)
+    ids, _ = oracle.nndescent(X, 16, 8, 4)
+    fd = oracle.fix_distances(X, ids)
+    nindex, nlist, ew, _ = oracle.enhanced_knng(ids, fd, X)
+    mst = oracle.sort_edges(oracle.build_mst(nindex, nlist, ew, oracle.kruskal(nindex, nlist, ew)))
+    hier = oracle.linkage_tree(mst, n)
+    cond = oracle.condensed_tree(hier, n, mpts)
+    stab, s64 = oracle.stability(cond)
+    h = torch.from_numpy(hier.view(np.int32).reshape(-1, 4).copy()).cuda()
+    from gpu_hdbscan_b200 import HDB_STAB_FP64
+    for mode, ref in ((0, None), (HDB_STAB_FP64, s64)):
+        labels, ncl, _, gstab = ctx.get_clusters(h, n, mpts, stability=mode, want_tree=True)
+        gs = _t(gstab).copy().view(oracle.STABILITY).reshape(-1)
+        np.testing.assert_array_equal(gs["lambda"].view(np.uint32), stab["lambda"].view(np.uint32))
+        rl, rn = oracle.get_clusters(cond, stab, n, ref)
+        assert ncl == rn
+        np.testing.assert_array_equal(_t(labels), rl)
