@@ -71,17 +71,17 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
   return v;
 }
 
-// Ascending bitonic sort of kMergeSlots u64 in shared memory by one warp.
-__device__ __forceinline__ void warp_sort_smem128(uint64_t *s) {
+// Ascending bitonic sort of the first `size` (32, 64 or 128) u64 of s in
+// shared memory by one warp.
+__device__ __forceinline__ void warp_sort_smem(uint64_t *s, int size) {
   const int lane = lane_id();
-  for (int size = 2; size <= kMergeSlots; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-#pragma unroll
-      for (int q = 0; q < kMergeSlots / 64; q++) {
-        int t = lane + 32 * q;                       // pair index 0..63
+  const int pairs = size >> 1;
+  for (int sz = 2; sz <= size; sz <<= 1) {
+    for (int stride = sz >> 1; stride > 0; stride >>= 1) {
+      for (int t = lane; t < pairs; t += 32) {
         int i = (t / stride) * (2 * stride) + (t % stride);
         int j = i + stride;
-        bool up = (i & size) == 0;
+        bool up = (i & sz) == 0;
         uint64_t a = s[i], b = s[j];
         if ((a > b) == up) { s[i] = b; s[j] = a; }
       }
@@ -143,10 +143,11 @@ struct Inbox {
 
 // Sorts the 128 candidates in sk, drops duplicates and ids already in the
 // row, and merges the rest into the row held one entry per lane (lane < k).
-__device__ __forceinline__ void merge_chunk(int k, int32_t &lab, float &dist, uint64_t *sk) {
+__device__ __forceinline__ void merge_chunk(int k, int32_t &lab, float &dist, uint64_t *sk,
+                                            int size) {
   const int lane = lane_id();
   __syncwarp();
-  warp_sort_smem128(sk);
+  warp_sort_smem(sk, size);
   const bool have = lane < k;
   const uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
   const int32_t rid = have ? decode(lab) : -1;
@@ -155,8 +156,8 @@ __device__ __forceinline__ void merge_chunk(int k, int32_t &lab, float &dist, ui
 #pragma unroll
   for (int q = 0; q < kMergeSlots / 32; q++) {
     int i = lane + 32 * q;
-    c[q] = sk[i];
-    uint64_t prev = i > 0 ? sk[i - 1] : ~0ull;
+    c[q] = i < size ? sk[i] : ~0ull;
+    uint64_t prev = (i > 0 && i < size) ? sk[i - 1] : ~0ull;
     ok[q] = c[q] != ~0ull && c[q] != prev;
   }
   for (int t = 0; t < k; t++) {
@@ -225,13 +226,17 @@ __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, floa
     if (ov != ~0ull) ib.best[row] = ~0ull;
     if (o0 != o1) { ib.ostart[row] = 0; ib.oend[row] = 0; }
   }
-  for (int i = lane; i < kMergeSlots; i += 32)
-    sk[i] = i < cnt ? ib.slots[row * kInboxCap + i] : (i == kInboxCap ? ov : ~0ull);
-  merge_chunk(k, lab, dist, sk);
+  {
+    const int used = cnt + (ov != ~0ull ? 1 : 0);
+    const int size = used <= 32 ? 32 : (used <= 64 ? 64 : kMergeSlots);
+    for (int i = lane; i < size; i += 32)
+      sk[i] = i < cnt ? ib.slots[row * kInboxCap + i] : (i == cnt && ov != ~0ull ? ov : ~0ull);
+    merge_chunk(k, lab, dist, sk, size);
+  }
   for (uint32_t base = o0; base < o1; base += kMergeSlots) {
     for (int i = lane; i < kMergeSlots; i += 32)
       sk[i] = base + i < o1 ? ib.ovf_key[ib.ovf_idx[base + i]] : ~0ull;
-    merge_chunk(k, lab, dist, sk);
+    merge_chunk(k, lab, dist, sk, kMergeSlots);
   }
 }
 
@@ -305,10 +310,11 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
 }
 
 struct JoinSmem {
-  // layout per warp: ids[64] | Dnn[32*33] | Dno[32*33] | X rows [64 * dp]
+  // layout per warp: best[96] (u64: best other-new, best old per new; best new
+  // per old) | ids[64] | X rows [64 * dp]
+  static constexpr int kBest = 96;  // u64 entries
   static constexpr int kIds = 64;
-  static constexpr int kMat = 32 * 33;
-  __host__ __device__ static int floats(int dp) { return kIds + 2 * kMat + 64 * dp; }
+  __host__ __device__ static int floats(int dp) { return 2 * kBest + kIds + 64 * dp + 2; }
 };
 
 __device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
@@ -331,24 +337,34 @@ __device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float 
   return 1;
 }
 
-// Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).
-__global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
+// Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).  The
+// sampled rows are staged in shared memory (new rows at slots 0..31, old rows
+// at 32..63).  The distance matrix new x (new U old) is cut into 4 x 4 tiles
+// spread over the lanes; a lane keeps its 16 sums in registers, so each
+// dimension costs 8 shared loads for 16 pair updates, and every pair is the
+// reference's sequential FP32 difference sum.  Tile row/column minima go to
+// the per-neighbour best candidates with one 64-bit shared-memory atomicMin
+// each: every new neighbour gets its closest other new one and its closest old
+// one, every old neighbour its closest new one.
+__device__ __forceinline__ const float *xs_row(const float *Xs, int r, int dp) {
+  return Xs + r * dp + (r >= 32 ? 1 : 0);  // old block shifted one bank
+}
+
+__global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64_t n, int d, int S,
                        const int32_t *__restrict__ newS, const int32_t *__restrict__ oldS,
                        const int8_t *__restrict__ nf, const int8_t *__restrict__ of,
                        int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
                        const float *__restrict__ worst, Inbox ib) {
   extern __shared__ float smem_join[];
-  __shared__ unsigned long long blk_rows, blk_cands;
-  if (threadIdx.x == 0) { blk_rows = 0; blk_cands = 0; }
-  __syncthreads();
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
   const int dp = (d & 1) ? d : d + 1;
   float *base = smem_join + (threadIdx.x >> 5) * JoinSmem::floats(dp);
-  int32_t *ids = reinterpret_cast<int32_t *>(base);
-  float *Dnn = base + JoinSmem::kIds;
-  float *Dno = Dnn + JoinSmem::kMat;
-  float *Xs = Dno + JoinSmem::kMat;
+  unsigned long long *best = reinterpret_cast<unsigned long long *>(base);
+  unsigned long long *best1 = best, *best2 = best + 32, *best3 = best + 64;
+  int32_t *ids = reinterpret_cast<int32_t *>(base + 2 * JoinSmem::kBest);
+  float *Xs = base + 2 * JoinSmem::kBest + JoinSmem::kIds;
+  unsigned long long w_rows = 0, w_cands = 0;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const int cnf = nf[row], cof = of[row];
@@ -366,81 +382,109 @@ __global__ void k_join(const float *__restrict__ X, int64_t n, int d, int S,
     vn = vn && (__ffs(pn) - 1 == lane);
     uint32_t po = __match_any_sync(0xffffffffu, oid);
     vo = vo && (__ffs(po) - 1 == lane);
+    uint32_t bo = __ballot_sync(0xffffffffu, vo);
+    const int no = __popc(bo);
+    if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
+    __syncwarp();
     // new \ old (:468-486)
-    for (int t = 0; t < 32; t++) {
-      int32_t o = __shfl_sync(0xffffffffu, oid, t);
-      bool ov = __shfl_sync(0xffffffffu, vo, t);
-      if (ov && o == nid) vn = false;
-    }
-    uint32_t bn = __ballot_sync(0xffffffffu, vn), bo = __ballot_sync(0xffffffffu, vo);
-    const int nn = __popc(bn), no = __popc(bo);
+    for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
+    uint32_t bn = __ballot_sync(0xffffffffu, vn);
+    const int nn = __popc(bn);
     if (vn) ids[__popc(bn & lanemask_lt())] = nid;
-    if (vo) ids[nn + __popc(bo & lanemask_lt())] = oid;
+    best1[lane] = ~0ull;
+    best2[lane] = ~0ull;
+    best3[lane] = ~0ull;
     __syncwarp();
-    const int T = nn + no;
-    if (nn == 0 || T < 2) continue;
-    if (lane == 0) atomicAdd(&blk_rows, (unsigned long long)T);
-    for (int idx = lane; idx < T * d; idx += 32) {
+    if (nn == 0 || nn + no < 2) continue;
+    w_rows += nn + no;
+    // stage rows
+    for (int idx = lane; idx < (nn + no) * d; idx += 32) {
       int r = idx / d, c = idx - r * d;
-      Xs[r * dp + c] = __ldg(X + (int64_t)ids[r] * d + c);
+      int slot = r < nn ? r : 32 + (r - nn);
+      float *dst = const_cast<float *>(xs_row(Xs, slot, dp));
+      dst[c] = __ldg(X + (int64_t)ids[slot] * d + c);
     }
     __syncwarp();
-    // new x new (upper triangle) and new x old distances
-    const int p1 = nn * (nn - 1) / 2, p2 = nn * no;
-    for (int p = lane; p < p1 + p2; p += 32) {
-      int a, b;
-      if (p < p1) {
-        // p -> (a, b), a < b, row-major over the upper triangle
-        a = 0;
-        int rem = p;
-        while (rem >= nn - 1 - a) { rem -= nn - 1 - a; a++; }
-        b = a + 1 + rem;
-        float dd = diffsum(Xs + a * dp, Xs + b * dp, d);
-        Dnn[a * 33 + b] = dd;
-        Dnn[b * 33 + a] = dd;
-      } else {
-        int q = p - p1;
-        a = q / no;
-        b = q - a * no;
-        Dno[a * 33 + b] = diffsum(Xs + a * dp, Xs + (nn + b) * dp, d);
+    const int rg = (nn + 3) >> 2;             // row groups (new rows)
+    const int cgn = rg, cgo = (no + 3) >> 2;  // column groups: new, old
+    const int cg = cgn + cgo;
+    const int tiles = rg * cg;
+    for (int t = lane; t < tiles; t += 32) {
+      const int r0 = (t / cg) * 4;
+      const int ci = t - (t / cg) * cg;
+      const bool oldcols = ci >= cgn;
+      const int c0 = oldcols ? 32 + (ci - cgn) * 4 : ci * 4;
+      const float *ra[4], *rc[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        ra[i] = xs_row(Xs, r0 + i, dp);
+        rc[i] = xs_row(Xs, c0 + i, dp);
       }
-    }
-    __syncwarp();
-    if (lane < nn) {
-      uint64_t best1 = ~0ull, best2 = ~0ull;
-      for (int b = 0; b < nn; b++)
-        if (b != lane) {
-          uint64_t c = pack(Dnn[lane * 33 + b], ids[b]);
-          best1 = c < best1 ? c : best1;
+      float acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+      for (int k2 = 0; k2 < d; k2++) {
+        float xa[4], xc[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) { xa[i] = ra[i][k2]; xc[i] = rc[i][k2]; }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            float df = __fsub_rn(xa[i], xc[j]);
+            acc[i][j] = __fmaf_rn(df, df, acc[i][j]);
+          }
+      }
+      const int ncol = oldcols ? no : nn;
+      const int cbase = oldcols ? c0 - 32 : c0;  // column index within its block
+      uint64_t colmin[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int a = r0 + i;
+        if (a >= nn) continue;
+        uint64_t rmin = ~0ull;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int c = cbase + j;
+          if (c >= ncol || (!oldcols && c == a)) continue;
+          const uint64_t kr = pack(acc[i][j], ids[c0 + j]);
+          rmin = kr < rmin ? kr : rmin;
+          if (oldcols) {
+            const uint64_t kc = pack(acc[i][j], ids[a]);
+            colmin[j] = kc < colmin[j] ? kc : colmin[j];
+          }
         }
-      for (int b = 0; b < no; b++) {
-        uint64_t c = pack(Dno[lane * 33 + b], ids[nn + b]);
-        best2 = c < best2 ? c : best2;
+        if (rmin != ~0ull) atomicMin(oldcols ? &best2[a] : &best1[a], (unsigned long long)rmin);
       }
+      if (oldcols) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (colmin[j] != ~0ull) atomicMin(&best3[cbase + j], (unsigned long long)colmin[j]);
+      }
+    }
+    __syncwarp();
+    int pushed = 0;
+    if (lane < nn) {
       const int32_t x = ids[lane];
-      int pushed = 0;
-      if (best1 != ~0ull)
-        pushed += push_candidate(x, pk_id(best1), pk_dist(best1), worst, ib);
-      if (best2 != ~0ull)
-        pushed += push_candidate(x, pk_id(best2), pk_dist(best2), worst, ib);
-      if (pushed) atomicAdd(&blk_cands, (unsigned long long)pushed);
+      const uint64_t b1 = best1[lane], b2 = best2[lane];
+      if (b1 != ~0ull) pushed += push_candidate(x, pk_id(b1), pk_dist(b1), worst, ib);
+      if (b2 != ~0ull) pushed += push_candidate(x, pk_id(b2), pk_dist(b2), worst, ib);
     }
     if (lane < no) {
-      uint64_t best = ~0ull;
-      for (int a = 0; a < nn; a++) {
-        uint64_t c = pack(Dno[a * 33 + lane], ids[a]);
-        best = c < best ? c : best;
-      }
-      if (best != ~0ull &&
-          push_candidate(ids[nn + lane], pk_id(best), pk_dist(best), worst, ib))
-        atomicAdd(&blk_cands, 1ull);
+      const uint64_t b3 = best3[lane];
+      if (b3 != ~0ull) pushed += push_candidate(ids[32 + lane], pk_id(b3), pk_dist(b3), worst, ib);
     }
+    w_cands += pushed;
     __syncwarp();
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    atomicAdd(&ib.counters[1], blk_rows);
-    atomicAdd(&ib.counters[2], blk_cands);
+  // per-warp totals, one atomic each (no block-wide barrier)
+#pragma unroll
+  for (int o = 16; o; o >>= 1) w_cands += __shfl_xor_sync(0xffffffffu, w_cands, o);
+  if (lane == 0) {
+    if (w_rows) atomicAdd(&ib.counters[1], w_rows);
+    if (w_cands) atomicAdd(&ib.counters[2], w_cands);
   }
 }
 
@@ -561,7 +605,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const size_t smem_sample = (size_t)wpb * kMergeSmemU64 * sizeof(uint64_t);
   const int dp = (d & 1) ? d : d + 1;
   const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
-  int jw = (int)((200 * 1024) / per_warp);
+  int jw = (int)((56 * 1024) / per_warp);  // about four blocks per SM
   jw = jw < 1 ? 1 : (jw > 8 ? 8 : jw);
   const size_t smem_join = per_warp * jw;
   HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "NN-Descent: d too large for the join tile");

@@ -467,32 +467,50 @@ __device__ T add_repeated(T s, T v, int64_t cnt) {
   return s;
 }
 
-// One thread per cluster: stability in the reference's row order.
+// One warp per cluster: stability in the reference's row order.  The warp
+// loads 32 chain items at a time (coalesced) and every lane replays the same
+// sequential sum from registers, so the serial chain walk never waits on a
+// dependent global load; lane 0 stores the result.
 __global__ void k_stability(int64_t C, const int64_t *__restrict__ seg_start,
                             const int64_t *__restrict__ seg_end, const ChainItem *__restrict__ items,
                             const float *__restrict__ birth, float *__restrict__ stab,
                             double *__restrict__ stab64) {
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
-       c += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  for (int64_t c = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); c < C;
+       c += (int64_t)gridDim.x * wpb) {
     const float b = birth[c];
     float s = 0.0f;
     double s64 = 0.0;
-    for (int64_t i = seg_start[c]; i < seg_end[c]; i++) {
-      const ChainItem it = items[i];
-      const float v = __fsub_rn(it.lam, b);
-      const double v64 = __dsub_rn((double)it.lam, (double)b);
-      if (it.a < 0) {  // split rows: (lambda - birth) * child_size, left then right
-        s = __fadd_rn(s, __fmul_rn(v, (float)(-it.a)));
-        s = __fadd_rn(s, __fmul_rn(v, (float)it.b));
-        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)(-it.a)));
-        s64 = __dadd_rn(s64, __dmul_rn(v64, (double)it.b));
-      } else {  // one row per point falling out here
-        s = add_repeated<float>(s, v, it.a);
-        s64 = add_repeated<double>(s64, v64, it.a);
+    const int64_t e = seg_end[c];
+    for (int64_t base = seg_start[c]; base < e; base += 32) {
+      ChainItem mine = {0.0f, 0, 0, 0};
+      if (base + lane < e) mine = items[base + lane];
+      const int m = (int)min((int64_t)32, e - base);
+      for (int t = 0; t < m; t++) {
+        const float lam = __shfl_sync(0xffffffffu, mine.lam, t);
+        const int32_t ia = __shfl_sync(0xffffffffu, mine.a, t);
+        const int32_t ib = __shfl_sync(0xffffffffu, mine.b, t);
+        const float v = __fsub_rn(lam, b);
+        const double v64 = __dsub_rn((double)lam, (double)b);
+        if (ia < 0) {  // split rows: (lambda - birth) * child_size, left then right
+          s = __fadd_rn(s, __fmul_rn(v, (float)(-ia)));
+          s = __fadd_rn(s, __fmul_rn(v, (float)ib));
+          s64 = __dadd_rn(s64, __dmul_rn(v64, (double)(-ia)));
+          s64 = __dadd_rn(s64, __dmul_rn(v64, (double)ib));
+        } else if (ia == 1) {  // one row
+          s = __fadd_rn(s, v);
+          s64 = __dadd_rn(s64, v64);
+        } else {  // one row per point falling out here
+          s = add_repeated<float>(s, v, ia);
+          s64 = add_repeated<double>(s64, v64, ia);
+        }
       }
     }
-    stab[c] = s;
-    stab64[c] = s64;
+    if (lane == 0) {
+      stab[c] = s;
+      stab64[c] = s64;
+    }
   }
 }
 
@@ -855,7 +873,7 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     Buf<ChainItem> items(ctx, nv_total);
     k_chain_items<<<grid_for(ctx, nv_total, 256), 256, 0, st>>>(t, chain, nv_total, kind, lam,
                                                                 items); ctx->launches++;
-    k_stability<<<gc, 32, 0, st>>>(C, s0, s1, items, birth, stab, stab64); ctx->launches++;
+    k_stability<<<grid_for(ctx, C, 4), 128, 0, st>>>(C, s0, s1, items, birth, stab, stab64); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
 

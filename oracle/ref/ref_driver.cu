@@ -1,0 +1,223 @@
+// Driver for the reference's own HDBSCAN code, compiled unmodified from the
+// reference tree (see oracle/ref/Makefile).  TEST INFRASTRUCTURE ONLY: it
+// produces golden outputs that pin the CPU oracle (oracle/hdb_oracle.c).
+//
+// The reference's multi-GPU plumbing (countDegrees, countThreshold_,
+// calculateUntieScore, calculateMutualReachabilityDistance) loops over 3 GPUs;
+// on a one-GPU box those loops fail, so this driver calls the same reference
+// kernels and host functions those wrappers call, on device 0, in the order of
+// buildEnhancedKNNG / buildECLgraph (HDBSCAN/graphs/graph.cu:16-176).
+// Everything after the graph -- cpuMST, buildMST (with sort_edges),
+// build_Linkage_tree, build_Condensed_tree, compute_stability, get_clusters --
+// is called directly.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "HDBSCAN/calculates/calculates.cuh"
+#include "HDBSCAN/counts/count.cuh"
+#include "HDBSCAN/getters/getters.cuh"
+#include "HDBSCAN/initializer/initialize.cuh"
+#include "HDBSCAN/mst/mst.cuh"
+#include "HDBSCAN/structs/ECLgraph.h"
+#include "HDBSCAN/structs/hdbscan_elements.cuh"
+#include "HDBSCAN/trees/tree.cuh"
+#include "HDBSCAN/graphs/graph.cuh"
+#include "gpuknn/nndescent.cuh"
+
+// ---- stand-ins for the reference's fixed-path file helpers (build_kNNG.cu) ----
+static const float *g_vectors = nullptr;
+static int g_dim = 0;
+
+// jesus (build_kNNG.cu:58-77) reads /nndescent/.../vectors.fvecs and gathers
+// the antihub rows; here the rows come from the caller's array.
+float *jesus(int *antihubs, int num_antihubs, int *paz) {
+  float *out = new float[(size_t)g_dim * num_antihubs];
+  for (long i = 0; i < num_antihubs; i++)
+    for (long j = 0; j < g_dim; j++) out[i * g_dim + j] = g_vectors[(long)antihubs[i] * g_dim + j];
+  *paz = g_dim;
+  return out;
+}
+// write_bool_dict (build_kNNG.cu:79-87) only persists the mutual flags.
+void write_bool_dict(int *, long, long) {}
+
+static int check(const char *what) {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
+    return 1;
+  }
+  return 0;
+}
+
+extern "C" {
+
+// Enhanced kNN graph.  Outputs are malloc'd; free with ref_free.
+long ref_enhanced_knng(const int *ids_in, const float *dist_in, const float *X, long n, int d,
+                       int kk, long **nindex_out, int **nlist_out, float **ew_out,
+                       int **antihubs_out, int *num_antihubs_out) {
+  if (kk != k) {
+    fprintf(stderr, "reference compiled with k = %d\n", k);
+    return -1;
+  }
+  g_vectors = X;
+  g_dim = d;
+  long vectorSize = n * (long)k;
+  int *kNN;
+  float *distances;
+  cudaMallocManaged(&kNN, vectorSize * sizeof(int));
+  cudaMallocManaged(&distances, vectorSize * sizeof(float));
+  memcpy(kNN, ids_in, vectorSize * sizeof(int));
+  memcpy(distances, dist_in, vectorSize * sizeof(float));
+  // calculate_degrees / countDegrees / countValues (calculates.cu:448, count.cu:10-110)
+  int *finalCounts;
+  cudaMallocManaged(&finalCounts, n * sizeof(int));
+  cudaMemset(finalCounts, 0, n * sizeof(int));
+  countValues<<<(unsigned)(vectorSize / blockSize + 1), blockSize>>>(kNN, finalCounts, vectorSize);
+  if (check("countValues")) return -1;
+  // buildEnhancedKNNG (graph.cu:108-151)
+  Vertex *vertexes;
+  cudaMallocManaged(&vertexes, n * sizeof(Vertex));
+  initializeVertex<<<(unsigned)((n + blockSize - 1) / blockSize), blockSize>>>(vertexes, finalCounts, n);
+  if (check("initializeVertex")) return -1;
+  int pos_threshold = get_NumThreshold(n);
+  std::partial_sort(vertexes, vertexes + pos_threshold, vertexes + n, compareVertexByDegree);
+  int value_threshold = vertexes[pos_threshold - 1].grau;
+  int countsTreshold = 0;  // countThreshold_ (count.cu:112-177)
+  for (long i = 0; i < n; i++) countsTreshold += (vertexes[i].grau == value_threshold);
+  int *antihubs = new int[pos_threshold];
+  if (countsTreshold > 1) {
+    // calculate_finalAntihubs (calculates.cu:491-523) with calculateUntieScore on one GPU
+    int *treshold_idx;
+    cudaMallocManaged(&treshold_idx, countsTreshold * sizeof(int));
+    get_IndexThreshold(finalCounts, treshold_idx, value_threshold, n);
+    Untie_hub *unties_dev;
+    cudaMalloc(&unties_dev, countsTreshold * sizeof(Untie_hub));
+    long numBlocks = countsTreshold / blockSize + 1;
+    initializeUntieHubs<<<(unsigned)numBlocks, blockSize>>>(unties_dev, 0, countsTreshold);
+    calculateScore<<<(unsigned)numBlocks, blockSize>>>(kNN, treshold_idx, unties_dev, finalCounts,
+                                                       countsTreshold, k, 0);
+    if (check("calculateScore")) return -1;
+    Untie_hub *unties = new Untie_hub[countsTreshold];
+    cudaMemcpy(unties, unties_dev, countsTreshold * sizeof(Untie_hub), cudaMemcpyDeviceToHost);
+    cudaFree(unties_dev);
+    int missing_ties = get_TiedVertexes(vertexes, pos_threshold, value_threshold);
+    int not_ties = pos_threshold - missing_ties;
+    std::partial_sort(unties, unties + missing_ties, unties + countsTreshold, compareVertexByScore);
+    joinAntiHubs(antihubs, vertexes, not_ties, unties, missing_ties);
+    delete[] unties;
+    cudaFree(treshold_idx);
+  } else {
+    for (int i = 0; i < pos_threshold; i++) antihubs[i] = vertexes[i].index;
+  }
+  std::sort(antihubs, antihubs + pos_threshold);
+  cudaFree(finalCounts);
+  cudaFree(vertexes);
+  // buildECLgraph (graph.cu:16-103)
+  ECLgraph g;
+  g.nodes = (int)n;
+  cudaMallocManaged(&g.nindex, (n + 1) * sizeof(long));
+  memset(g.nindex, 0, (n + 1) * sizeof(long));
+  int *flag_knn = (int *)malloc(vectorSize * sizeof(int));
+  calculate_nindex((int)n, kNN, flag_knn, &g, antihubs, pos_threshold);
+  long *auxiliar_edges;
+  cudaMallocManaged(&auxiliar_edges, n * sizeof(long));
+  memset(auxiliar_edges, 0, n * sizeof(long));
+  cudaMallocManaged(&g.nlist, g.nindex[n] * sizeof(int));
+  g.edges = g.nindex[n];
+  calculate_nlist((int)n, kNN, k, flag_knn, &g, antihubs, pos_threshold, auxiliar_edges);
+  free(flag_knn);
+  cudaMallocManaged(&g.eweight, g.edges * sizeof(float));
+  int *aux_nodes;
+  cudaMallocManaged(&aux_nodes, g.edges * sizeof(int));
+  createNodeList(aux_nodes, &g);
+  float *coreDistances;
+  cudaMallocManaged(&coreDistances, n * sizeof(float));
+  calculateCoreDistance(distances, coreDistances, n, k, k - 1);
+  // calculateMutualReachabilityDistance (calculates.cu:199-273) on one GPU
+  calculateMRD<<<(unsigned)(g.edges / blockSize + 1), blockSize>>>(g.eweight, aux_nodes, g.nlist,
+                                                                   coreDistances, g.edges);
+  if (check("calculateMRD")) return -1;
+  calculate_coreDistance_antihubs(&g, auxiliar_edges, antihubs, pos_threshold);
+  long E = g.edges;
+  *nindex_out = (long *)malloc((n + 1) * sizeof(long));
+  *nlist_out = (int *)malloc(E * sizeof(int));
+  *ew_out = (float *)malloc(E * sizeof(float));
+  *antihubs_out = (int *)malloc(pos_threshold * sizeof(int));
+  memcpy(*nindex_out, g.nindex, (n + 1) * sizeof(long));
+  memcpy(*nlist_out, g.nlist, E * sizeof(int));
+  memcpy(*ew_out, g.eweight, E * sizeof(float));
+  memcpy(*antihubs_out, antihubs, pos_threshold * sizeof(int));
+  *num_antihubs_out = pos_threshold;
+  delete[] antihubs;
+  cudaFree(kNN);
+  cudaFree(distances);
+  cudaFree(aux_nodes);
+  cudaFree(coreDistances);
+  cudaFree(auxiliar_edges);
+  cudaFree(g.nindex);
+  cudaFree(g.nlist);
+  cudaFree(g.eweight);
+  return E;
+}
+
+// cpuMST + buildMST (sort_edges) + build_Linkage_tree + build_Condensed_tree
+// + compute_stability + get_clusters (HDBSCAN/_new.cu:311-347).
+int ref_mst_trees(const long *nindex, const int *nlist, const float *ew, long n, int mpts,
+                  MSTedge *mst_out, SingleLinkageNode *hier_out, int *labels_out,
+                  CondensedTreeNode **cond_out, long *cond_size, Stability **stab_out,
+                  long *stab_size) {
+  ECLgraph g;
+  g.nodes = (int)n;
+  g.edges = nindex[n];
+  cudaMallocManaged(&g.nindex, (n + 1) * sizeof(long));
+  cudaMallocManaged(&g.nlist, g.edges * sizeof(int));
+  cudaMallocManaged(&g.eweight, g.edges * sizeof(float));
+  memcpy(g.nindex, nindex, (n + 1) * sizeof(long));
+  memcpy(g.nlist, nlist, g.edges * sizeof(int));
+  memcpy(g.eweight, ew, g.edges * sizeof(float));
+  bool *edges = cpuMST(g);
+  MSTedge *mst = buildMST(g, edges);
+  if (check("buildMST")) return 1;
+  memcpy(mst_out, mst, (n - 1) * sizeof(MSTedge));
+  SingleLinkageNode *h = build_Linkage_tree(mst, (int)n, (int)n);
+  memcpy(hier_out, h, (n - 1) * sizeof(SingleLinkageNode));
+  int csize = 0;
+  CondensedTreeNode *ct = build_Condensed_tree(h, (int)n, (int)n - 1, mpts, &csize);
+  int ssize = 0;
+  Stability *st = compute_stability(ct, csize, &ssize);
+  *stab_out = (Stability *)malloc(ssize * sizeof(Stability));
+  memcpy(*stab_out, st, ssize * sizeof(Stability));  // before get_clusters updates it
+  *stab_size = ssize;
+  *cond_out = (CondensedTreeNode *)malloc(csize * sizeof(CondensedTreeNode));
+  memcpy(*cond_out, ct, csize * sizeof(CondensedTreeNode));
+  *cond_size = csize;
+  int *labels = get_clusters(ct, csize, st, ssize, (int)n);
+  memcpy(labels_out, labels, n * sizeof(int));
+  cudaFree(g.nindex);
+  cudaFree(g.nlist);
+  cudaFree(g.eweight);
+  return check("trees");
+}
+
+// gpuknn::NNDescent (gpuknn/nndescent.cu:2088-2199) as compiled: VEC_DIM = 12,
+// NEIGHB_NUM_PER_LIST = 32, SAMPLE_NUM = 16.
+int ref_nndescent(const float *X, long n, int d, int iterations, NNDElement *G_out) {
+  if (d != VEC_DIM) return 1;
+  float *Xd;
+  cudaMalloc(&Xd, n * d * sizeof(float));
+  cudaMemcpy(Xd, X, n * d * sizeof(float), cudaMemcpyHostToDevice);
+  NNDElement *G = nullptr;
+  gpuknn::NNDescent(&G, Xd, (int)n, d, iterations, false);
+  if (check("NNDescent")) return 1;
+  memcpy(G_out, G, n * NEIGHB_NUM_PER_LIST * sizeof(NNDElement));
+  delete[] G;
+  cudaFree(Xd);
+  return 0;
+}
+
+void ref_free(void *p) { free(p); }
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+"""Generates the golden fixtures that pin the CPU oracle: runs the reference's
+own code (oracle/_ref/libhdbref.so, built by oracle/ref/Makefile from the
+unmodified reference sources) on small seeded inputs and stores inputs and
+outputs as compressed .npz files.
+
+Needs a GPU (the reference's tree stages allocate managed memory and launch
+fill kernels).  Usage on a GPU box, from the repository root:
+
+    python tests/golden/make_ref_golden.py OUTDIR
+
+The kNN graphs fed to the reference come from the oracle's NN-Descent (with
+fix_distances applied), so every later stage sees one shared input.  The
+reference NN-Descent itself (compiled with VEC_DIM = 12) is also run on the
+d = 12 cases and its recall@32 against the exact FP64 kNN is recorded.
+"""
+import ctypes as C
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from conftest import blobs  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+MST_EDGE, LINK, COND, STAB = O.MST_EDGE, O.LINKAGE_NODE, O.CONDENSED_NODE, O.STABILITY
+
+CASES = [
+    # name, n, d, blobs, noise, seed, mpts list
+    ("blobs_d12", 1500, 12, 6, 0.05, 101, [32, 8]),
+    ("noisy_d3", 1200, 3, 4, 0.20, 102, [16, 32]),
+    ("grid_ties_d2", 900, 2, 0, 0.0, 103, [32, 5]),
+]
+
+
+def grid_points(n, seed):
+    """Integer grid points with duplicates: many equal distances and weights."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 12, size=(n, 2)).astype(np.float32)
+
+
+def load_ref():
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libhdbref.so"), mode=C.RTLD_GLOBAL)
+    P = C.c_void_p
+    L.ref_enhanced_knng.restype = C.c_long
+    L.ref_enhanced_knng.argtypes = [P, P, P, C.c_long, C.c_int, C.c_int, P, P, P, P, P]
+    L.ref_mst_trees.restype = C.c_int
+    L.ref_mst_trees.argtypes = [P, P, P, C.c_long, C.c_int, P, P, P, P, P, P, P]
+    L.ref_nndescent.restype = C.c_int
+    L.ref_nndescent.argtypes = [P, C.c_long, C.c_int, C.c_int, P]
+    L.ref_free.argtypes = [P]
+    return L
+
+
+def p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def take(L, ptr, count, ctype):
+    arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count,)).copy()
+    L.ref_free(ptr)
+    return arr
+
+
+def run_case(L, name, n, d, nblobs, noise, seed, mpts_list, outdir):
+    X = grid_points(n, seed) if nblobs == 0 else blobs(n, d, seed, blobs=nblobs, noise=noise)
+    X = np.ascontiguousarray(X, np.float32)
+    ids, _ = O.nndescent(X, 32, 16, 6)
+    dist = O.fix_distances(X, ids)
+    ids = np.ascontiguousarray(ids, np.int32)
+    pn, pl, pw, pa = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    nah = C.c_int(0)
+    E = L.ref_enhanced_knng(p(ids), p(dist), p(X), n, d, 32, C.byref(pn), C.byref(pl), C.byref(pw),
+                            C.byref(pa), C.byref(nah))
+    assert E > 0, "reference enhanced kNN graph failed"
+    nindex = take(L, pn, n + 1, C.c_long).astype(np.int64)
+    nlist = take(L, pl, E, C.c_int)
+    ew = take(L, pw, E, C.c_float)
+    ah = take(L, pa, nah.value, C.c_int)
+    out = dict(X=X, ids=ids, dist=dist, nindex=nindex, nlist=nlist, eweight=ew, antihubs=ah)
+    meta = {"name": name, "n": n, "d": d, "k": 32, "edges": int(E), "mpts": mpts_list}
+    for mpts in mpts_list:
+        mst = np.zeros(n - 1, MST_EDGE)
+        hier = np.zeros(n - 1, LINK)
+        labels = np.zeros(n, np.int32)
+        pc, ps = C.c_void_p(), C.c_void_p()
+        cs, ss = C.c_long(0), C.c_long(0)
+        rc = L.ref_mst_trees(p(nindex), p(nlist), p(ew), n, mpts, p(mst), p(hier), p(labels),
+                             C.byref(pc), C.byref(cs), C.byref(ps), C.byref(ss))
+        assert rc == 0, "reference MST / trees failed"
+        cond = take(L, pc, cs.value * 4, C.c_int).view(COND)
+        stab = take(L, ps, ss.value * 2, C.c_int).view(STAB)
+        out[f"mst_{mpts}"] = mst
+        out[f"hier_{mpts}"] = hier
+        out[f"labels_{mpts}"] = labels
+        out[f"cond_{mpts}"] = cond
+        out[f"stab_{mpts}"] = stab
+    if d == 12:
+        G = np.zeros((n, 32, 2), np.int32)
+        assert L.ref_nndescent(p(X), n, d, 6, p(G)) == 0
+        rids = G[:, :, 1].copy()
+        rids = np.where(rids < 0, -rids - 1, rids)
+        gt, _ = O.bruteforce_knn(X, 32)
+        meta["ref_nndescent_recall32"] = O.recall(rids, gt, 32)
+        meta["oracle_nndescent_recall32"] = O.recall(ids, gt, 32)
+        out["ref_knn_ids"] = rids.astype(np.int32)
+    np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **out)
+    with open(os.path.join(outdir, f"ref_{name}.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    print(name, meta, flush=True)
+
+
+def main():
+    outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden")
+    os.makedirs(outdir, exist_ok=True)
+    O.build()
+    L = load_ref()
+    for case in CASES:
+        run_case(L, *case, outdir)
+
+
+if __name__ == "__main__":
+    main()

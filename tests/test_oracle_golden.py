@@ -1,0 +1,75 @@
+"""The oracle against golden outputs of the reference's own code.
+
+tests/golden/ref_*.npz were produced by tests/golden/make_ref_golden.py, which
+runs the unmodified reference sources (compiled by oracle/ref/Makefile) on a
+GPU box.  These CPU tests pin every stage of the oracle to them; the GPU tests
+(test_gpu_golden.py) pin the CUDA path to the same files."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
+
+
+def load(path):
+    data = dict(np.load(path))
+    with open(path[:-4] + ".json") as f:
+        meta = json.load(f)
+    return data, meta
+
+
+pytestmark = pytest.mark.skipif(not FILES, reason="no golden fixtures")
+
+
+@pytest.fixture(params=FILES, ids=lambda p: os.path.basename(p)[4:-4])
+def golden(request):
+    return load(request.param)
+
+
+def test_enhanced_knng_matches_reference(oracle, golden):
+    g, meta = golden
+    nindex, nlist, ew, ah = oracle.enhanced_knng(g["ids"], g["dist"], g["X"])
+    np.testing.assert_array_equal(ah, g["antihubs"])
+    np.testing.assert_array_equal(nindex, g["nindex"])
+    np.testing.assert_array_equal(nlist, g["nlist"])
+    np.testing.assert_array_equal(ew.view(np.uint32), g["eweight"].view(np.uint32))
+
+
+def test_mst_and_trees_match_reference(oracle, golden):
+    g, meta = golden
+    n = meta["n"]
+    inm = oracle.kruskal(g["nindex"], g["nlist"], g["eweight"])
+    mst = oracle.sort_edges(oracle.build_mst(g["nindex"], g["nlist"], g["eweight"], inm))
+    for mpts in meta["mpts"]:
+        ref_mst = g[f"mst_{mpts}"]
+        for f in ("from_node", "to_node"):
+            np.testing.assert_array_equal(mst[f], ref_mst[f])
+        np.testing.assert_array_equal(mst["weight"].view(np.uint32), ref_mst["weight"].view(np.uint32))
+        hier = oracle.linkage_tree(ref_mst, n)
+        ref_h = g[f"hier_{mpts}"]
+        for f in ("left_node", "right_node", "node_size"):
+            np.testing.assert_array_equal(hier[f], ref_h[f])
+        cond = oracle.condensed_tree(ref_h, n, mpts)
+        ref_c = g[f"cond_{mpts}"]
+        assert len(cond) == len(ref_c)
+        for f in ("parent", "child", "child_size"):
+            np.testing.assert_array_equal(cond[f], ref_c[f])  # same row order
+        np.testing.assert_array_equal(cond["lambda_val"].view(np.uint32),
+                                      ref_c["lambda_val"].view(np.uint32))
+        stab, _ = oracle.stability(ref_c)
+        np.testing.assert_array_equal(stab["cluster_id"], g[f"stab_{mpts}"]["cluster_id"])
+        np.testing.assert_array_equal(stab["lambda"].view(np.uint32),
+                                      g[f"stab_{mpts}"]["lambda"].view(np.uint32))
+        labels, _ = oracle.get_clusters(ref_c, g[f"stab_{mpts}"], n)
+        np.testing.assert_array_equal(labels, g[f"labels_{mpts}"])
+
+
+def test_oracle_nndescent_recall_is_within_half_a_point_of_the_reference(oracle, golden):
+    g, meta = golden
+    if "ref_nndescent_recall32" not in meta:
+        pytest.skip("the reference NN-Descent is compiled for d = 12 only")
+    assert abs(meta["oracle_nndescent_recall32"] - meta["ref_nndescent_recall32"]) <= 0.005 + 0.02, meta
