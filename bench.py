@@ -40,8 +40,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="blobs_10m_d12")
-    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--workload", default="blobs_20m_d128")
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default="bf16")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the other form (plain FP32 vs BF16-TC)")
+    ap.add_argument("--recall-queries", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="points in the CPU baseline sample (0: sized per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -130,6 +133,29 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def exact_recall(X, G_ids, queries, k):
+    """recall@k of G_ids[queries] against the exact FP64 kNN (torch, chunked)."""
+    import torch
+    q = torch.as_tensor(queries, device=X.device)
+    Xq = X[q].double()
+    best_d = torch.full((len(q), k), float("inf"), dtype=torch.float64, device=X.device)
+    best_i = torch.zeros((len(q), k), dtype=torch.int64, device=X.device)
+    chunk = 1 << 18
+    for s0 in range(0, X.shape[0], chunk):
+        Xc = X[s0:s0 + chunk].double()
+        dd = torch.cdist(Xq, Xc).square_()
+        idx = torch.arange(s0, s0 + Xc.shape[0], device=X.device)
+        dd[idx[None, :] == q[:, None]] = float("inf")  # exclude the point itself
+        cd = torch.cat([best_d, dd], dim=1)
+        ci = torch.cat([best_i, idx[None, :].expand(len(q), -1)], dim=1)
+        top = torch.topk(cd, k, dim=1, largest=False)
+        best_d = top.values
+        best_i = torch.gather(ci, 1, top.indices)
+    got = G_ids[q].long()
+    hits = (got[:, :, None] == best_i[:, None, :]).any(dim=2).sum().item()
+    return hits / (len(q) * k)
+
+
 def cpu_baseline_run(workload, n_sample, steps):
     """The reference algorithm on the host cores (oracle port, OpenMP over all
     available threads): NN-Descent + the _new.cu stages on a sample."""
@@ -153,7 +179,7 @@ def cpu_baseline_run(workload, n_sample, steps):
 
 
 def default_cpu_sample(w):
-    return 100_000 if w.d <= 16 else 20_000
+    return 100_000 if w.d <= 16 else 15_000
 
 
 def run_reference(args, w):
@@ -203,31 +229,60 @@ def run_ours(args, w):
         if world > 1:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        ctx.hdbscan(X, **kw)
-    torch.cuda.synchronize()
+    def timed(kwx, steps, warmup):
+        for _ in range(warmup):
+            ctx.hdbscan(X, **kwx)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        stream = torch.cuda.current_stream()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        stats = []
+        ev0.record(stream)
+        for _ in range(steps):
+            _, st = ctx.hdbscan(X, **kwx)
+            stats.append(st)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), stats
+
     clocks = ClockSampler(local)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    stream = torch.cuda.current_stream()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    stats = []
-    ev0.record(stream)
-    for _ in range(args.steps):
-        _, st = ctx.hdbscan(X, **kw)
-        stats.append(st)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+    ms_max, stats = timed(kw, args.steps, args.warmup)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
     value = w.n * args.steps * world / (ms_max / 1e3)
+    stream = torch.cuda.current_stream()
+
+    # the other form, for the BF16-TC vs plain FP32 comparison, and recall@32
+    # of both against the exact FP64 kNN on a sample of rows
+    compare = None
+    if not args.no_compare:
+        other = g.HDB_PREC_FP32 if prec == g.HDB_PREC_BF16 else g.HDB_PREC_BF16
+        kwo = {**kw, "precision": other}
+        osteps = max(1, args.steps // 2)
+        oms, ostats = timed(kwo, osteps, 1)
+        compare = {"form": "fp32" if other == g.HDB_PREC_FP32 else "bf16",
+                   "points_per_s": round(w.n * osteps * world / (oms / 1e3), 1),
+                   "ms_per_step": round(oms / osteps, 3), "steps": osteps,
+                   "stage_ms": {s_: round(ostats[-1][f"ms_{s_}"], 3) for s_ in
+                                ("knn", "graph", "mst", "tree", "total")}}
+    recall = {}
+    if args.recall_queries > 0:
+        qidx = torch.randperm(w.n, generator=torch.Generator().manual_seed(7))[:args.recall_queries]
+        for name_, pr in (("bf16", g.HDB_PREC_BF16), ("fp32", g.HDB_PREC_FP32)):
+            if compare is None and pr != prec:
+                continue
+            G = ctx.NNDescent(X, k=w.k, sample_num=w.sample_num, iterations=w.iterations,
+                              precision=pr)
+            ids, _ = ctx.knn_split(G)
+            recall[name_] = round(exact_recall(X, ids, qidx.to(dev), w.k), 4)
+            del G, ids
+        torch.cuda.empty_cache()
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -289,7 +344,10 @@ def run_ours(args, w):
                            "stage_ms": {s: round(last[f"ms_{s}"], 3) for s in
                                         ("knn", "graph", "mst", "tree", "total")},
                            "num_clusters": last["num_clusters"], "edges": last["edges"],
-                           "mst_rounds": last["mst_rounds"], "knn_dropped": last["knn_dropped"]},
+                           "mst_rounds": last["mst_rounds"], "knn_dropped": last["knn_dropped"],
+                           "other_form": compare, "recall_at_k": recall,
+                           "speedup_vs_other_form": (round(value / compare["points_per_s"], 3)
+                                                     if compare else None)},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
                 "gpu_launches": int(sum(s["gpu_launches"] for s in stats))}
         print(json.dumps(line), flush=True)

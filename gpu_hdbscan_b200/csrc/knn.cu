@@ -14,6 +14,8 @@
 //  * distances are the reference's sequential FP32 difference sum
 //    (nndescent.cu:1086-1093, fmaf per element), so every pair has one exact
 //    value wherever it is computed.
+#include <cuda_bf16.h>
+
 #include <vector>
 
 #include "hdb_internal.cuh"
@@ -488,6 +490,275 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
   }
 }
 
+// ---------------------------------------------------------------------------
+// BF16 tensor-core form of the local join.
+//
+// Candidate distances come from ||x||^2 + ||y||^2 - 2 x.y with x, y rounded to
+// BF16 (norms of the rounded rows, FP32), the dot products on the tensor cores
+// with FP32 accumulation (mma.sync m16n8k16, operands staged with cp.async
+// and ldmatrix).  One pair always gets one value, whichever row joins it.
+// After the last iteration every kept neighbour is re-ranked with the exact
+// FP32 difference sum (k_rerank), so the graph handed on carries the
+// reference's distances.
+// ---------------------------------------------------------------------------
+struct JoinSmemBf16 {
+  // per warp: best[96] u64 | ids[64] | norms[64] | rows [64][dpad + 8] bf16
+  __host__ __device__ static size_t bytes(int dpad) {
+    return 96 * 8 + 64 * 4 + 64 * 4 + (size_t)64 * (dpad + 8) * 2;
+  }
+};
+
+__global__ void k_bf16_prepare(const float *__restrict__ X, int64_t n, int d, int dpad,
+                               __nv_bfloat16 *__restrict__ Xb, float *__restrict__ nrm) {
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    float part = 0.0f;
+    for (int j = lane; j < dpad; j += 32) {
+      __nv_bfloat16 b = __float2bfloat16_rn(j < d ? X[row * d + j] : 0.0f);
+      Xb[row * dpad + j] = b;
+      float v = __bfloat162float(b);
+      part = __fmaf_rn(v, v, part);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) part = __fadd_rn(part, __shfl_xor_sync(0xffffffffu, part, o));
+    if (lane == 0) nrm[row] = part;
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3,
+                                        const void *smem) {
+  uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(s));
+}
+__device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restrict__ Xb,
+                                                   const float *__restrict__ nrm, int64_t n,
+                                                   int dpad, int S,
+                                                   const int32_t *__restrict__ newS,
+                                                   const int32_t *__restrict__ oldS,
+                                                   const int8_t *__restrict__ nf,
+                                                   const int8_t *__restrict__ of,
+                                                   int32_t *__restrict__ nrev,
+                                                   int32_t *__restrict__ orev,
+                                                   const float *__restrict__ worst, Inbox ib) {
+  extern __shared__ __align__(16) unsigned char smem_bf[];
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  unsigned char *base = smem_bf + (threadIdx.x >> 5) * JoinSmemBf16::bytes(dpad);
+  unsigned long long *best = reinterpret_cast<unsigned long long *>(base);
+  unsigned long long *best1 = best, *best2 = best + 32, *best3 = best + 64;
+  int32_t *ids = reinterpret_cast<int32_t *>(base + 96 * 8);
+  float *nr = reinterpret_cast<float *>(base + 96 * 8 + 256);
+  __nv_bfloat16 *Bs = reinterpret_cast<__nv_bfloat16 *>(base + 96 * 8 + 512);
+  const int ld = dpad + 8;  // row stride in elements (16-byte aligned, ldmatrix conflict free)
+  const int chunks = dpad >> 3;  // 16-byte chunks per row
+  unsigned long long w_rows = 0, w_cands = 0;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const int cnf = nf[row], cof = of[row];
+    const int cnr = min(nrev[row], S), cor = min(orev[row], S);
+    __syncwarp();
+    if (lane == 0) { nrev[row] = 0; orev[row] = 0; }
+    const int64_t sb = row * (2 * S);
+    bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
+    bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
+    int32_t nid = vn ? newS[sb + lane] : -1 - lane;
+    int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    uint32_t pn = __match_any_sync(0xffffffffu, nid);
+    vn = vn && (__ffs(pn) - 1 == lane);
+    uint32_t po = __match_any_sync(0xffffffffu, oid);
+    vo = vo && (__ffs(po) - 1 == lane);
+    uint32_t bo = __ballot_sync(0xffffffffu, vo);
+    const int no = __popc(bo);
+    if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
+    __syncwarp();
+    for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
+    uint32_t bn = __ballot_sync(0xffffffffu, vn);
+    const int nn = __popc(bn);
+    if (vn) ids[__popc(bn & lanemask_lt())] = nid;
+    best1[lane] = ~0ull;
+    best2[lane] = ~0ull;
+    best3[lane] = ~0ull;
+    __syncwarp();
+    if (nn == 0 || nn + no < 2) continue;
+    w_rows += nn + no;
+    // stage rows: new at slots 0..nn-1, old at 32..32+no-1 (cp.async, 16 B)
+    const int T = nn + no;
+    for (int idx = lane; idx < T * chunks; idx += 32) {
+      int r = idx / chunks, c = idx - r * chunks;
+      int slot = r < nn ? r : 32 + (r - nn);
+      cp_async16(Bs + slot * ld + c * 8, Xb + (int64_t)ids[slot] * dpad + c * 8);
+    }
+    if (lane < nn) nr[lane] = nrm[ids[lane]];
+    if (lane < no) nr[32 + lane] = nrm[ids[32 + lane]];
+    cp_async_wait_all();
+    __syncwarp();
+    // G = B_new (32 x dpad) * B_all (64 x dpad)^T
+    float acc[2][8][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[i][j][e] = 0.0f;
+    const int mts = nn > 16 ? 2 : 1;
+    const bool any_old = no > 0;
+    for (int kt = 0; kt < dpad; kt += 16) {
+      uint32_t a[2][4];
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++)
+        if (mt < mts)
+          ldsm_x4(a[mt][0], a[mt][1], a[mt][2], a[mt][3],
+                  Bs + (16 * mt + (lane & 15)) * ld + kt + ((lane >> 4) << 3));
+#pragma unroll
+      for (int pr = 0; pr < 4; pr++) {
+        if (pr >= 2 && !any_old) continue;
+        uint32_t b0, b1, b2, b3;
+        const int prow = 16 * pr + ((lane >> 4) << 3) + (lane & 7);
+        ldsm_x4(b0, b1, b2, b3, Bs + prow * ld + kt + (((lane >> 3) & 1) << 3));
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+          if (mt >= mts) continue;
+          mma_bf16(acc[mt][2 * pr], a[mt], b0, b1);
+          mma_bf16(acc[mt][2 * pr + 1], a[mt], b2, b3);
+        }
+      }
+    }
+    // epilogue: distances, row minima (best1 / best2) and old-column minima (best3)
+    uint64_t cmin[4][2];  // old n-tiles 4..7, two columns each
+#pragma unroll
+    for (int q = 0; q < 4; q++) cmin[q][0] = cmin[q][1] = ~0ull;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int a = 16 * mt + (lane >> 2) + 8 * h;
+        const bool arow = mt < mts && a < nn;
+        const float na = arow ? nr[a] : 0.0f;
+        uint64_t rn = ~0ull, ro = ~0ull;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int c = 8 * nt + 2 * (lane & 3) + e;
+            const bool oldc = c >= 32;
+            const bool ok = arow && (oldc ? (c - 32 < no) : (c < nn && c != a));
+            if (!ok) continue;
+            float dd = __fmaf_rn(-2.0f, acc[mt][nt][2 * h + e], __fadd_rn(na, nr[c]));
+            dd = dd > 0.0f ? dd : 0.0f;
+            const uint64_t kr = pack(dd, ids[c]);
+            if (oldc) {
+              ro = kr < ro ? kr : ro;
+              const uint64_t kc = pack(dd, ids[a]);
+              uint64_t &m = cmin[nt - 4][e];
+              m = kc < m ? kc : m;
+            } else {
+              rn = kr < rn ? kr : rn;
+            }
+          }
+        }
+        // the four lanes of a row
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+          uint64_t x = __shfl_xor_sync(0xffffffffu, rn, o);
+          rn = x < rn ? x : rn;
+          x = __shfl_xor_sync(0xffffffffu, ro, o);
+          ro = x < ro ? x : ro;
+        }
+        if (arow && (lane & 3) == 0) {
+          best1[a] = rn;
+          best2[a] = ro;
+        }
+      }
+    }
+    // the eight row-lanes of a column
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        uint64_t m = cmin[q][e];
+#pragma unroll
+        for (int o = 4; o <= 16; o <<= 1) {
+          uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+          m = x < m ? x : m;
+        }
+        const int c = 8 * q + 2 * (lane & 3) + e;  // old column index
+        if (lane < 4 && c < no) best3[c] = m;
+      }
+    __syncwarp();
+    int pushed = 0;
+    if (lane < nn) {
+      const int32_t x = ids[lane];
+      const uint64_t b1 = best1[lane], b2 = best2[lane];
+      if (b1 != ~0ull) pushed += push_candidate(x, pk_id(b1), pk_dist(b1), worst, ib);
+      if (b2 != ~0ull) pushed += push_candidate(x, pk_id(b2), pk_dist(b2), worst, ib);
+    }
+    if (lane < no) {
+      const uint64_t b3 = best3[lane];
+      if (b3 != ~0ull) pushed += push_candidate(ids[32 + lane], pk_id(b3), pk_dist(b3), worst, ib);
+    }
+    w_cands += pushed;
+    __syncwarp();
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) w_cands += __shfl_xor_sync(0xffffffffu, w_cands, o);
+  if (lane == 0) {
+    if (w_rows) atomicAdd(&ib.counters[1], w_rows);
+    if (w_cands) atomicAdd(&ib.counters[2], w_cands);
+  }
+}
+
+// FP32 re-rank of every kept neighbour (one warp per row): the reference's
+// difference sum for each (row, neighbour) pair, rows re-sorted by (distance,
+// id); old/new flags travel with their ids.
+__global__ void k_rerank(const float *__restrict__ X, int64_t n, int d, int k,
+                         hdb_nnd_element *__restrict__ G) {
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    uint64_t key = ~0ull;
+    int32_t lab = 0;
+    if (lane < k) {
+      hdb_nnd_element e = G[row * k + lane];
+      lab = e.label_;
+      const int32_t id = decode(lab);
+      key = pack(diffsum(X + row * d, X + (int64_t)id * d, d), id);
+    }
+    const uint64_t sorted = warp_sort32(key);
+    const int32_t sid = pk_id(sorted);
+    int32_t slab = sid;
+    for (int t = 0; t < k; t++) {
+      const int32_t l = __shfl_sync(0xffffffffu, lab, t);
+      if (decode(l) == sid) slab = l;
+    }
+    if (lane < k) {
+      hdb_nnd_element e;
+      e.distance_ = pk_dist(sorted);
+      e.label_ = slab;
+      G[row * k + lane] = e;
+    }
+  }
+}
+
 __global__ void k_split(const hdb_nnd_element *__restrict__ G, int64_t total, int32_t *__restrict__ ids,
                         float *__restrict__ dist) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
@@ -571,8 +842,8 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   HDB_REQUIRE(n > k && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "NN-Descent: need k < n < 2^31");
   HDB_REQUIRE(d >= 1 && d <= 4096, HDB_ERR_ARG, "NN-Descent: d must be in [1, 4096]");
   HDB_REQUIRE(p.iterations >= 0, HDB_ERR_ARG, "NN-Descent: negative iteration count");
-  HDB_REQUIRE(p.precision == HDB_PREC_FP32, HDB_ERR_ARG,
-              "NN-Descent: only HDB_PREC_FP32 is available in this build");
+  HDB_REQUIRE(p.precision == HDB_PREC_FP32 || p.precision == HDB_PREC_BF16, HDB_ERR_ARG,
+              "NN-Descent: unknown precision");
   cudaStream_t st = ctx->stream;
   Buf<int32_t> gid(ctx, n * k);
   Buf<float> gdist(ctx, n * k), worst(ctx, n);
@@ -611,13 +882,36 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "NN-Descent: d too large for the join tile");
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
   const int grid_join = grid_for(ctx, n, jw, 64);
+  const bool bf16 = p.precision == HDB_PREC_BF16;
+  const int dpad = (d + 15) & ~15;
+  Buf<__nv_bfloat16> Xb;
+  Buf<float> nrm;
+  int jw16 = 4;
+  size_t smem_bf = 0;
+  int grid_bf = 0;
+  if (bf16) {
+    Xb = Buf<__nv_bfloat16>(ctx, (size_t)n * dpad);
+    nrm = Buf<float>(ctx, n);
+    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, Xb, nrm); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    smem_bf = JoinSmemBf16::bytes(dpad) * jw16;
+    HDB_REQUIRE(smem_bf <= 227 * 1024, HDB_ERR_ARG, "NN-Descent BF16: d too large for the join tile");
+    HDB_CUDA(cudaFuncSetAttribute(k_join_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_bf));
+    grid_bf = grid_for(ctx, n, jw16, 64);
+  }
   for (int it = 0; it < p.iterations; it++) {
     k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
                                                        newS, oldS, nf, of, nrev, orev); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
-    k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
-                                                  ib); ctx->launches++;
+    if (bf16)
+      k_join_bf16<<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, newS, oldS, nf, of, nrev,
+                                                       orev, worst, ib);
+    else
+      k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
+                                                    ib);
+    ctx->launches++;
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
     HDB_CHECK_LAUNCH();
     sort_overflow(ctx, ib, n);
@@ -625,6 +919,10 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   }
   k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
+  if (bf16) {
+    k_rerank<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, G); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
   HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   ctx->sync();

@@ -155,3 +155,50 @@ def test_argument_errors(ctx):
         ctx.hdbscan(X, k=16, sample_num=9)
     with pytest.raises(HdbError, match="k"):
         ctx.hdbscan(X, k=64)
+
+
+@pytest.mark.parametrize("n,d", [(6000, 128), (5000, 12), (4000, 96)])
+def test_bf16_nndescent_graph_is_valid_and_reranked_exactly(ctx, oracle, n, d):
+    """BF16 tensor-core candidate distances, then an FP32 re-rank: the graph
+    handed on is valid, sorted, and carries the exact FP32 difference sums."""
+    from gpu_hdbscan_b200 import HDB_PREC_BF16
+    X = blobs(n, d, seed=31 + d, blobs=10, spread=20.0)
+    G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=HDB_PREC_BF16)
+    ids, dist = (_t(a) for a in ctx.knn_split(G))
+    assert oracle.validate_knn(ids)
+    key = dist.view(np.uint32).astype(np.uint64) << np.uint64(32) | ids.astype(np.uint64)
+    assert (np.diff(key, axis=1) > 0).all()
+    rng = np.random.default_rng(1)
+    for i in rng.choice(n, 100, replace=False):
+        for j in range(0, 32, 3):
+            assert np.float32(oracle.diffsum(X[i], X[ids[i, j]])).view(np.uint32) == \
+                dist[i, j].view(np.uint32)
+
+
+@pytest.mark.parametrize("d", [128, 64])
+def test_bf16_recall_matches_fp32_form(ctx, oracle, d):
+    """Recall@32 of the BF16 form within 0.5 pt of the plain FP32 form (the
+    benchmark's 'equal recall@k' condition) on blob data like the 20M x 128
+    workload."""
+    from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
+    w = synth.scaled("blobs_20m_d128", 30000)
+    X = synth.generate(w) if d == 128 else blobs(30000, d, seed=5, blobs=60, spread=20.0)
+    q = np.arange(0, len(X), 11)
+    gt, _ = oracle.bruteforce_knn(X, 32, q)
+    rec = {}
+    for name, prec in (("fp32", HDB_PREC_FP32), ("bf16", HDB_PREC_BF16)):
+        G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=prec)
+        rec[name] = oracle.recall(_t(ctx.knn_split(G)[0])[q], gt, 32)
+    assert rec["bf16"] >= rec["fp32"] - 0.005, rec
+
+
+def test_bf16_pipeline_labels_identical_on_shared_graph(ctx, oracle):
+    from gpu_hdbscan_b200 import HDB_PREC_BF16
+    X = blobs(6000, 64, seed=41, blobs=8, spread=20.0)
+    G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=HDB_PREC_BF16)
+    labels, stats = ctx.hdbscan_from_knn(G, X, k=32, mpts=32)
+    ids = _t(ctx.knn_split(G)[0])
+    _, ref, ncl = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 32)
+    np.testing.assert_array_equal(_t(labels), ref)
+    lab2, st2 = ctx.hdbscan(X, precision=HDB_PREC_BF16)
+    assert st2["num_clusters"] >= 2
