@@ -88,6 +88,22 @@ def generate(w: Workload) -> np.ndarray:
     return X[rng.permutation(w.n)]
 
 
+def sample(w: Workload, n_sample: int, seed: int = 12345) -> np.ndarray:
+    """n_sample points drawn from the same mixture as `w` (same blob centres,
+    sigmas and relative sizes, same noise fraction) -- a bounded sample of the
+    full workload for CPU timing, without generating all of it."""
+    rng = np.random.default_rng(w.seed)
+    sizes, centers, sigmas, _ = _layout(w, rng)
+    r2 = np.random.default_rng(seed)
+    n_noise = int(round(n_sample * w.noise))
+    p = sizes / max(1, sizes.sum())
+    which = r2.choice(w.blobs, size=n_sample - n_noise, p=p)
+    Xb = centers[which] + r2.normal(size=(len(which), w.d)) * sigmas[which]
+    lo, hi = Xb.min(axis=0), Xb.max(axis=0)
+    X = np.concatenate([Xb, r2.uniform(lo, hi, size=(n_noise, w.d))]).astype(np.float32)
+    return X[r2.permutation(n_sample)]
+
+
 def generate_torch(w: Workload, device="cuda"):
     """The same distribution built on `device` with a seeded torch generator."""
     import torch
