@@ -852,7 +852,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   Buf<int8_t> nf(ctx, n), of(ctx, n);
   Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
-  const int64_t ovf_cap = n * 4 > (1 << 20) ? n * 4 : (1 << 20);
+  const int64_t ovf_cap = n * 16 > (1 << 22) ? n * 16 : (1 << 22);
   Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ovf_idx(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
   Buf<uint64_t> ovf_key(ctx, ovf_cap);
   HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
