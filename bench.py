@@ -49,7 +49,16 @@ def parse_args():
                     help="points in the CPU baseline sample (0: sized per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--n", type=int, default=0,
+                    help="points (0: the workload's size); blob count scales with n")
+    ap.add_argument("--bare", action="store_true",
+                    help="time only the K steps (no other form, recall, e2e or CPU baseline); "
+                         "for profiler captures")
+    args = ap.parse_args()
+    if args.bare:
+        args.no_compare = args.no_e2e = args.no_cpu_baseline = True
+        args.recall_queries = 0
+    return args
 
 
 def measured_peaks():
@@ -131,6 +140,28 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def replica_workload(w, rank):
+    """Each replica (rank) clusters its own seeded copy of the workload."""
+    from gpu_hdbscan_b200 import synth
+    return synth.Workload(**{**w.__dict__, "seed": w.seed + 1000 * rank})
+
+
+def max_over_ranks(ms, device):
+    """The largest per-rank duration over all ranks of the process group (the
+    value itself on one rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(n, steps, world, ms):
+    """Points/s of the whole job: every replica clusters n points per step."""
+    return n * steps * world / (ms / 1e3)
 
 
 def exact_recall(X, G_ids, queries, k):
@@ -218,9 +249,7 @@ def run_ours(args, w):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
-    # each replica clusters its own seeded copy of the workload
-    wr = synth.Workload(**{**w.__dict__, "seed": w.seed + 1000 * rank})
-    X = synth.generate_torch(wr, device=dev)
+    X = synth.generate_torch(replica_workload(w, rank), device=dev)
     ctx = g.Context(local)
     kw = dict(k=w.k, mpts=w.mpts, sample_num=w.sample_num, iterations=w.iterations,
               precision=prec)
@@ -246,16 +275,13 @@ def run_ours(args, w):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), stats
+        return max_over_ranks(ev0.elapsed_time(ev1), dev), stats
 
     clocks = ClockSampler(local)
     clocks.start()
     ms_max, stats = timed(kw, args.steps, args.warmup)
     clk = clocks.stop()
-    value = w.n * args.steps * world / (ms_max / 1e3)
+    value = whole_job_rate(w.n, args.steps, world, ms_max)
     stream = torch.cuda.current_stream()
 
     # the other form, for the BF16-TC vs plain FP32 comparison, and recall@32
@@ -267,7 +293,7 @@ def run_ours(args, w):
         osteps = max(1, args.steps // 2)
         oms, ostats = timed(kwo, osteps, 1)
         compare = {"form": "fp32" if other == g.HDB_PREC_FP32 else "bf16",
-                   "points_per_s": round(w.n * osteps * world / (oms / 1e3), 1),
+                   "points_per_s": round(whole_job_rate(w.n, osteps, world, oms), 1),
                    "ms_per_step": round(oms / osteps, 3), "steps": osteps,
                    "stage_ms": {s_: round(ostats[-1][f"ms_{s_}"], 3) for s_ in
                                 ("knn", "graph", "mst", "tree", "total")}}
@@ -300,13 +326,14 @@ def run_ours(args, w):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": w.n * args.steps * world / (float(te.item()) / 1e3), "unit": UNIT,
+        te = max_over_ranks(e0.elapsed_time(e1), dev)
+        e2e = {"value": whole_job_rate(w.n, args.steps, world, te), "unit": UNIT,
                "h2d_bytes_per_step": int(w.n * w.d * 4), "d2h_bytes_per_step": int(w.n * 4)}
 
-    if rank == 0:
+    if rank == 0 and args.bare:
+        print(json.dumps({"bare": True, "workload": w.name, "ms_per_step": ms_max / args.steps,
+                          "stats": stats[-1]}), flush=True)
+    elif rank == 0:
         hbm, _, peak_kind = measured_peaks()
         last = stats[-1]
         S = w.sample_num
@@ -365,6 +392,10 @@ def main():
     args = parse_args()
     from gpu_hdbscan_b200 import synth
     w = synth.WORKLOADS[args.workload]
+    if args.n and args.n != w.n:
+        blobs = max(1, round(w.blobs * args.n / w.n))
+        w = synth.Workload(**{**w.__dict__, "name": f"{w.name}_n{args.n}", "n": args.n,
+                              "blobs": blobs})
     if args.impl == "reference":
         run_reference(args, w)
     else:
