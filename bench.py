@@ -341,15 +341,19 @@ def run_ours(args, w):
         # algorithmic bytes of the local join (per launch): staged sample rows,
         # the sample lists and counters, and each pushed candidate (inbox entry,
         # counter atomic, k-th distance read)
-        row_bytes = ((w.d + 15) // 16 * 16) * 2 if prec == g.HDB_PREC_BF16 else w.d * 4
+        if prec == g.HDB_PREC_BF16:
+            tc = (w.d + 63) // 64 * 64 <= 256  # tensor-core tiles, else the mma.sync join
+            jkernel = "k_join_tc" if tc else "k_join_bf16"
+            row_bytes = ((w.d + 63) // 64 * 64 if tc else (w.d + 15) // 16 * 16) * 2
+        else:
+            jkernel, row_bytes = "k_join", w.d * 4
         join_bytes = (last["join_rows_gathered"] * row_bytes
                       + launches * w.n * (2 * 2 * S * 4 + 2 * 4 + 2 * 1)
                       + last["join_candidates"] * (8 + 4 + 4)) / launches
         join_ms = last["join_ms"] / launches
         achieved = join_bytes / (join_ms / 1e3) / 1e9
-        tpr = profiled_traffic("k_join_bf16" if prec == g.HDB_PREC_BF16 else "k_join")
-        roofline = {"kernel": ("k_join_bf16" if prec == g.HDB_PREC_BF16 else "k_join")
-                              + " (NN-Descent local join)", "bound": "hbm",
+        tpr = profiled_traffic(jkernel)
+        roofline = {"kernel": jkernel + " (NN-Descent local join)", "bound": "hbm",
                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(achieved / hbm, 4),
                     "traffic": None if tpr is None else round(tpr * w.n),

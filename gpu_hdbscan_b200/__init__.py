@@ -110,6 +110,20 @@ class Context:
                                             _ptr(dist)))
         return dist
 
+    def bf16_distance_tiles(self, X, ids, counts):
+        """BF16 tensor-core distances of explicit slot lists (the arithmetic of
+        the BF16 local join): ids [tiles, 128], counts [tiles, 4] ->
+        [tiles, 128, 64] float32 (see hdb_bf16_distance_tiles)."""
+        torch = self._torch
+        X = self._dev(X, torch.float32)
+        ids = self._dev(ids, torch.int32)
+        counts = self._dev(counts, torch.int32)
+        tiles = ids.shape[0]
+        out = torch.empty((tiles, 128, 64), dtype=torch.float32, device=self.device)
+        _lib.check(self.L.hdb_bf16_distance_tiles(self.h, _ptr(X), X.shape[0], X.shape[1],
+                                                  _ptr(ids), _ptr(counts), tiles, _ptr(out)))
+        return out
+
     def buildEnhancedKNNG(self, ids, dist, X) -> EnhancedGraph:
         torch = self._torch
         ids = self._dev(ids, torch.int32)

@@ -24,7 +24,7 @@ HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
-           "hdb_run_knn", "hdb_sort_edges_noalloc")
+           "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles")
 
 
 class HdbError(RuntimeError):
@@ -91,6 +91,7 @@ def load(path: str = LIB_PATH):
         "hdb_run_knn": (C.c_int, [_P, _P, _P, _I64, _I32, C.POINTER(Params), _P,
                                   C.POINTER(RunStats)]),
         "hdb_sort_edges_noalloc": (C.c_int, [_P, _I64, _P]),
+        "hdb_bf16_distance_tiles": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _I64, _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,7 +1,10 @@
 // extern "C" entry points of libhdb_b200 (include/hdb/hdb.h) and the
 // end-to-end pipeline in the reference's HDBSCAN/_new.cu order.
+#include <vector>
+
 #include "graph.cuh"
 #include "hdb_internal.cuh"
+#include "join_tc.cuh"
 #include "knn.cuh"
 #include "mst.cuh"
 #include "trees.cuh"
@@ -71,6 +74,34 @@ HDB_API hdb_status hdb_fix_distances(hdb_ctx *h, const float *X, int64_t n, int3
     HDB_REQUIRE(n >= 0 && k >= 1 && d >= 1, HDB_ERR_ARG, "bad n, k or d");
     fix_distances(ctx, X, n, d, ids, k, dist);
     ctx->sync();
+  });
+}
+
+HDB_API hdb_status hdb_bf16_distance_tiles(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                                           const int32_t *ids, const int32_t *counts,
+                                           int64_t tiles, float *out) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(X, "X");
+    require_ptr(ids, "ids");
+    require_ptr(counts, "counts");
+    require_ptr(out, "out");
+    HDB_REQUIRE(tiles >= 0 && tiles <= (int64_t(1) << 24), HDB_ERR_ARG, "bad tile count");
+    // the slot lists are small: check them on the host before any device read
+    std::vector<int32_t> hc((size_t)tiles * 4), hi((size_t)tiles * kTcTileRows);
+    HDB_CUDA(cudaMemcpy(hc.data(), counts, hc.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    HDB_CUDA(cudaMemcpy(hi.data(), ids, hi.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int64_t t = 0; t < tiles; t++)
+      for (int j = 0; j < 2; j++)
+        for (int h2 = 0; h2 < 2; h2++) {
+          const int32_t c = hc[t * 4 + 2 * j + h2];
+          HDB_REQUIRE(c >= 0 && c <= 32, HDB_ERR_ARG, "slot count outside [0, 32]");
+          for (int s = 0; s < c; s++) {
+            const int32_t id = hi[t * kTcTileRows + 64 * j + 32 * h2 + s];
+            HDB_REQUIRE(id >= 0 && id < n, HDB_ERR_ARG, "slot id outside [0, n)");
+          }
+        }
+    bf16_distance_tiles(ctx, X, n, d, ids, counts, tiles, out);
   });
 }
 

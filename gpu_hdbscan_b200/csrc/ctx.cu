@@ -64,7 +64,10 @@ void ensure_capacity(Context *ctx, void **ptr, size_t *cap, size_t bytes) {
     *ptr = nullptr;
     *cap = 0;
   }
-  size_t want = bytes < 256 ? 256 : bytes;
+  // 25 % headroom: sizes that follow the kNN graph (edge counts) vary a little
+  // from run to run, and a re-allocation of a multi-GB buffer costs far more
+  // than the unused tail
+  size_t want = bytes < 256 ? 256 : bytes + bytes / 4;
   HDB_CUDA(cudaMalloc(ptr, want));
   *cap = want;
 }

@@ -1,0 +1,714 @@
+// BF16 local join of NN-Descent (UpdateGraph, nndescent.cu:1487-1580) on the
+// 5th-generation tensor cores.
+//
+// One tile holds two row-joins: for each of two consecutive rows of the graph,
+// its new sample at slots 0..31 and its old sample at slots 32..63 (after the
+// reference's de-duplication, ShrinkGraph :285-291 and new \ old :468-486).
+// The 128 staged BF16 rows are gathered by TMA (tile::gather4, four rows per
+// instruction, 128-byte swizzle) straight into the K-major operand layout of
+// tcgen05.mma, and one M = N = 128 MMA chain per tile computes their Gram
+// matrix G = R R^T into tensor memory (FP32).  Only the two 64 x 64 diagonal
+// blocks are read back: distance = ||a||^2 + ||c||^2 - 2 a.c with the norms of
+// the rounded rows, as in the SIMT BF16 join.
+//
+// Warp roles (192 threads, a persistent loop over tiles):
+//   warp 4      producer: sample lists, de-duplication, TMA gathers of the
+//               rows, cp.async of their norms and worst[] into the stage;
+//   warp 5      one thread issues the MMAs and commits them to mbarriers;
+//   warps 0..3  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
+//               lanes 32w..32w+31 = tile rows), row minima, candidate pushes.
+// Stages form a ring of three (full / empty mbarriers); accumulators a ring
+// of two (acc_full / acc_empty).  Every wait is bounded in time: a wait that
+// gives up sets DEVERR_TIMEOUT and makes every role of the CTA stop, after
+// which the CTA still waits (bounded) for its own copies and MMAs before it
+// frees its tensor memory and exits.
+//
+// Row minima: each distance is clamped at 0 and its float bits (order-preserving
+// for non-negative floats) have their low 6 bits replaced by the column, so one
+// unsigned min picks the closest column; the pushed distance is that value with
+// the column bits cleared.  The candidate therefore carries its distance to
+// within 2^-17 relative, and every (row, column) pair maps to one value.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "join_tc.cuh"
+
+namespace hdb {
+
+using namespace knn;
+
+namespace {
+
+constexpr int kStages = 3;
+constexpr int kKBlockBytes = kTcTileRows * 128;  // one 64-element K block of a stage
+constexpr int kAccCols = 128;                     // FP32 accumulator columns (N)
+constexpr uint32_t kTmemCols = 2 * kAccCols;
+constexpr int kEpiWarps = 4;
+constexpr int kProducerWarp = 4;
+constexpr int kMmaWarp = 5;
+constexpr int kThreads = 32 * (kEpiWarps + 2);
+constexpr uint32_t kFullArrivals = 1 + 32;          // expect_tx + one cp.async arrival per lane
+constexpr uint32_t kEmptyArrivals = 1 + kEpiWarps;  // MMA commit + epilogue warps
+constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s
+constexpr uint32_t kNoKey = 0x7F800000u;            // keys at or above: no candidate
+// Shared memory is padded to at least this size so that no more than two
+// CTAs (2 x 256 tensor-memory columns = all 512) are resident on one SM.
+constexpr size_t kMinSmem = 80 * 1024;
+
+// M = N = 128, BF16 x BF16 -> FP32, both operands K-major.
+constexpr uint32_t kIdesc = (1u << 4)                       // D format F32
+                            | (1u << 7) | (1u << 10)         // A, B format BF16
+                            | ((uint32_t)(128 >> 3) << 17)   // N / 8
+                            | ((uint32_t)(128 >> 4) << 24);  // M / 16
+
+struct StageMeta {
+  int32_t ids[kTcTileRows];
+  float nrm[kTcTileRows];  // squared norm of the staged row; +inf marks an empty column
+  float wst[kTcTileRows];  // worst[] of the slot's row: the push threshold
+  int32_t nn[2], no[2];    // per row-join: new and old rows staged
+};
+
+struct Shared {
+  StageMeta meta[kStages];
+  unsigned long long full[kStages], empty[kStages], acc_full[2], acc_empty[2];
+  uint32_t tmem_base;
+  int abort;
+};
+
+struct JoinArgs {
+  const float *nrm;
+  const int32_t *newS, *oldS;
+  const int8_t *nf, *of;
+  int32_t *nrev, *orev;
+  const float *worst;
+  Inbox ib;
+  // probe mode
+  const int32_t *probe_ids, *probe_counts;
+  float *probe_out;
+  uint32_t *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// ---- mbarriers --------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase of `bar` with the given parity.  Gives up after kWaitNs,
+// or (when `abort` is non-null) as soon as another role of the CTA gave up.
+__device__ __noinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity,
+                                       volatile int *abort) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1;; it++) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 15) == 0) {
+      if (abort && *abort) return false;
+      if (globaltimer() - t0 > kWaitNs) return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void give_up(Shared &sh, uint32_t *err) {
+  *reinterpret_cast<volatile int *>(&sh.abort) = 1;
+  atomicOr(err, DEVERR_TIMEOUT);
+}
+
+// ---- copies -----------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Four rows (r0..r3) x 64 BF16 columns starting at column x, written as four
+// consecutive 128-byte rows at dst (128-byte swizzle); completes on bar.
+__device__ __forceinline__ void tma_gather4(void *dst, const CUtensorMap *map, int32_t x,
+                                            int32_t r0, int32_t r1, int32_t r2, int32_t r3,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(r0), "r"(r1), "r"(r2), "r"(r3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ---- tensor memory and MMA ---------------------------------------------------
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory operand descriptor: K-major rows of 128 bytes, 128-byte
+// swizzle, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address
+  d |= (uint64_t)1 << 16;                            // leading byte offset (unused here)
+  d |= (uint64_t)(1024 >> 4) << 32;                  // stride byte offset
+  d |= (uint64_t)1 << 46;                            // descriptor version
+  d |= (uint64_t)2 << 61;                            // 128-byte swizzle
+  return d;
+}
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+// 32 consecutive accumulator columns of TMEM lane (warp's lane base + lane).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+// Waits for this thread's tensor-memory loads; the registers are tied to the
+// wait so that no use of them is scheduled before it.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.wait::ld.sync.aligned;"
+      : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]),
+        "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]),
+        "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]),
+        "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]),
+        "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+      :
+      : "memory");
+}
+
+// ---- producer ------------------------------------------------------------------
+// Sample lists of one row, one sample slot per lane (lane < 2S).
+struct RowLoad {
+  int32_t nid, oid;
+  int cnf, cof, cnr, cor;
+};
+
+__device__ __forceinline__ RowLoad load_row(const JoinArgs &a, int64_t row, int64_t n, int S) {
+  const int lane = lane_id();
+  RowLoad r{-1, -1, 0, 0, 0, 0};
+  if (row >= n) return r;
+  r.cnf = a.nf[row];
+  r.cof = a.of[row];
+  r.cnr = min(a.nrev[row], S);
+  r.cor = min(a.orev[row], S);
+  const int64_t sb = row * (2 * S);
+  if (lane < 2 * S) {
+    r.nid = a.newS[sb + lane];
+    r.oid = a.oldS[sb + lane];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    a.nrev[row] = 0;
+    a.orev[row] = 0;
+  }
+  return r;
+}
+
+// Fills row-join j of stage m from its sample lists: ids (de-duplicated, empty
+// slots of a partly used group of four padded with the group's first id),
+// nn / no, norms (+inf for every slot that is not a staged row) and worst[]
+// by cp.async.  Returns the number of four-row groups to gather.
+__device__ __forceinline__ int stage_join(const JoinArgs &a, const RowLoad &r, int S, int j,
+                                          StageMeta &m, int &nn_out, int &no_out) {
+  const int lane = lane_id();
+  const int base = 64 * j;
+  int32_t *ids = m.ids + base;
+  bool vn = (lane < S) ? (lane < r.cnf) : (lane < 2 * S && lane - S < r.cnr);
+  bool vo = (lane < S) ? (lane < r.cof) : (lane < 2 * S && lane - S < r.cor);
+  const int32_t nid = vn ? r.nid : -1 - lane;
+  const int32_t oid = vo ? r.oid : -100 - lane;
+  const uint32_t pn = __match_any_sync(0xffffffffu, nid);
+  vn = vn && (__ffs(pn) - 1 == lane);
+  const uint32_t po = __match_any_sync(0xffffffffu, oid);
+  vo = vo && (__ffs(po) - 1 == lane);
+  const uint32_t bo = __ballot_sync(0xffffffffu, vo);
+  int no = __popc(bo);
+  if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
+  __syncwarp();
+  for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
+  const uint32_t bn = __ballot_sync(0xffffffffu, vn);
+  int nn = __popc(bn);
+  if (vn) ids[__popc(bn & lanemask_lt())] = nid;
+  if (nn == 0 || nn + no < 2) nn = no = 0;  // nothing to compare
+  __syncwarp();
+  const int gnn = (nn + 3) & ~3, gno = (no + 3) & ~3;
+  // new slot = lane, old slot = 32 + lane
+  if (lane >= nn && lane < gnn) ids[lane] = ids[lane & ~3];
+  if (lane >= no && lane < gno) ids[32 + lane] = ids[32 + (lane & ~3)];
+  const float inf = __int_as_float(0x7f800000);
+  if (lane < nn) {
+    cp_async4(&m.nrm[base + lane], a.nrm + ids[lane]);
+    cp_async4(&m.wst[base + lane], a.worst + ids[lane]);
+  } else {
+    m.nrm[base + lane] = inf;
+  }
+  if (lane < no) {
+    cp_async4(&m.nrm[base + 32 + lane], a.nrm + ids[32 + lane]);
+    cp_async4(&m.wst[base + 32 + lane], a.worst + ids[32 + lane]);
+  } else {
+    m.nrm[base + 32 + lane] = inf;
+  }
+  if (lane == 0) {
+    m.nn[j] = nn;
+    m.no[j] = no;
+  }
+  nn_out = nn;
+  no_out = no;
+  return (gnn + gno) >> 2;
+}
+
+// Probe form of stage_join: the slot lists are given.
+__device__ __forceinline__ int stage_probe(const JoinArgs &a, int64_t t, int j, StageMeta &m,
+                                           int &nn_out, int &no_out) {
+  const int lane = lane_id();
+  const int base = 64 * j;
+  const int nn = a.probe_counts[t * 4 + 2 * j], no = a.probe_counts[t * 4 + 2 * j + 1];
+  const int32_t *src = a.probe_ids + t * kTcTileRows + base;
+  const int gnn = (nn + 3) & ~3, gno = (no + 3) & ~3;
+  const float inf = __int_as_float(0x7f800000);
+  int32_t idn = src[lane < nn ? lane : (lane & ~3)];
+  int32_t ido = src[32 + (lane < no ? lane : (lane & ~3))];
+  if (lane < gnn) m.ids[base + lane] = idn;
+  if (lane < gno) m.ids[base + 32 + lane] = ido;
+  if (lane < nn) cp_async4(&m.nrm[base + lane], a.nrm + idn); else m.nrm[base + lane] = inf;
+  if (lane < no) cp_async4(&m.nrm[base + 32 + lane], a.nrm + ido); else m.nrm[base + 32 + lane] = inf;
+  m.wst[base + lane] = inf;
+  m.wst[base + 32 + lane] = inf;
+  if (lane == 0) {
+    m.nn[j] = nn;
+    m.no[j] = no;
+  }
+  nn_out = nn;
+  no_out = no;
+  return (gnn + gno) >> 2;
+}
+
+template <bool kProbe>
+__device__ void producer(const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
+                         unsigned char *tiles, int64_t n, int64_t ntiles, int kbc, int S,
+                         unsigned long long &rows_staged) {
+  const int lane = lane_id();
+  uint32_t armed = 0;  // stages armed so far (phase bookkeeping for the drain)
+  int64_t t = blockIdx.x;
+  RowLoad cur[2], nxt[2];
+  if (!kProbe && t < ntiles) {
+    cur[0] = load_row(a, 2 * t, n, S);
+    cur[1] = load_row(a, 2 * t + 1, n, S);
+  }
+  for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
+    const int s = i % kStages;
+    const uint32_t use = i / kStages;
+    if (!mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort)) {
+      give_up(sh, a.err);
+      break;
+    }
+    StageMeta &m = sh.meta[s];
+    int nn[2], no[2], groups;
+    if (kProbe) {
+      groups = stage_probe(a, t, 0, m, nn[0], no[0]);
+      groups += stage_probe(a, t, 1, m, nn[1], no[1]);
+    } else {
+      groups = stage_join(a, cur[0], S, 0, m, nn[0], no[0]);
+      groups += stage_join(a, cur[1], S, 1, m, nn[1], no[1]);
+      // next tile's sample lists, in flight while this one is gathered
+      const int64_t tn = t + gridDim.x;
+      if (tn < ntiles) {
+        nxt[0] = load_row(a, 2 * tn, n, S);
+        nxt[1] = load_row(a, 2 * tn + 1, n, S);
+      }
+    }
+    rows_staged += nn[0] + no[0] + nn[1] + no[1];
+    __syncwarp();
+    if (lane == 0) mbar_arrive_tx(&sh.full[s], (uint32_t)groups * kbc * 512u);
+    __syncwarp();
+    {
+      // lane g: four-row group g & 15 of row-join g >> 4 (new groups 0..7,
+      // old groups 8..15)
+      const int j = lane >> 4, q = lane & 15;
+      const bool oldg = q >= 8;
+      const int slot = oldg ? 32 + 4 * (q - 8) : 4 * q;
+      const int cnt = oldg ? no[j] : nn[j];
+      if (4 * (q & 7) < cnt) {
+        const int32_t *gi = m.ids + 64 * j + slot;
+        for (int kb = 0; kb < kbc; kb++) {
+          unsigned char *dst = tiles + ((size_t)s * kbc + kb) * kKBlockBytes + (64 * j + slot) * 128;
+          tma_gather4(dst, xmap, kb * kTcKBlock, gi[0], gi[1], gi[2], gi[3], &sh.full[s]);
+        }
+      }
+    }
+    cp_async_arrive_noinc(&sh.full[s]);
+    armed = i + 1;
+    if (!kProbe) {
+      cur[0] = nxt[0];
+      cur[1] = nxt[1];
+    }
+  }
+  // drain: the copies of the last armed use of every stage have landed
+  for (int s = 0; s < kStages; s++) {
+    if ((uint32_t)s >= armed) break;
+    const uint32_t last = (armed - 1 - s) / kStages;  // last use of stage s
+    if (!mbar_wait(&sh.full[s], last & 1, nullptr)) atomicOr(a.err, DEVERR_TIMEOUT);
+  }
+}
+
+__device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int64_t ntiles,
+                           int kbc, uint32_t *err) {
+  int64_t t = blockIdx.x;
+  int last_b = -1;
+  uint32_t last_parity = 0;
+  for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
+    const int s = i % kStages;
+    const uint32_t use = i / kStages;
+    const int b = i & 1;
+    const uint32_t ub = i >> 1;
+    if (!mbar_wait(&sh.acc_empty[b], (ub & 1) ^ 1, &sh.abort)) {
+      give_up(sh, err);
+      break;
+    }
+    tc_fence_after();
+    if (!mbar_wait(&sh.full[s], use & 1, &sh.abort)) {
+      give_up(sh, err);
+      break;
+    }
+    tc_fence_after();
+    const uint32_t d = tmem + (uint32_t)(b * kAccCols);
+    for (int kb = 0; kb < kbc; kb++) {
+      const uint32_t base = smem_u32(tiles + ((size_t)s * kbc + kb) * kKBlockBytes);
+#pragma unroll
+      for (int kk = 0; kk < kTcKBlock / 16; kk++) {
+        const uint64_t desc = sw128_desc(base + 32u * kk);
+        tc_mma(d, desc, desc, (kb | kk) != 0 ? 1u : 0u);
+      }
+    }
+    tc_commit(&sh.acc_full[b]);
+    tc_commit(&sh.empty[s]);
+    last_b = b;
+    last_parity = ub & 1;
+  }
+  // drain: the last MMA chain has completed before tensor memory is freed
+  if (last_b >= 0 && !mbar_wait(&sh.acc_full[last_b], last_parity, nullptr))
+    atomicOr(err, DEVERR_TIMEOUT);
+}
+
+// A push whose inbox slot was claimed; the store waits for the next tile so
+// that the atomic's round trip overlaps it.
+struct PendingPush {
+  int32_t target;
+  int32_t slot;  // -1: none
+  uint64_t key;
+};
+
+__device__ __forceinline__ void finish_push(PendingPush &p, const Inbox &ib) {
+  if (p.slot < 0) return;
+  if (p.slot < kInboxCap) {
+    ib.slots[(int64_t)p.target * kInboxCap + p.slot] = p.key;
+  } else {
+    unsigned long long pos = atomicAdd(&ib.counters[3], 1ull);
+    if ((int64_t)pos < ib.ovf_cap) {
+      ib.ovf_tgt[pos] = (uint32_t)p.target;
+      ib.ovf_key[pos] = p.key;
+    } else {
+      atomicMin(&ib.best[p.target], (unsigned long long)p.key);
+      atomicAdd(&ib.counters[0], 1ull);
+    }
+  }
+  p.slot = -1;
+}
+
+__device__ __forceinline__ int start_push(PendingPush &p, int32_t target, int32_t cand,
+                                          uint32_t dbits, float wst, const Inbox &ib) {
+  const float dist = __uint_as_float(dbits);
+  if (!(dist < wst)) return 0;  // cannot enter the target's list
+  p.target = target;
+  p.key = pack(dist, cand);
+  p.slot = atomicAdd(&ib.cnt[target], 1);
+  return 1;
+}
+
+// Row minimum over 32 columns: key = clamped distance bits with the column in
+// the low 6 bits (skip_col: the row's own column, or -1).
+__device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const float *cn, float na,
+                                              int skip_col) {
+  uint32_t best = 0xffffffffu;
+#pragma unroll
+  for (int c4 = 0; c4 < 8; c4++) {
+    const float4 nc = reinterpret_cast<const float4 *>(cn)[c4];
+    const float ncs[4] = {nc.x, nc.y, nc.z, nc.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int c = 4 * c4 + e;
+      float dd = __fmaf_rn(-2.0f, __uint_as_float(v[c]), __fadd_rn(na, ncs[e]));
+      dd = dd < 0.0f ? 0.0f : dd;
+      uint32_t key = (__float_as_uint(dd) & ~63u) | (uint32_t)c;
+      key = c == skip_col ? 0xffffffffu : key;
+      best = key < best ? key : best;
+    }
+  }
+  return best;
+}
+
+template <bool kProbe>
+__device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t ntiles,
+                         unsigned long long &cands) {
+  const int w = threadIdx.x >> 5, lane = lane_id();
+  const int j = w >> 1;                 // row-join of this warp's 32 rows
+  const bool isnew = (w & 1) == 0;      // new rows (slots 0..31) or old rows (32..63)
+  const int slot = (isnew ? 0 : 32) + lane;
+  PendingPush p0{0, -1, 0}, p1{0, -1, 0};
+  int64_t t = blockIdx.x;
+  for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
+    const int s = i % kStages;
+    const uint32_t use = i / kStages;
+    const int b = i & 1;
+    const uint32_t ub = i >> 1;
+    if (!mbar_wait(&sh.full[s], use & 1, &sh.abort)) {
+      give_up(sh, a.err);
+      break;
+    }
+    const StageMeta &M = sh.meta[s];
+    const int nn = M.nn[j], no = M.no[j];
+    const bool vrow = isnew ? lane < nn : lane < no;
+    const int32_t myid = M.ids[64 * j + slot];
+    const float na = M.nrm[64 * j + slot];
+    const float wst = M.wst[64 * j + slot];
+    if (!mbar_wait(&sh.acc_full[b], ub & 1, &sh.abort)) {
+      give_up(sh, a.err);
+      break;
+    }
+    tc_fence_after();
+    uint32_t v0[32], v1[32];
+    const uint32_t taddr = tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(b * kAccCols + 64 * j);
+    tmem_ld32(taddr, v0);
+    tmem_wait_ld(v0);
+    if (kProbe || isnew) {
+      tmem_ld32(taddr + 32, v1);
+      tmem_wait_ld(v1);
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh.acc_empty[b]);
+    const float *cn = M.nrm + 64 * j;
+    if (kProbe) {
+      float *o = a.probe_out + ((size_t)t * kTcTileRows + 64 * j + slot) * 64;
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        o[c] = __fmaf_rn(-2.0f, __uint_as_float(v0[c]), __fadd_rn(na, cn[c]));
+        o[32 + c] = __fmaf_rn(-2.0f, __uint_as_float(v1[c]), __fadd_rn(na, cn[32 + c]));
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.empty[s]);
+      continue;
+    }
+    // the previous tile's claimed slots: their atomics have returned by now
+    finish_push(p0, a.ib);
+    finish_push(p1, a.ib);
+    uint32_t k1, k2 = 0xffffffffu;
+    int32_t id1 = -1, id2 = -1;
+    if (isnew) {
+      k1 = row_min32(v0, cn, na, lane);       // closest other new row
+      k2 = row_min32(v1, cn + 32, na, -1);    // closest old row
+      if (k2 < kNoKey) id2 = M.ids[64 * j + 32 + (k2 & 63u)];
+    } else {
+      k1 = row_min32(v0, cn, na, -1);         // closest new row
+    }
+    if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh.empty[s]);
+    if (vrow) {
+      if (id1 >= 0) cands += start_push(p0, myid, id1, k1 & ~63u, wst, a.ib);
+      if (id2 >= 0) cands += start_push(p1, myid, id2, k2 & ~63u, wst, a.ib);
+    }
+  }
+  if (!kProbe) {
+    finish_push(p0, a.ib);
+    finish_push(p1, a.ib);
+  }
+}
+
+template <bool kProbe>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_join_tc(const __grid_constant__ CUtensorMap xmap, int64_t n, int64_t ntiles, int kbc, int S,
+              JoinArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  // the swizzled operand tiles start on a 1024-byte boundary of shared memory
+  unsigned char *tiles = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  Shared &sh = *reinterpret_cast<Shared *>(tiles + (size_t)kStages * kbc * kKBlockBytes);
+  const int warp = threadIdx.x >> 5;
+  // stale columns of a stage must hold finite values: start from zeros
+  {
+    uint4 *z = reinterpret_cast<uint4 *>(tiles);
+    const int nz = kStages * kbc * kKBlockBytes / 16;
+    for (int i = threadIdx.x; i < nz; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&sh.full[s], kFullArrivals);
+      mbar_init(&sh.empty[s], kEmptyArrivals);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&sh.acc_full[b], 1);
+      mbar_init(&sh.acc_empty[b], kEpiWarps);
+    }
+    sh.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&sh.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem_base;
+  unsigned long long stat = 0;
+  if (warp == kProducerWarp) {
+    producer<kProbe>(&xmap, a, sh, tiles, n, ntiles, kbc, S, stat);
+    if (!kProbe && lane_id() == 0 && stat) atomicAdd(&a.ib.counters[1], stat);
+  } else if (warp == kMmaWarp) {
+    if (lane_id() == 0) mma_issuer(sh, tiles, tmem, ntiles, kbc, a.err);
+    __syncwarp();
+  } else {
+    epilogue<kProbe>(a, sh, tmem, ntiles, stat);
+    if (!kProbe) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) stat += __shfl_xor_sync(0xffffffffu, stat, o);
+      if (lane_id() == 0 && stat) atomicAdd(&a.ib.counters[2], stat);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ---- host ----------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+size_t smem_bytes(int kbc) {
+  size_t b = 1024 + (size_t)kStages * kbc * kKBlockBytes + sizeof(Shared);
+  return b < kMinSmem ? kMinSmem : b;
+}
+
+template <bool kProbe>
+void launch(Context *ctx, const TcJoin &tj, int64_t ntiles, int S, const JoinArgs &a) {
+  const int kbc = tj.dpad / kTcKBlock;
+  HDB_CUDA(cudaFuncSetAttribute(k_join_tc<kProbe>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(kTcMaxDpad / kTcKBlock)));
+  const int64_t g = std::min<int64_t>(ntiles, 2 * (int64_t)ctx->num_sms);
+  if (g <= 0) return;
+  k_join_tc<kProbe><<<(int)g, kThreads, tj.smem, ctx->stream>>>(tj.xmap, tj.n, ntiles, kbc, S, a);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad, TcJoin *tj) {
+  HDB_REQUIRE(dpad % kTcKBlock == 0 && dpad >= kTcKBlock && dpad <= kTcMaxDpad, HDB_ERR_ARG,
+              "tensor-core join: padded dimension must be a multiple of 64 in [64, 256]");
+  HDB_REQUIRE(n >= 1 && n < (int64_t(1) << 31), HDB_ERR_ARG, "tensor-core join: bad row count");
+  HDB_REQUIRE((reinterpret_cast<uintptr_t>(Xb) & 15) == 0, HDB_ERR_INTERNAL,
+              "tensor-core join: rows not 16-byte aligned");
+  auto fn = encode_tiled();
+  HDB_REQUIRE(fn != nullptr, HDB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  cuuint64_t gdim[2] = {(cuuint64_t)dpad, (cuuint64_t)n};
+  cuuint64_t gstride[1] = {(cuuint64_t)dpad * sizeof(__nv_bfloat16)};
+  cuuint32_t box[2] = {(cuuint32_t)kTcKBlock, 1};  // one row high (gather4)
+  cuuint32_t estride[2] = {1, 1};
+  CUresult r = fn(&tj->xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(Xb),
+                  gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  HDB_REQUIRE(r == CUDA_SUCCESS, HDB_ERR_CUDA,
+              "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  tj->n = n;
+  tj->dpad = dpad;
+  tj->smem = smem_bytes(dpad / kTcKBlock);
+  (void)ctx;
+}
+
+void tc_join_launch(Context *ctx, const TcJoin &tj, int S, const float *nrm, const int32_t *newS,
+                    const int32_t *oldS, const int8_t *nf, const int8_t *of, int32_t *nrev,
+                    int32_t *orev, const float *worst, const Inbox &ib) {
+  HDB_REQUIRE(S >= 1 && 2 * S <= 32, HDB_ERR_ARG, "tensor-core join: need 2 * SAMPLE_NUM <= 32");
+  JoinArgs a{nrm, newS, oldS, nf, of, nrev, orev, worst, ib, nullptr, nullptr, nullptr, ctx->dev_err};
+  launch<false>(ctx, tj, (tj.n + 1) / 2, S, a);
+}
+
+void tc_gram_probe(Context *ctx, const __nv_bfloat16 *Xb, const float *nrm, int64_t n, int dpad,
+                   const int32_t *ids, const int32_t *counts, int64_t tiles, float *out) {
+  TcJoin tj;
+  tc_join_prepare(ctx, Xb, n, dpad, &tj);
+  JoinArgs a{nrm,     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+             Inbox{}, ids,     counts,  out,     ctx->dev_err};
+  launch<true>(ctx, tj, tiles, 1, a);
+}
+
+}  // namespace hdb

@@ -19,14 +19,16 @@
 #include <vector>
 
 #include "hdb_internal.cuh"
+#include "join_tc.cuh"
 #include "knn.cuh"
+#include "knn_common.cuh"
 
 namespace hdb {
 
+using namespace knn;
+
 namespace {
 
-constexpr int kMaxK = 32;
-constexpr int kInboxCap = 127;  // + 1 overflow slot = 128 sorted candidates per merge
 constexpr int kMergeSlots = 128;
 
 __host__ __device__ __forceinline__ uint64_t xorshift64star(uint64_t x) {
@@ -38,23 +40,6 @@ __host__ __device__ __forceinline__ uint64_t xorshift64star(uint64_t x) {
   return x * 0x2545F4914F6CDD1DULL;
 }
 
-__device__ __forceinline__ uint64_t pack(float d, int32_t id) {
-  return ((uint64_t)__float_as_uint(d) << 32) | (uint32_t)id;
-}
-__device__ __forceinline__ float pk_dist(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
-__device__ __forceinline__ int32_t pk_id(uint64_t k) { return (int32_t)(uint32_t)k; }
-
-__device__ __forceinline__ int32_t decode(int32_t label) { return label >= 0 ? label : -label - 1; }
-
-// Sequential FP32 difference sum (nndescent.cu:1086-1093).
-__device__ __forceinline__ float diffsum(const float *a, const float *b, int d) {
-  float s = 0.0f;
-  for (int j = 0; j < d; j++) {
-    float df = __fsub_rn(a[j], b[j]);
-    s = __fmaf_rn(df, df, s);
-  }
-  return s;
-}
 
 // Ascending bitonic sort of one u64 per lane across the warp.
 __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
@@ -93,11 +78,54 @@ __device__ __forceinline__ void warp_sort_smem(uint64_t *s, int size) {
 }
 
 // ---------------------------------------------------------------------------
+// Exact sequential difference sums of one row against up to 32 other rows,
+// one per lane.  The 32 rows are staged through shared memory 32 dimensions
+// at a time, read as coalesced row segments (lanes on consecutive columns),
+// and each lane then walks its own row's staged segment in dimension order:
+// the reference's sequential FP32 difference sum (nndescent.cu:1086-1093),
+// sum = fmaf(a_j - b_j, a_j - b_j, sum) for j = 0..d-1.
+constexpr int kStageCols = 32;
+constexpr int kStageLd = kStageCols + 1;                  // conflict-free column walk
+constexpr int kStageFloats = kStageCols + 32 * kStageLd;  // own segment + 32 rows
+
+__device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int d, int64_t row,
+                                                int32_t id, bool active, float *__restrict__ sm) {
+  const int lane = lane_id();
+  float *own = sm;
+  float *nb = sm + kStageCols;
+  const uint32_t act = __ballot_sync(0xffffffffu, active);
+  float s = 0.0f;
+  for (int c0 = 0; c0 < d; c0 += kStageCols) {
+    const int w = min(kStageCols, d - c0);
+    __syncwarp();
+    if (lane < w) own[lane] = X[row * d + c0 + lane];
+    // 32 rows x w columns, flattened: element e -> row e / w, column e % w
+#pragma unroll 8
+    for (int i = 0; i < w; i++) {
+      const int e = i * 32 + lane;
+      const int r = e / w, c = e - r * w;
+      const int32_t rid = __shfl_sync(0xffffffffu, id, r);
+      if ((act >> r) & 1u) nb[r * kStageLd + c] = __ldg(X + (int64_t)rid * d + c0 + c);
+    }
+    __syncwarp();
+    if (active) {
+      const float *mine = nb + lane * kStageLd;
+      for (int j = 0; j < w; j++) {
+        float df = __fsub_rn(own[j], mine[j]);
+        s = __fmaf_rn(df, df, s);
+      }
+    }
+  }
+  return s;
+}
+
 __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
                        int32_t *__restrict__ gid, float *__restrict__ gdist,
                        float *__restrict__ worst) {
+  extern __shared__ float smem_stage[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
+  float *sm = smem_stage + (threadIdx.x >> 5) * kStageFloats;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     // InitKNNGraphIndexKernel (nndescent.cu:1673-1692): xorshift64star(pos) % n,
@@ -111,8 +139,9 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
         if (lane == t) label = (label + 1) % n;
       }
     }
+    const float ds = diffsum_staged(X, d, row, (int32_t)label, lane < k, sm);
     uint64_t key = ~0ull;
-    if (lane < k) key = pack(diffsum(X + row * d, X + label * d, d), (int32_t)label);
+    if (lane < k) key = pack(ds, (int32_t)label);
     key = warp_sort32(key);
     if (lane < k) {
       gid[row * k + lane] = pk_id(key);  // all "new"
@@ -126,22 +155,6 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
 // Per-warp shared memory of a merge: 128 sorted candidates, then the k output
 // keys and labels.
 constexpr int kMergeSmemU64 = kMergeSlots + kMaxK + kMaxK / 2;
-
-// Where the join leaves its candidates: a fixed inbox per row, then a global
-// overflow list (radix-sorted by target row between the join and the merge).
-// Only when the overflow list is full is a candidate dropped; the best
-// dropped one per row is still kept in `best`.
-struct Inbox {
-  int32_t *cnt;                  // [n] candidates offered this iteration
-  uint64_t *slots;               // [n * kInboxCap] packed (distance, id)
-  unsigned long long *best;      // [n]
-  uint32_t *ovf_tgt;             // [ovf_cap] overflow: target row (sorted in place)
-  uint64_t *ovf_key;             // [ovf_cap] overflow: packed candidate
-  uint32_t *ovf_idx;             // [ovf_cap] overflow: permutation from the sort
-  uint32_t *ostart, *oend;       // [n] segment of each row in the sorted overflow list
-  unsigned long long *counters;  // [0] dropped [1] rows gathered [2] candidates [3] overflow
-  int64_t ovf_cap;
-};
 
 // Sorts the 128 candidates in sk, drops duplicates and ids already in the
 // row, and merges the rest into the row held one entry per lane (lane < k).
@@ -318,26 +331,6 @@ struct JoinSmem {
   static constexpr int kIds = 64;
   __host__ __device__ static int floats(int dp) { return 2 * kBest + kIds + 64 * dp + 2; }
 };
-
-__device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
-                                              const float *__restrict__ worst, const Inbox &ib) {
-  if (!(d < worst[target])) return 0;  // cannot enter the target's list
-  int slot = atomicAdd(&ib.cnt[target], 1);
-  uint64_t key = pack(d, id);
-  if (slot < kInboxCap) {
-    ib.slots[(int64_t)target * kInboxCap + slot] = key;
-  } else {
-    unsigned long long pos = atomicAdd(&ib.counters[3], 1ull);
-    if ((int64_t)pos < ib.ovf_cap) {
-      ib.ovf_tgt[pos] = (uint32_t)target;
-      ib.ovf_key[pos] = key;
-    } else {
-      atomicMin(&ib.best[target], (unsigned long long)key);
-      atomicAdd(&ib.counters[0], 1ull);
-    }
-  }
-  return 1;
-}
 
 // Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).  The
 // sampled rows are staged in shared memory (new rows at slots 0..31, old rows
@@ -731,18 +724,17 @@ __global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restri
 // id); old/new flags travel with their ids.
 __global__ void k_rerank(const float *__restrict__ X, int64_t n, int d, int k,
                          hdb_nnd_element *__restrict__ G) {
+  extern __shared__ float smem_stage[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
+  float *sm = smem_stage + (threadIdx.x >> 5) * kStageFloats;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
-    uint64_t key = ~0ull;
     int32_t lab = 0;
-    if (lane < k) {
-      hdb_nnd_element e = G[row * k + lane];
-      lab = e.label_;
-      const int32_t id = decode(lab);
-      key = pack(diffsum(X + row * d, X + (int64_t)id * d, d), id);
-    }
+    if (lane < k) lab = G[row * k + lane].label_;
+    const int32_t id = decode(lab);
+    const float ds = diffsum_staged(X, d, row, id, lane < k, sm);
+    const uint64_t key = lane < k ? pack(ds, id) : ~0ull;
     const uint64_t sorted = warp_sort32(key);
     const int32_t sid = pk_id(sorted);
     int32_t slab = sid;
@@ -871,7 +863,8 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
 
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
-  k_init<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, gid, gdist, worst); ctx->launches++;
+  const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, gid, gdist, worst); ctx->launches++;
   HDB_CHECK_LAUNCH();
   const size_t smem_sample = (size_t)wpb * kMergeSmemU64 * sizeof(uint64_t);
   const int dp = (d & 1) ? d : d + 1;
@@ -883,35 +876,47 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
   const int grid_join = grid_for(ctx, n, jw, 64);
   const bool bf16 = p.precision == HDB_PREC_BF16;
-  const int dpad = (d + 15) & ~15;
+  // BF16 form: the tensor-core tile pipeline (tcgen05) up to 256 padded
+  // dimensions, the mma.sync join beyond
+  const bool use_tc = bf16 && tc_dpad(d) <= kTcMaxDpad;
+  const int dpad = use_tc ? tc_dpad(d) : (d + 15) & ~15;
   Buf<__nv_bfloat16> Xb;
   Buf<float> nrm;
   int jw16 = 4;
   size_t smem_bf = 0;
   int grid_bf = 0;
+  TcJoin tj;
   if (bf16) {
     Xb = Buf<__nv_bfloat16>(ctx, (size_t)n * dpad);
     nrm = Buf<float>(ctx, n);
     k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, Xb, nrm); ctx->launches++;
     HDB_CHECK_LAUNCH();
-    smem_bf = JoinSmemBf16::bytes(dpad) * jw16;
-    HDB_REQUIRE(smem_bf <= 227 * 1024, HDB_ERR_ARG, "NN-Descent BF16: d too large for the join tile");
-    HDB_CUDA(cudaFuncSetAttribute(k_join_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_bf));
-    grid_bf = grid_for(ctx, n, jw16, 64);
+    if (use_tc) {
+      tc_join_prepare(ctx, Xb, n, dpad, &tj);
+    } else {
+      smem_bf = JoinSmemBf16::bytes(dpad) * jw16;
+      HDB_REQUIRE(smem_bf <= 227 * 1024, HDB_ERR_ARG, "NN-Descent BF16: d too large for the join tile");
+      HDB_CUDA(cudaFuncSetAttribute(k_join_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_bf));
+      grid_bf = grid_for(ctx, n, jw16, 64);
+    }
   }
   for (int it = 0; it < p.iterations; it++) {
     k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
                                                        newS, oldS, nf, of, nrev, orev); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
-    if (bf16)
-      k_join_bf16<<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, newS, oldS, nf, of, nrev,
-                                                       orev, worst, ib);
-    else
-      k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev, worst,
-                                                    ib);
-    ctx->launches++;
+    if (use_tc) {
+      tc_join_launch(ctx, tj, S, nrm, newS, oldS, nf, of, nrev, orev, worst, ib);
+    } else {
+      if (bf16)
+        k_join_bf16<<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, newS, oldS, nf, of,
+                                                         nrev, orev, worst, ib);
+      else
+        k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev,
+                                                      worst, ib);
+      ctx->launches++;
+    }
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
     HDB_CHECK_LAUNCH();
     sort_overflow(ctx, ib, n);
@@ -920,12 +925,15 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (bf16) {
-    k_rerank<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, k, G); ctx->launches++;
+    k_rerank<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, G); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   ctx->sync();
+  if (use_tc)
+    HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_TIMEOUT), HDB_ERR_TIMEOUT,
+                "NN-Descent: a wait of the tensor-core join pipeline gave up");
   const int64_t *hs = static_cast<const int64_t *>(ctx->pinned);
   if (dropped_out) *dropped_out = hs[0];
   if (js) {
@@ -940,6 +948,24 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     }
     for (auto &e : jev) cudaEventDestroy(e);
   }
+}
+
+void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
+                         const int32_t *counts, int64_t tiles, float *out) {
+  HDB_REQUIRE(n >= 1 && n < (int64_t(1) << 31) && d >= 1 && tc_dpad(d) <= kTcMaxDpad, HDB_ERR_ARG,
+              "BF16 distance tiles: need 1 <= n < 2^31 and 1 <= d <= 256");
+  HDB_REQUIRE(tiles >= 0, HDB_ERR_ARG, "BF16 distance tiles: negative tile count");
+  if (tiles == 0) return;
+  const int dpad = tc_dpad(d);
+  Buf<__nv_bfloat16> Xb(ctx, (size_t)n * dpad);
+  Buf<float> nrm(ctx, n);
+  k_bf16_prepare<<<grid_for(ctx, n, 8, 16), 256, 0, ctx->stream>>>(X, n, d, dpad, Xb, nrm);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  tc_gram_probe(ctx, Xb, nrm, n, dpad, ids, counts, tiles, out);
+  ctx->sync();
+  HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_TIMEOUT), HDB_ERR_TIMEOUT,
+              "BF16 distance tiles: a pipeline wait gave up");
 }
 
 void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,

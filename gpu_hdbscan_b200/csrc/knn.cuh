@@ -13,6 +13,9 @@ struct JoinStats {
 
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr);
+// BF16 tensor-core distances for explicit slot lists (hdb_bf16_distance_tiles).
+void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
+                         const int32_t *counts, int64_t tiles, float *out);
 void knn_split(Context *ctx, const hdb_nnd_element *G, int64_t n, int32_t k, int32_t *ids,
                float *dist);
 void fix_distances(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,

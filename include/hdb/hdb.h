@@ -186,6 +186,22 @@ HDB_API hdb_status hdb_run_knn(hdb_ctx *ctx, const hdb_nnd_element *G, const flo
                                int32_t d, const hdb_params *params, int32_t *labels,
                                hdb_run_stats *stats);
 
+/* hdb_bf16_distance_tiles -- a diagnostic with no counterpart in the
+ * reference: the distances the BF16 tensor-core local join of hdb_nndescent
+ * computes, for given slot lists instead of NN-Descent's samples.  Tile t
+ * stages two row-joins j = 0, 1 of 64 slots each (ids[t*128 + 64*j + s]):
+ * "new" slots s = 0..31, of which the first counts[t*4 + 2*j] are used, and
+ * "old" slots s = 32..63, of which the first counts[t*4 + 2*j + 1] are used.
+ * out[(t*128 + 64*j + r) * 64 + c] = |x_a|^2 + |x_b|^2 - 2 x_a.x_b for the
+ * rows a, b in slots r and c of row-join j, with x rounded to BF16 and FP32
+ * norms and accumulation (no clamp at 0); +inf where slot c is unused.  Rows
+ * in unused slots r carry unspecified values.  X [n, d] (d <= 256), ids,
+ * counts and out are device memory; counts must lie in [0, 32] and used ids
+ * in [0, n) (both are checked, HDB_ERR_ARG). */
+HDB_API hdb_status hdb_bf16_distance_tiles(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
+                                           const int32_t *ids, const int32_t *counts,
+                                           int64_t tiles, float *out);
+
 /* hdb_sort_edges_noalloc -- no counterpart in the reference.  The same
  * stable ascending sort by weight as hdb_sort_edges, for callers that cannot
  * call cudaMalloc (a host framework that owns every device byte, or a device
