@@ -145,27 +145,29 @@ __global__ void k_compact_flags(const int32_t *__restrict__ flag, const int64_t 
 __global__ void k_mutual(const int32_t *__restrict__ ids, int64_t n, int k,
                          uint32_t *__restrict__ mutual, int32_t *__restrict__ revcnt,
                          int32_t *__restrict__ nonmutual) {
+  // One warp per row: neighbour t's list is read as one coalesced segment
+  // (lane = position), eight lists in flight at a time, and a vote tells
+  // whether the row is in it.
   const int lane = lane_id();
   int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
   for (; row < n; row += stride) {
-    bool found = false;
-    int32_t v = -1;
-    if (lane < k) {
-      v = ids[row * k + lane];
-      const int32_t *r = ids + (int64_t)v * k;
-      if ((k & 3) == 0) {
-        const int4 *r4 = reinterpret_cast<const int4 *>(r);
-        for (int t = 0; t < (k >> 2); t++) {
-          int4 q = __ldg(r4 + t);
-          found |= (q.x == row) | (q.y == row) | (q.z == row) | (q.w == row);
-        }
-      } else {
-        for (int t = 0; t < k; t++) found |= (__ldg(r + t) == row);
+    const int32_t v = lane < k ? ids[row * k + lane] : 0;
+    uint32_t m = 0;
+    for (int t0 = 0; t0 < k; t0 += 8) {
+      int32_t x[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int t = t0 + u;
+        const int32_t vt = __shfl_sync(0xffffffffu, v, t & 31);
+        x[u] = (t < k && lane < k) ? __ldg(ids + (int64_t)vt * k + lane) : -1;
       }
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+        if (__any_sync(0xffffffffu, x[u] == (int32_t)row)) m |= 1u << (t0 + u);
     }
-    uint32_t m = __ballot_sync(0xffffffffu, found);
-    if (lane < k && !found) atomicAdd(&revcnt[v], 1);
+    if (k < 32) m &= (1u << k) - 1u;
+    if (lane < k && !((m >> lane) & 1u)) atomicAdd(&revcnt[v], 1);
     if (lane == 0) {
       mutual[row] = m;
       nonmutual[row] = k - __popc(m);

@@ -2,26 +2,31 @@
 // 5th-generation tensor cores.
 //
 // One tile holds two row-joins: for each of two consecutive rows of the graph,
-// its new sample at slots 0..31 and its old sample at slots 32..63 (after the
-// reference's de-duplication, ShrinkGraph :285-291 and new \ old :468-486).
-// The 128 staged BF16 rows are gathered by TMA (tile::gather4, four rows per
-// instruction, 128-byte swizzle) straight into the K-major operand layout of
-// tcgen05.mma, and one M = N = 128 MMA chain per tile computes their Gram
-// matrix G = R R^T into tensor memory (FP32).  Only the two 64 x 64 diagonal
-// blocks are read back: distance = ||a||^2 + ||c||^2 - 2 a.c with the norms of
-// the rounded rows, as in the SIMT BF16 join.
+// its new sample at slots 0..31 and its old sample at slots 32..63, as
+// compacted beforehand by k_join_lists (the reference's de-duplication,
+// ShrinkGraph :285-291, and new \ old, :468-486).  The staged BF16 rows are
+// gathered by TMA (tile::gather4, four rows per instruction, 128-byte
+// swizzle) straight into the K-major operand layout of tcgen05.mma, and one
+// M = N = 128 MMA chain per tile computes their Gram matrix G = R R^T into
+// tensor memory (FP32).  Only the two 64 x 64 diagonal blocks are read back:
+// distance = ||a||^2 + ||c||^2 - 2 a.c with the norms of the rounded rows, as
+// in the SIMT BF16 join.
 //
-// Warp roles (192 threads, a persistent loop over tiles):
-//   warp 4      producer: sample lists, de-duplication, TMA gathers of the
-//               rows, cp.async of their norms and worst[] into the stage;
-//   warp 5      one thread issues the MMAs and commits them to mbarriers;
+// Warp roles (224 threads, a persistent loop over tiles):
+//   warps 4, 5  producers (alternate tiles): slot lists, TMA gathers of the
+//               rows, cp.async of their norms and worst[] into the stage; a
+//               TMA gather occupies its issuing warp for a while, so two
+//               warps keep more gathers in flight;
+//   warp 6      one thread issues the MMAs and commits them to mbarriers;
 //   warps 0..3  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
 //               lanes 32w..32w+31 = tile rows), row minima, candidate pushes.
 // Stages form a ring of three (full / empty mbarriers); accumulators a ring
 // of two (acc_full / acc_empty).  Every wait is bounded in time: a wait that
 // gives up sets DEVERR_TIMEOUT and makes every role of the CTA stop, after
 // which the CTA still waits (bounded) for its own copies and MMAs before it
-// frees its tensor memory and exits.
+// frees its tensor memory and exits.  tcgen05.ld / alloc are .sync.aligned:
+// the warp is reconverged with __syncwarp() right before each, because the
+// code ahead of them branches per lane.
 //
 // Row minima: each distance is clamped at 0 and its float bits (order-preserving
 // for non-negative floats) have their low 6 bits replaced by the column, so one
@@ -47,9 +52,10 @@ constexpr int kKBlockBytes = kTcTileRows * 128;  // one 64-element K block of a 
 constexpr int kAccCols = 128;                     // FP32 accumulator columns (N)
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kEpiWarps = 4;
-constexpr int kProducerWarp = 4;
-constexpr int kMmaWarp = 5;
-constexpr int kThreads = 32 * (kEpiWarps + 2);
+constexpr int kProducers = 2;  // producer warps, alternating tiles
+constexpr int kProducerWarp0 = kEpiWarps;
+constexpr int kMmaWarp = kProducerWarp0 + kProducers;
+constexpr int kThreads = 32 * (kMmaWarp + 1);
 constexpr uint32_t kFullArrivals = 1 + 32;          // expect_tx + one cp.async arrival per lane
 constexpr uint32_t kEmptyArrivals = 1 + kEpiWarps;  // MMA commit + epilogue warps
 constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s
@@ -74,6 +80,7 @@ struct StageMeta {
 struct Shared {
   StageMeta meta[kStages];
   unsigned long long full[kStages], empty[kStages], acc_full[2], acc_empty[2];
+  uint32_t armed[kStages];  // uses of each stage armed so far (for the drain)
   uint32_t tmem_base;
   int abort;
 };
@@ -198,6 +205,7 @@ __device__ __forceinline__ void tc_commit(unsigned long long *bar) {
 }
 // 32 consecutive accumulator columns of TMEM lane (warp's lane base + lane).
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  __syncwarp();  // .sync.aligned: the whole warp issues it together
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
       "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
@@ -223,75 +231,106 @@ __device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
       : "memory");
 }
 
+// ---- slot lists ------------------------------------------------------------------
+// One warp per row, before the join: the row's new and old samples (forward
+// slots 0..S-1, reverse slots S..2S-1) de-duplicated (ShrinkGraph
+// RemoveDuplicates :285-291), new minus old (:468-486), written back in place
+// as compact lists with every partly used group of four padded with the
+// group's first id; nf / of become the list lengths (both 0 when the row has
+// nothing to compare).  The reverse counters are reset for the next iteration.
+__global__ void k_join_lists(int64_t n, int S, int32_t *__restrict__ newS, int32_t *__restrict__ oldS,
+                             int8_t *__restrict__ nf, int8_t *__restrict__ of,
+                             int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
+  __shared__ int32_t news_smem[8][32], olds_smem[8][32];  // launched with 8 warps
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  int32_t *news = news_smem[threadIdx.x >> 5];
+  int32_t *olds = olds_smem[threadIdx.x >> 5];
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const int cnf = nf[row], cof = of[row];
+    const int cnr = min(nrev[row], S), cor = min(orev[row], S);
+    const int64_t sb = row * (2 * S);
+    bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
+    bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
+    const int32_t nid = vn ? newS[sb + lane] : -1 - lane;
+    const int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    const uint32_t pn = __match_any_sync(0xffffffffu, nid);
+    vn = vn && (__ffs(pn) - 1 == lane);
+    const uint32_t po = __match_any_sync(0xffffffffu, oid);
+    vo = vo && (__ffs(po) - 1 == lane);
+    const uint32_t bo = __ballot_sync(0xffffffffu, vo);
+    int no = __popc(bo);
+    if (vo) olds[__popc(bo & lanemask_lt())] = oid;
+    __syncwarp();
+    for (int t = 0; t < no && vn; t++) vn = olds[t] != nid;
+    const uint32_t bn = __ballot_sync(0xffffffffu, vn);
+    int nn = __popc(bn);
+    if (vn) news[__popc(bn & lanemask_lt())] = nid;
+    if (nn == 0 || nn + no < 2) nn = no = 0;  // nothing to compare
+    __syncwarp();
+    // compact lists; the last group of four padded with its first id
+    int32_t outn = lane < nn ? news[lane] : 0;
+    int32_t outo = lane < no ? olds[lane] : 0;
+    const int32_t firstn = __shfl_sync(0xffffffffu, outn, lane & ~3);
+    const int32_t firsto = __shfl_sync(0xffffffffu, outo, lane & ~3);
+    if (lane >= nn) outn = firstn;
+    if (lane >= no) outo = firsto;
+    __syncwarp();
+    if (lane < 2 * S) {
+      newS[sb + lane] = outn;
+      oldS[sb + lane] = outo;
+    }
+    if (lane == 0) {
+      nf[row] = (int8_t)nn;
+      of[row] = (int8_t)no;
+      nrev[row] = 0;
+      orev[row] = 0;
+    }
+  }
+}
+
 // ---- producer ------------------------------------------------------------------
-// Sample lists of one row, one sample slot per lane (lane < 2S).
+// The compact slot lists of one row (k_join_lists), one slot per lane.
 struct RowLoad {
   int32_t nid, oid;
-  int cnf, cof, cnr, cor;
+  int8_t nn, no;
 };
 
 __device__ __forceinline__ RowLoad load_row(const JoinArgs &a, int64_t row, int64_t n, int S) {
   const int lane = lane_id();
-  RowLoad r{-1, -1, 0, 0, 0, 0};
+  RowLoad r{0, 0, 0, 0};
   if (row >= n) return r;
-  r.cnf = a.nf[row];
-  r.cof = a.of[row];
-  r.cnr = min(a.nrev[row], S);
-  r.cor = min(a.orev[row], S);
-  const int64_t sb = row * (2 * S);
+  r.nn = a.nf[row];
+  r.no = a.of[row];
   if (lane < 2 * S) {
-    r.nid = a.newS[sb + lane];
-    r.oid = a.oldS[sb + lane];
-  }
-  __syncwarp();
-  if (lane == 0) {
-    a.nrev[row] = 0;
-    a.orev[row] = 0;
+    r.nid = a.newS[row * (2 * S) + lane];
+    r.oid = a.oldS[row * (2 * S) + lane];
   }
   return r;
 }
 
-// Fills row-join j of stage m from its sample lists: ids (de-duplicated, empty
-// slots of a partly used group of four padded with the group's first id),
-// nn / no, norms (+inf for every slot that is not a staged row) and worst[]
-// by cp.async.  Returns the number of four-row groups to gather.
-__device__ __forceinline__ int stage_join(const JoinArgs &a, const RowLoad &r, int S, int j,
-                                          StageMeta &m, int &nn_out, int &no_out) {
+// Fills row-join j of stage m from its compact lists: ids (padded groups of
+// four), nn / no, norms (+inf for every slot that is not a staged row) and
+// worst[] by cp.async.  Returns the number of four-row groups to gather.
+__device__ __forceinline__ int stage_join(const JoinArgs &a, const RowLoad &r, int j, StageMeta &m,
+                                          int &nn_out, int &no_out) {
   const int lane = lane_id();
   const int base = 64 * j;
-  int32_t *ids = m.ids + base;
-  bool vn = (lane < S) ? (lane < r.cnf) : (lane < 2 * S && lane - S < r.cnr);
-  bool vo = (lane < S) ? (lane < r.cof) : (lane < 2 * S && lane - S < r.cor);
-  const int32_t nid = vn ? r.nid : -1 - lane;
-  const int32_t oid = vo ? r.oid : -100 - lane;
-  const uint32_t pn = __match_any_sync(0xffffffffu, nid);
-  vn = vn && (__ffs(pn) - 1 == lane);
-  const uint32_t po = __match_any_sync(0xffffffffu, oid);
-  vo = vo && (__ffs(po) - 1 == lane);
-  const uint32_t bo = __ballot_sync(0xffffffffu, vo);
-  int no = __popc(bo);
-  if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
-  __syncwarp();
-  for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
-  const uint32_t bn = __ballot_sync(0xffffffffu, vn);
-  int nn = __popc(bn);
-  if (vn) ids[__popc(bn & lanemask_lt())] = nid;
-  if (nn == 0 || nn + no < 2) nn = no = 0;  // nothing to compare
-  __syncwarp();
+  const int nn = r.nn, no = r.no;
   const int gnn = (nn + 3) & ~3, gno = (no + 3) & ~3;
-  // new slot = lane, old slot = 32 + lane
-  if (lane >= nn && lane < gnn) ids[lane] = ids[lane & ~3];
-  if (lane >= no && lane < gno) ids[32 + lane] = ids[32 + (lane & ~3)];
+  if (lane < gnn) m.ids[base + lane] = r.nid;
+  if (lane < gno) m.ids[base + 32 + lane] = r.oid;
   const float inf = __int_as_float(0x7f800000);
   if (lane < nn) {
-    cp_async4(&m.nrm[base + lane], a.nrm + ids[lane]);
-    cp_async4(&m.wst[base + lane], a.worst + ids[lane]);
+    cp_async4(&m.nrm[base + lane], a.nrm + r.nid);
+    cp_async4(&m.wst[base + lane], a.worst + r.nid);
   } else {
     m.nrm[base + lane] = inf;
   }
   if (lane < no) {
-    cp_async4(&m.nrm[base + 32 + lane], a.nrm + ids[32 + lane]);
-    cp_async4(&m.wst[base + 32 + lane], a.worst + ids[32 + lane]);
+    cp_async4(&m.nrm[base + 32 + lane], a.nrm + r.oid);
+    cp_async4(&m.wst[base + 32 + lane], a.worst + r.oid);
   } else {
     m.nrm[base + 32 + lane] = inf;
   }
@@ -330,19 +369,23 @@ __device__ __forceinline__ int stage_probe(const JoinArgs &a, int64_t t, int j, 
   return (gnn + gno) >> 2;
 }
 
+// Producer p of the CTA stages the CTA's tiles i = p, p + kProducers, ...
+// (tile index blockIdx.x + i * gridDim.x): TMA gathers are issued lane by
+// lane and occupy the issuing warp, so several producer warps keep more of
+// them in flight.
 template <bool kProbe>
-__device__ void producer(const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
+__device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
                          unsigned char *tiles, int64_t n, int64_t ntiles, int kbc, int S,
                          unsigned long long &rows_staged) {
   const int lane = lane_id();
-  uint32_t armed = 0;  // stages armed so far (phase bookkeeping for the drain)
-  int64_t t = blockIdx.x;
+  const int64_t step = (int64_t)kProducers * gridDim.x;
+  int64_t t = blockIdx.x + (int64_t)p * gridDim.x;
   RowLoad cur[2], nxt[2];
   if (!kProbe && t < ntiles) {
     cur[0] = load_row(a, 2 * t, n, S);
     cur[1] = load_row(a, 2 * t + 1, n, S);
   }
-  for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
+  for (uint32_t i = p; t < ntiles; t += step, i += kProducers) {
     const int s = i % kStages;
     const uint32_t use = i / kStages;
     if (!mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort)) {
@@ -355,10 +398,10 @@ __device__ void producer(const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
       groups = stage_probe(a, t, 0, m, nn[0], no[0]);
       groups += stage_probe(a, t, 1, m, nn[1], no[1]);
     } else {
-      groups = stage_join(a, cur[0], S, 0, m, nn[0], no[0]);
-      groups += stage_join(a, cur[1], S, 1, m, nn[1], no[1]);
-      // next tile's sample lists, in flight while this one is gathered
-      const int64_t tn = t + gridDim.x;
+      groups = stage_join(a, cur[0], 0, m, nn[0], no[0]);
+      groups += stage_join(a, cur[1], 1, m, nn[1], no[1]);
+      // this warp's next tile: its lists are in flight while this one is gathered
+      const int64_t tn = t + step;
       if (tn < ntiles) {
         nxt[0] = load_row(a, 2 * tn, n, S);
         nxt[1] = load_row(a, 2 * tn + 1, n, S);
@@ -384,17 +427,11 @@ __device__ void producer(const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
       }
     }
     cp_async_arrive_noinc(&sh.full[s]);
-    armed = i + 1;
+    if (lane == 0) atomicAdd(&sh.armed[s], 1u);
     if (!kProbe) {
       cur[0] = nxt[0];
       cur[1] = nxt[1];
     }
-  }
-  // drain: the copies of the last armed use of every stage have landed
-  for (int s = 0; s < kStages; s++) {
-    if ((uint32_t)s >= armed) break;
-    const uint32_t last = (armed - 1 - s) / kStages;  // last use of stage s
-    if (!mbar_wait(&sh.full[s], last & 1, nullptr)) atomicOr(a.err, DEVERR_TIMEOUT);
   }
 }
 
@@ -476,7 +513,7 @@ __device__ __forceinline__ int start_push(PendingPush &p, int32_t target, int32_
 // the low 6 bits (skip_col: the row's own column, or -1).
 __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const float *cn, float na,
                                               int skip_col) {
-  uint32_t best = 0xffffffffu;
+  uint32_t best[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};  // four chains
 #pragma unroll
   for (int c4 = 0; c4 < 8; c4++) {
     const float4 nc = reinterpret_cast<const float4 *>(cn)[c4];
@@ -484,14 +521,13 @@ __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const flo
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const int c = 4 * c4 + e;
-      float dd = __fmaf_rn(-2.0f, __uint_as_float(v[c]), __fadd_rn(na, ncs[e]));
-      dd = dd < 0.0f ? 0.0f : dd;
+      const float dd = fmaxf(__fmaf_rn(-2.0f, __uint_as_float(v[c]), __fadd_rn(na, ncs[e])), 0.0f);
       uint32_t key = (__float_as_uint(dd) & ~63u) | (uint32_t)c;
       key = c == skip_col ? 0xffffffffu : key;
-      best = key < best ? key : best;
+      best[e] = min(best[e], key);
     }
   }
-  return best;
+  return min(min(best[0], best[1]), min(best[2], best[3]));
 }
 
 template <bool kProbe>
@@ -596,11 +632,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&sh.acc_full[b], 1);
       mbar_init(&sh.acc_empty[b], kEpiWarps);
     }
+    for (int s = 0; s < kStages; s++) sh.armed[s] = 0;
     sh.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == kMmaWarp) {
+    __syncwarp();  // .sync.aligned: after the per-thread zeroing loop, reconverge first
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&sh.tmem_base)),
                  "r"(kTmemCols)
@@ -612,8 +650,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = sh.tmem_base;
   unsigned long long stat = 0;
-  if (warp == kProducerWarp) {
-    producer<kProbe>(&xmap, a, sh, tiles, n, ntiles, kbc, S, stat);
+  if (warp >= kProducerWarp0 && warp < kMmaWarp) {
+    producer<kProbe>(warp - kProducerWarp0, &xmap, a, sh, tiles, n, ntiles, kbc, S, stat);
     if (!kProbe && lane_id() == 0 && stat) atomicAdd(&a.ib.counters[1], stat);
   } else if (warp == kMmaWarp) {
     if (lane_id() == 0) mma_issuer(sh, tiles, tmem, ntiles, kbc, a.err);
@@ -627,6 +665,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
   tc_fence_before();
+  __syncthreads();
+  // drain, once every role is done: the copies of the last armed use of each
+  // stage have landed before the CTA's shared memory goes away
+  if (threadIdx.x == 32 * kProducerWarp0) {
+    for (int s = 0; s < kStages; s++) {
+      const uint32_t u = sh.armed[s];
+      if (u > 0 && !mbar_wait(&sh.full[s], (u - 1) & 1, nullptr)) atomicOr(a.err, DEVERR_TIMEOUT);
+    }
+  }
   __syncthreads();
   if (warp == kMmaWarp) {
     tc_fence_after();
@@ -698,6 +745,11 @@ void tc_join_launch(Context *ctx, const TcJoin &tj, int S, const float *nrm, con
                     const int32_t *oldS, const int8_t *nf, const int8_t *of, int32_t *nrev,
                     int32_t *orev, const float *worst, const Inbox &ib) {
   HDB_REQUIRE(S >= 1 && 2 * S <= 32, HDB_ERR_ARG, "tensor-core join: need 2 * SAMPLE_NUM <= 32");
+  k_join_lists<<<grid_for(ctx, tj.n, 8, 8), 256, 0, ctx->stream>>>(
+      tj.n, S, const_cast<int32_t *>(newS), const_cast<int32_t *>(oldS),
+      const_cast<int8_t *>(nf), const_cast<int8_t *>(of), nrev, orev);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
   JoinArgs a{nrm, newS, oldS, nf, of, nrev, orev, worst, ib, nullptr, nullptr, nullptr, ctx->dev_err};
   launch<false>(ctx, tj, (tj.n + 1) / 2, S, a);
 }

@@ -29,7 +29,6 @@ using namespace knn;
 
 namespace {
 
-constexpr int kMergeSlots = 128;
 
 __host__ __device__ __forceinline__ uint64_t xorshift64star(uint64_t x) {
   // gpuknn/knncuda_tools.cu:126-132
@@ -56,25 +55,6 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
     }
   }
   return v;
-}
-
-// Ascending bitonic sort of the first `size` (32, 64 or 128) u64 of s in
-// shared memory by one warp.
-__device__ __forceinline__ void warp_sort_smem(uint64_t *s, int size) {
-  const int lane = lane_id();
-  const int pairs = size >> 1;
-  for (int sz = 2; sz <= size; sz <<= 1) {
-    for (int stride = sz >> 1; stride > 0; stride >>= 1) {
-      for (int t = lane; t < pairs; t += 32) {
-        int i = (t / stride) * (2 * stride) + (t % stride);
-        int j = i + stride;
-        bool up = (i & sz) == 0;
-        uint64_t a = s[i], b = s[j];
-        if ((a > b) == up) { s[i] = b; s[j] = a; }
-      }
-      __syncwarp();
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -152,83 +132,44 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
   }
 }
 
-// Per-warp shared memory of a merge: 128 sorted candidates, then the k output
-// keys and labels.
-constexpr int kMergeSmemU64 = kMergeSlots + kMaxK + kMaxK / 2;
-
-// Sorts the 128 candidates in sk, drops duplicates and ids already in the
-// row, and merges the rest into the row held one entry per lane (lane < k).
-__device__ __forceinline__ void merge_chunk(int k, int32_t &lab, float &dist, uint64_t *sk,
-                                            int size) {
+// Offers a chunk of up to 32 candidates (one per lane, ~0 for none) to the
+// row held one sorted entry per lane (lane < k; key = (distance, id)).  Only
+// candidates below the row's current k-th key can enter, and the k-th key
+// never grows, so those are found with one ballot; each is then placed by
+// rank (ballot of the keys below it) unless its id is already listed, the
+// entries above it moving up one lane and the last one dropping out.  The
+// result is the first k distinct ids of the union in key order, whatever the
+// order of the candidates.  Inserted entries carry the "new" flag.
+__device__ __forceinline__ void insert_chunk(int k, uint64_t &rkey, int32_t &lab, uint64_t cand) {
   const int lane = lane_id();
-  __syncwarp();
-  warp_sort_smem(sk, size);
   const bool have = lane < k;
-  const uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
-  const int32_t rid = have ? decode(lab) : -1;
-  uint64_t c[kMergeSlots / 32];
-  bool ok[kMergeSlots / 32];
-#pragma unroll
-  for (int q = 0; q < kMergeSlots / 32; q++) {
-    int i = lane + 32 * q;
-    c[q] = i < size ? sk[i] : ~0ull;
-    uint64_t prev = (i > 0 && i < size) ? sk[i - 1] : ~0ull;
-    ok[q] = c[q] != ~0ull && c[q] != prev;
-  }
-  for (int t = 0; t < k; t++) {
-    int32_t r = __shfl_sync(0xffffffffu, rid, t);
-#pragma unroll
-    for (int q = 0; q < kMergeSlots / 32; q++)
-      if (pk_id(c[q]) == r) ok[q] = false;
-  }
-  __syncwarp();
-  int ns = 0;
-#pragma unroll
-  for (int q = 0; q < kMergeSlots / 32; q++) {
-    uint32_t bal = __ballot_sync(0xffffffffu, ok[q]);
-    if (ok[q]) sk[ns + __popc(bal & lanemask_lt())] = c[q];
-    ns += __popc(bal);
-  }
-  __syncwarp();
-  if (ns == 0) return;
-  uint64_t *out_key = sk + kMergeSlots;
-  int32_t *out_lab = reinterpret_cast<int32_t *>(out_key + kMaxK);
-  // row entry of this lane: rank = lane + #(survivors below it)
-  int lo = 0, hi = ns;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (sk[mid] < rkey) lo = mid + 1; else hi = mid;
-  }
-  if (have && lane + lo < k) {
-    out_key[lane + lo] = rkey;
-    out_lab[lane + lo] = lab;
-  }
-  // survivor i: rank = i + #(row entries below it)
-#pragma unroll
-  for (int q = 0; q < kMergeSlots / 32; q++) {
-    int i = lane + 32 * q;
-    uint64_t cc = i < ns ? sk[i] : ~0ull;
-    int below = 0;
-    for (int t = 0; t < k; t++) below += __shfl_sync(0xffffffffu, rkey, t) < cc;
-    if (i < ns && i + below < k) {
-      out_key[i + below] = cc;
-      out_lab[i + below] = pk_id(cc);  // inserted as "new"
+  const uint64_t kth = __shfl_sync(0xffffffffu, rkey, k - 1);
+  uint32_t todo = __ballot_sync(0xffffffffu, cand < kth);
+  while (todo) {
+    const int t = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint64_t c = __shfl_sync(0xffffffffu, cand, t);
+    const int pos = __popc(__ballot_sync(0xffffffffu, have && rkey < c));
+    if (pos >= k) continue;
+    const int32_t cid = pk_id(c);
+    if (__any_sync(0xffffffffu, have && pk_id(rkey) == cid)) continue;
+    const uint64_t up = __shfl_up_sync(0xffffffffu, rkey, 1);
+    const int32_t uplab = __shfl_up_sync(0xffffffffu, lab, 1);
+    if (lane == pos) {
+      rkey = c;
+      lab = cid;
+    } else if (have && lane > pos) {
+      rkey = up;
+      lab = uplab;
     }
   }
-  __syncwarp();
-  if (have) {
-    lab = out_lab[lane];
-    dist = pk_dist(out_key[lane]);
-  }
-  __syncwarp();
 }
 
 // Merge of everything offered to a row (inbox, overflow segment, best
 // dropped) into its sorted list (one warp).  On return, lane j (< k) holds the
-// j-th entry of the merged row.  Candidates of one pair always carry the same
-// distance, so duplicates are adjacent after each sort.
+// j-th entry of the merged row.
 __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, float &dist,
-                                          const Inbox &ib, uint64_t *sk) {
+                                          const Inbox &ib) {
   const int lane = lane_id();
   int cnt = ib.cnt[row];
   const uint64_t ov = ib.best[row];
@@ -241,18 +182,20 @@ __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, floa
     if (ov != ~0ull) ib.best[row] = ~0ull;
     if (o0 != o1) { ib.ostart[row] = 0; ib.oend[row] = 0; }
   }
-  {
-    const int used = cnt + (ov != ~0ull ? 1 : 0);
-    const int size = used <= 32 ? 32 : (used <= 64 ? 64 : kMergeSlots);
-    for (int i = lane; i < size; i += 32)
-      sk[i] = i < cnt ? ib.slots[row * kInboxCap + i] : (i == cnt && ov != ~0ull ? ov : ~0ull);
-    merge_chunk(k, lab, dist, sk, size);
-  }
-  for (uint32_t base = o0; base < o1; base += kMergeSlots) {
-    for (int i = lane; i < kMergeSlots; i += 32)
-      sk[i] = base + i < o1 ? ib.ovf_key[ib.ovf_idx[base + i]] : ~0ull;
-    merge_chunk(k, lab, dist, sk, kMergeSlots);
-  }
+  const bool have = lane < k;
+  uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
+  // the inbox (<= 127 slots) in four coalesced loads, all in flight at once
+  const uint64_t *sl = ib.slots + row * kInboxCap;
+  uint64_t c[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) c[q] = 32 * q + lane < cnt ? sl[32 * q + lane] : ~0ull;
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (32 * q < cnt) insert_chunk(k, rkey, lab, c[q]);
+  if (ov != ~0ull) insert_chunk(k, rkey, lab, lane == 0 ? ov : ~0ull);
+  for (uint32_t base = o0; base < o1; base += 32)
+    insert_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[ib.ovf_idx[base + lane]] : ~0ull);
+  if (have) dist = pk_dist(rkey);
 }
 
 // Merge (iterations >= 1), sample (PrepareGraph :44-98 and reverse samples
@@ -262,16 +205,14 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
                          int32_t *__restrict__ newS,
                          int32_t *__restrict__ oldS, int8_t *__restrict__ nf, int8_t *__restrict__ of,
                          int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
-  extern __shared__ uint64_t smem_sample[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
-  uint64_t *sk = smem_sample + (threadIdx.x >> 5) * kMergeSmemU64;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    if (do_merge) merge_row(row, k, lab, dist, ib, sk);
+    if (do_merge) merge_row(row, k, lab, dist, ib);
     const bool isnew = have && lab >= 0;
     const bool isold = have && lab < 0;
     const int32_t id = decode(lab);
@@ -305,16 +246,14 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
 __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
                            const float *__restrict__ gdist, Inbox ib,
                            hdb_nnd_element *__restrict__ out) {
-  extern __shared__ uint64_t smem_fin[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
-  uint64_t *sk = smem_fin + (threadIdx.x >> 5) * kMergeSmemU64;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    merge_row(row, k, lab, dist, ib, sk);
+    merge_row(row, k, lab, dist, ib);
     if (have) {
       hdb_nnd_element e;
       e.distance_ = dist;
@@ -501,15 +440,35 @@ struct JoinSmemBf16 {
   }
 };
 
+// Column sums of X (FP64, one thread per column, rows split over blocks):
+// the BF16 copy is taken of the centred rows.
+__global__ void k_col_sums(const float *__restrict__ X, int64_t n, int d, double *__restrict__ sums) {
+  for (int j = threadIdx.x; j < d; j += blockDim.x) {
+    double s = 0.0;
+    for (int64_t row = blockIdx.x; row < n; row += gridDim.x) s += (double)X[row * d + j];
+    atomicAdd(&sums[j], s);
+  }
+}
+
+__global__ void k_col_mean(const double *__restrict__ sums, int d, int64_t n, float *__restrict__ mean) {
+  for (int j = threadIdx.x; j < d; j += blockDim.x) mean[j] = (float)(sums[j] / (double)n);
+}
+
+// BF16 copy of (X - mean) (mean may be null: no centring), zero padded to
+// dpad columns, and the FP32 squared norm of every rounded row.  Distances
+// do not change under a common shift, and centring keeps the coordinates
+// small, which is where BF16 rounding is finest.
 __global__ void k_bf16_prepare(const float *__restrict__ X, int64_t n, int d, int dpad,
-                               __nv_bfloat16 *__restrict__ Xb, float *__restrict__ nrm) {
+                               const float *__restrict__ mean, __nv_bfloat16 *__restrict__ Xb,
+                               float *__restrict__ nrm) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     float part = 0.0f;
     for (int j = lane; j < dpad; j += 32) {
-      __nv_bfloat16 b = __float2bfloat16_rn(j < d ? X[row * d + j] : 0.0f);
+      const float x = j < d ? __fsub_rn(X[row * d + j], mean ? mean[j] : 0.0f) : 0.0f;
+      __nv_bfloat16 b = __float2bfloat16_rn(x);
       Xb[row * dpad + j] = b;
       float v = __bfloat162float(b);
       part = __fmaf_rn(v, v, part);
@@ -866,7 +825,6 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
   k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, gid, gdist, worst); ctx->launches++;
   HDB_CHECK_LAUNCH();
-  const size_t smem_sample = (size_t)wpb * kMergeSmemU64 * sizeof(uint64_t);
   const int dp = (d & 1) ? d : d + 1;
   const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
   int jw = (int)((56 * 1024) / per_warp);  // about four blocks per SM
@@ -889,7 +847,12 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   if (bf16) {
     Xb = Buf<__nv_bfloat16>(ctx, (size_t)n * dpad);
     nrm = Buf<float>(ctx, n);
-    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, Xb, nrm); ctx->launches++;
+    Buf<double> csum(ctx, d);
+    Buf<float> cmean(ctx, d);
+    HDB_CUDA(cudaMemsetAsync(csum, 0, d * sizeof(double), st));
+    k_col_sums<<<2 * ctx->num_sms, 256, 0, st>>>(X, n, d, csum); ctx->launches++;
+    k_col_mean<<<1, 256, 0, st>>>(csum, d, n, cmean); ctx->launches++;
+    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, cmean, Xb, nrm); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (use_tc) {
       tc_join_prepare(ctx, Xb, n, dpad, &tj);
@@ -902,7 +865,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     }
   }
   for (int it = 0; it < p.iterations; it++) {
-    k_sample<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
+    k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
                                                        newS, oldS, nf, of, nrev, orev); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
@@ -922,7 +885,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     sort_overflow(ctx, ib, n);
     HDB_CHECK_LAUNCH();
   }
-  k_finalize<<<grid_rows, 32 * wpb, smem_sample, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
+  k_finalize<<<grid_rows, 32 * wpb, 0, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (bf16) {
     k_rerank<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, G); ctx->launches++;
@@ -959,7 +922,8 @@ void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, con
   const int dpad = tc_dpad(d);
   Buf<__nv_bfloat16> Xb(ctx, (size_t)n * dpad);
   Buf<float> nrm(ctx, n);
-  k_bf16_prepare<<<grid_for(ctx, n, 8, 16), 256, 0, ctx->stream>>>(X, n, d, dpad, Xb, nrm);
+  k_bf16_prepare<<<grid_for(ctx, n, 8, 16), 256, 0, ctx->stream>>>(X, n, d, dpad, nullptr, Xb,
+                                                                    nrm);
   ctx->launches++;
   HDB_CHECK_LAUNCH();
   tc_gram_probe(ctx, Xb, nrm, n, dpad, ids, counts, tiles, out);

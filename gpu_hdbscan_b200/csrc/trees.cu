@@ -471,6 +471,12 @@ __device__ T add_repeated(T s, T v, int64_t cnt) {
 // loads 32 chain items at a time (coalesced) and every lane replays the same
 // sequential sum from registers, so the serial chain walk never waits on a
 // dependent global load; lane 0 stores the result.
+// Stability of each cluster: its chain items summed in FP32 in the
+// reference's row order (and in FP64 alongside when kBoth).  One warp per
+// cluster, 32 items per load; each lane forms its item's addends first, so the
+// serial part is just the chain of adds, unrolled over the 32 items.  Items
+// that stand for many rows with one addend go through add_repeated.
+template <bool kBoth>
 __global__ void k_stability(int64_t C, const int64_t *__restrict__ seg_start,
                             const int64_t *__restrict__ seg_end, const ChainItem *__restrict__ items,
                             const float *__restrict__ birth, float *__restrict__ stab,
@@ -484,32 +490,54 @@ __global__ void k_stability(int64_t C, const int64_t *__restrict__ seg_start,
     double s64 = 0.0;
     const int64_t e = seg_end[c];
     for (int64_t base = seg_start[c]; base < e; base += 32) {
-      ChainItem mine = {0.0f, 0, 0, 0};
-      if (base + lane < e) mine = items[base + lane];
+      ChainItem mine = {0.0f, 1, 0, 0};
+      const bool valid = base + lane < e;
+      if (valid) mine = items[base + lane];
       const int m = (int)min((int64_t)32, e - base);
+      const float v = __fsub_rn(mine.lam, b);
+      // split rows: (lambda - birth) * child_size, left then right; one row: v
+      const bool split = mine.a < 0;
+      const float x0 = split ? __fmul_rn(v, (float)(-mine.a)) : v;
+      const float x1 = split ? __fmul_rn(v, (float)mine.b) : 0.0f;
+      const uint32_t split_mask = __ballot_sync(0xffffffffu, valid && split);
+      const uint32_t rep_mask = __ballot_sync(0xffffffffu, valid && mine.a > 1);
+      if (!kBoth && rep_mask == 0) {
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+          const float y0 = __shfl_sync(0xffffffffu, x0, t);
+          const float y1 = __shfl_sync(0xffffffffu, x1, t);
+          if (t < m) {
+            s = __fadd_rn(s, y0);
+            if ((split_mask >> t) & 1u) s = __fadd_rn(s, y1);
+          }
+        }
+        continue;
+      }
       for (int t = 0; t < m; t++) {
         const float lam = __shfl_sync(0xffffffffu, mine.lam, t);
         const int32_t ia = __shfl_sync(0xffffffffu, mine.a, t);
         const int32_t ib = __shfl_sync(0xffffffffu, mine.b, t);
-        const float v = __fsub_rn(lam, b);
+        const float vt = __fsub_rn(lam, b);
         const double v64 = __dsub_rn((double)lam, (double)b);
-        if (ia < 0) {  // split rows: (lambda - birth) * child_size, left then right
-          s = __fadd_rn(s, __fmul_rn(v, (float)(-ia)));
-          s = __fadd_rn(s, __fmul_rn(v, (float)ib));
-          s64 = __dadd_rn(s64, __dmul_rn(v64, (double)(-ia)));
-          s64 = __dadd_rn(s64, __dmul_rn(v64, (double)ib));
+        if (ia < 0) {
+          s = __fadd_rn(s, __fmul_rn(vt, (float)(-ia)));
+          s = __fadd_rn(s, __fmul_rn(vt, (float)ib));
+          if (kBoth) {
+            s64 = __dadd_rn(s64, __dmul_rn(v64, (double)(-ia)));
+            s64 = __dadd_rn(s64, __dmul_rn(v64, (double)ib));
+          }
         } else if (ia == 1) {  // one row
-          s = __fadd_rn(s, v);
-          s64 = __dadd_rn(s64, v64);
+          s = __fadd_rn(s, vt);
+          if (kBoth) s64 = __dadd_rn(s64, v64);
         } else {  // one row per point falling out here
-          s = add_repeated<float>(s, v, ia);
-          s64 = add_repeated<double>(s64, v64, ia);
+          s = add_repeated<float>(s, vt, ia);
+          if (kBoth) s64 = add_repeated<double>(s64, v64, ia);
         }
       }
     }
     if (lane == 0) {
       stab[c] = s;
-      stab64[c] = s64;
+      stab64[c] = kBoth ? s64 : (double)s;
     }
   }
 }
@@ -873,7 +901,11 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
     Buf<ChainItem> items(ctx, nv_total);
     k_chain_items<<<grid_for(ctx, nv_total, 256), 256, 0, st>>>(t, chain, nv_total, kind, lam,
                                                                 items); ctx->launches++;
-    k_stability<<<grid_for(ctx, C, 4), 128, 0, st>>>(C, s0, s1, items, birth, stab, stab64); ctx->launches++;
+    if (stab_mode == HDB_STAB_FP64)
+      k_stability<true><<<grid_for(ctx, C, 4), 128, 0, st>>>(C, s0, s1, items, birth, stab, stab64);
+    else
+      k_stability<false><<<grid_for(ctx, C, 4), 128, 0, st>>>(C, s0, s1, items, birth, stab, stab64);
+    ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
 

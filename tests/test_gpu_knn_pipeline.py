@@ -133,9 +133,14 @@ def test_disconnected_graph_is_reported(ctx):
 
 
 def test_small_and_edge_sizes(ctx, oracle):
-    """n just above k, k < 32, and mpts = 2."""
+    """n just above k, k < 32, and mpts = 2.  Overlapping blobs: with separated
+    ones the exact 8-NN graph of 100 points already falls apart, and whether the
+    antihub clique joins the pieces depends on which points the approximate
+    graph leaves with the lowest in-degree (the reference then fails with
+    "MST montada incorretamente", as this library does with
+    HDB_ERR_DISCONNECTED)."""
     for n, k, mpts in [(40, 32, 32), (100, 8, 8), (33, 32, 2), (500, 16, 16)]:
-        X = blobs(n, 3, seed=n)
+        X = blobs(n, 3, seed=n, spread=2.5)
         G = ctx.NNDescent(X, k=k, sample_num=k // 2)
         labels, _ = ctx.hdbscan_from_knn(G, X, k=k, mpts=mpts)
         ids = _t(ctx.knn_split(G)[0])
@@ -178,12 +183,17 @@ def test_bf16_nndescent_graph_is_valid_and_reranked_exactly(ctx, oracle, n, d):
 @pytest.mark.parametrize("d", [128, 64])
 def test_bf16_recall_matches_fp32_form(ctx, oracle, d):
     """Recall@32 of the BF16 form within 0.5 pt of the plain FP32 form (the
-    benchmark's 'equal recall@k' condition) on blob data like the 20M x 128
-    workload."""
+    benchmark's 'equal recall@k' condition) on the 20M x 128 workload's
+    distribution (blob centres in [-20, 20], sigma in [0.5, 1.5]) at 30,000
+    points, in 128 and in 64 dimensions."""
+    from dataclasses import replace
+
     from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
     w = synth.scaled("blobs_20m_d128", 30000)
-    X = synth.generate(w) if d == 128 else blobs(30000, d, seed=5, blobs=60, spread=20.0)
-    q = np.arange(0, len(X), 11)
+    X = synth.generate(w if d == 128 else replace(w, d=d, seed=5))
+    # every row is a query: two independent NN-Descent runs differ by a few
+    # tenths of a point on a subsample, which this comparison must not see
+    q = np.arange(len(X))
     gt, _ = oracle.bruteforce_knn(X, 32, q)
     rec = {}
     for name, prec in (("fp32", HDB_PREC_FP32), ("bf16", HDB_PREC_BF16)):
