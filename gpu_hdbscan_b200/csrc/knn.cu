@@ -79,13 +79,26 @@ __device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int
     const int w = min(kStageCols, d - c0);
     __syncwarp();
     if (lane < w) own[lane] = X[row * d + c0 + lane];
-    // 32 rows x w columns, flattened: element e -> row e / w, column e % w
+    if (w == kStageCols) {
+      // full chunk: row i's segment is one coalesced load (lane = column), and
+      // all 32 are issued before any is stored, so they are in flight together
+      float t[kStageCols];
+#pragma unroll
+      for (int i = 0; i < kStageCols; i++) {
+        const int32_t rid = __shfl_sync(0xffffffffu, id, i);
+        t[i] = ((act >> i) & 1u) ? __ldg(X + (int64_t)rid * d + c0 + lane) : 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < kStageCols; i++) nb[i * kStageLd + lane] = t[i];
+    } else {
+      // ragged chunk: 32 rows x w columns, flattened: element e -> row e / w, column e % w
 #pragma unroll 8
-    for (int i = 0; i < w; i++) {
-      const int e = i * 32 + lane;
-      const int r = e / w, c = e - r * w;
-      const int32_t rid = __shfl_sync(0xffffffffu, id, r);
-      if ((act >> r) & 1u) nb[r * kStageLd + c] = __ldg(X + (int64_t)rid * d + c0 + c);
+      for (int i = 0; i < w; i++) {
+        const int e = i * 32 + lane;
+        const int r = e / w, c = e - r * w;
+        const int32_t rid = __shfl_sync(0xffffffffu, id, r);
+        if ((act >> r) & 1u) nb[r * kStageLd + c] = __ldg(X + (int64_t)rid * d + c0 + c);
+      }
     }
     __syncwarp();
     if (active) {
