@@ -388,7 +388,7 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
   for (uint32_t i = p; t < ntiles; t += step, i += kProducers) {
     const int s = i % kStages;
     const uint32_t use = i / kStages;
-    if (!mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort)) {
+    if (!__all_sync(0xffffffffu, mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }
@@ -544,7 +544,7 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     const uint32_t use = i / kStages;
     const int b = i & 1;
     const uint32_t ub = i >> 1;
-    if (!mbar_wait(&sh.full[s], use & 1, &sh.abort)) {
+    if (!__all_sync(0xffffffffu, mbar_wait(&sh.full[s], use & 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }
@@ -554,7 +554,7 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     const int32_t myid = M.ids[64 * j + slot];
     const float na = M.nrm[64 * j + slot];
     const float wst = M.wst[64 * j + slot];
-    if (!mbar_wait(&sh.acc_full[b], ub & 1, &sh.abort)) {
+    if (!__all_sync(0xffffffffu, mbar_wait(&sh.acc_full[b], ub & 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }

@@ -178,11 +178,73 @@ __device__ __forceinline__ void insert_chunk(int k, uint64_t &rkey, int32_t &lab
   }
 }
 
+// Rank of x among the sorted keys held by lanes 0..m-1 (number of keys
+// below x), by binary search over shuffled lanes; every lane its own x.
+__device__ __forceinline__ int rank_in_lanes(uint64_t sorted, int m, uint64_t x) {
+  int lo = 0, hi = m;
+#pragma unroll
+  for (int it = 0; it < 6; it++) {  // 2^6 > 33 possible answers
+    const int mid = (lo + hi) >> 1;
+    const uint64_t v = __shfl_sync(0xffffffffu, sorted, mid & 31);
+    if (lo < hi) {
+      if (v < x) lo = mid + 1; else hi = mid;
+    }
+  }
+  return lo;
+}
+
+// The same merge as insert_chunk for a chunk with many candidates: ids
+// already listed and repeats within the chunk are dropped first (one value
+// per pair, so repeats carry equal keys), the survivors are sorted across
+// the lanes, each side of the merge finds its rank in the other by binary
+// search, and the first k entries are placed through per-warp shared memory
+// (sk: 32 keys, sl: 32 labels).  Chunks with few candidates take the
+// one-at-a-time insertion, which is cheaper there.
+__device__ __forceinline__ void merge_chunk(int k, uint64_t &rkey, int32_t &lab, uint64_t cand,
+                                            uint64_t *sk, int32_t *sl) {
+  const int lane = lane_id();
+  const bool have = lane < k;
+  const uint64_t kth = __shfl_sync(0xffffffffu, rkey, k - 1);
+  bool ok = cand < kth;
+  if (__ballot_sync(0xffffffffu, ok) == 0) return;
+  const int32_t cid = pk_id(cand);
+  const int32_t rid = pk_id(rkey);
+  for (int t = 0; t < k; t++) {
+    const int32_t r = __shfl_sync(0xffffffffu, rid, t);  // every lane takes part
+    ok = ok && cid != r;
+  }
+  const uint32_t same = __match_any_sync(0xffffffffu, ok ? cid : -1 - lane);
+  ok = ok && (__ffs(same) - 1 == lane);
+  const int nc = __popc(__ballot_sync(0xffffffffu, ok));
+  if (nc == 0) return;
+  if (nc <= 12) {
+    insert_chunk(k, rkey, lab, ok ? cand : ~0ull);
+    return;
+  }
+  const uint64_t c = warp_sort32(ok ? cand : ~0ull);  // survivors in lanes 0..nc-1
+  const int pos_r = lane + rank_in_lanes(c, nc, rkey);  // row entry: its merged rank
+  const int pos_c = lane + rank_in_lanes(rkey, k, c);   // candidate: its merged rank
+  __syncwarp();
+  if (have && pos_r < k) {
+    sk[pos_r] = rkey;
+    sl[pos_r] = lab;
+  }
+  if (lane < nc && pos_c < k) {
+    sk[pos_c] = c;
+    sl[pos_c] = pk_id(c);  // inserted as "new"
+  }
+  __syncwarp();
+  if (have) {
+    rkey = sk[lane];
+    lab = sl[lane];
+  }
+}
+
 // Merge of everything offered to a row (inbox, overflow segment, best
 // dropped) into its sorted list (one warp).  On return, lane j (< k) holds the
 // j-th entry of the merged row.
 __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, float &dist,
-                                          const Inbox &ib) {
+                                          const Inbox &ib, uint64_t *sk, int32_t *sl) {
   const int lane = lane_id();
   int cnt = ib.cnt[row];
   const uint64_t ov = ib.best[row];
@@ -198,16 +260,17 @@ __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, floa
   const bool have = lane < k;
   uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
   // the inbox (<= 127 slots) in four coalesced loads, all in flight at once
-  const uint64_t *sl = ib.slots + row * kInboxCap;
+  const uint64_t *inbox = ib.slots + row * kInboxCap;
   uint64_t c[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) c[q] = 32 * q + lane < cnt ? sl[32 * q + lane] : ~0ull;
+  for (int q = 0; q < 4; q++) c[q] = 32 * q + lane < cnt ? inbox[32 * q + lane] : ~0ull;
 #pragma unroll
   for (int q = 0; q < 4; q++)
-    if (32 * q < cnt) insert_chunk(k, rkey, lab, c[q]);
+    if (32 * q < cnt) merge_chunk(k, rkey, lab, c[q], sk, sl);
   if (ov != ~0ull) insert_chunk(k, rkey, lab, lane == 0 ? ov : ~0ull);
   for (uint32_t base = o0; base < o1; base += 32)
-    insert_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[ib.ovf_idx[base + lane]] : ~0ull);
+    merge_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[ib.ovf_idx[base + lane]] : ~0ull, sk,
+                sl);
   if (have) dist = pk_dist(rkey);
 }
 
@@ -220,12 +283,16 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
                          int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
+  __shared__ uint64_t merge_keys[8][32];  // per-warp merge scratch (8 warps per block)
+  __shared__ int32_t merge_labs[8][32];
+  uint64_t *sk = merge_keys[threadIdx.x >> 5];
+  int32_t *sl = merge_labs[threadIdx.x >> 5];
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    if (do_merge) merge_row(row, k, lab, dist, ib);
+    if (do_merge) merge_row(row, k, lab, dist, ib, sk, sl);
     const bool isnew = have && lab >= 0;
     const bool isold = have && lab < 0;
     const int32_t id = decode(lab);
@@ -261,12 +328,16 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
                            hdb_nnd_element *__restrict__ out) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
+  __shared__ uint64_t merge_keys[8][32];  // per-warp merge scratch (8 warps per block)
+  __shared__ int32_t merge_labs[8][32];
+  uint64_t *sk = merge_keys[threadIdx.x >> 5];
+  int32_t *sl = merge_labs[threadIdx.x >> 5];
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    merge_row(row, k, lab, dist, ib);
+    merge_row(row, k, lab, dist, ib, sk, sl);
     if (have) {
       hdb_nnd_element e;
       e.distance_ = dist;
