@@ -209,12 +209,47 @@ __global__ void k_core_from_dist(const float *__restrict__ dist, int64_t n, int 
 
 // Core distance as the reference's fix_distances would give it for the k-th
 // neighbour (only that entry of each row reaches the MRD weights).
-__global__ void k_core_sqrt(const float *__restrict__ X, const int32_t *__restrict__ ids,
-                            int64_t n, int d, int k, float *__restrict__ core) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t v = ids[i * k + (k - 1)];
-    core[i] = euclid_ref(X + i * d, X + v * d, d);
+// Core distance with the reference's rounding (euclid_ref) against the k-th
+// neighbour: one warp per 32 rows (lane = row).  Each 32-column chunk of the
+// 32 own rows and of their 32 neighbour rows is staged in shared memory by
+// coalesced row-segment loads; every lane then walks its pair of rows in
+// dimension order, so the sum is the same sequence as euclid_ref's.
+constexpr int kCoreCols = 32, kCoreLd = kCoreCols + 1, kCoreWarps = 4;
+__global__ void __launch_bounds__(32 * kCoreWarps)
+    k_core_sqrt(const float *__restrict__ X, const int32_t *__restrict__ ids, int64_t n, int d, int k,
+                float *__restrict__ core) {
+  __shared__ float stage[kCoreWarps][2][32 * kCoreLd];
+  const int lane = lane_id(), w = threadIdx.x >> 5;
+  float *own = stage[w][0], *nb = stage[w][1];
+  for (int64_t r0 = ((int64_t)blockIdx.x * kCoreWarps + w) * 32; r0 < n;
+       r0 += (int64_t)gridDim.x * kCoreWarps * 32) {
+    const int64_t row = r0 + lane;
+    const bool active = row < n;
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    const int32_t v = active ? ids[row * k + (k - 1)] : 0;
+    float soma = 0.0f;
+    for (int c0 = 0; c0 < d; c0 += kCoreCols) {
+      const int wd = min(kCoreCols, d - c0);
+      __syncwarp();
+      for (int i = 0; i < 32; i++) {
+        if (!((act >> i) & 1u)) continue;
+        const int32_t vi = __shfl_sync(0xffffffffu, v, i);  // the loop is warp-uniform
+        if (lane < wd) {
+          own[i * kCoreLd + lane] = X[(r0 + i) * d + c0 + lane];
+          nb[i * kCoreLd + lane] = X[(int64_t)vi * d + c0 + lane];
+        }
+      }
+      __syncwarp();
+      if (active) {
+        const float *a = own + lane * kCoreLd, *b = nb + lane * kCoreLd;
+        for (int j = 0; j < wd; j++) {
+          const float diff = __fsub_rn(a[j], b[j]);
+          const double sq = __dmul_rn((double)diff, (double)diff);
+          soma = __double2float_rn(__dadd_rn((double)soma, sq));
+        }
+      }
+    }
+    if (active) core[row] = __fsqrt_rn(soma);
   }
 }
 
@@ -292,7 +327,8 @@ void core_distances(Context *ctx, const float *dist, const float *X, const int32
                     int64_t n, int32_t d, int32_t k, int32_t mode, float *core) {
   int g = grid_for(ctx, n, 256);
   if (mode == HDB_DIST_SQRT)
-    k_core_sqrt<<<g, 256, 0, ctx->stream>>>(X, ids, n, d, k, core);
+    k_core_sqrt<<<grid_for(ctx, (n + 31) / 32, kCoreWarps, 8), 32 * kCoreWarps, 0, ctx->stream>>>(
+        X, ids, n, d, k, core);
   else
     k_core_from_dist<<<g, 256, 0, ctx->stream>>>(dist, n, k, core);
   ctx->launches++;

@@ -263,7 +263,12 @@ __global__ void k_join_lists(int64_t n, int S, int32_t *__restrict__ newS, int32
     int no = __popc(bo);
     if (vo) olds[__popc(bo & lanemask_lt())] = oid;
     __syncwarp();
-    for (int t = 0; t < no && vn; t++) vn = olds[t] != nid;
+    {
+      bool in_old = false;  // independent reads, not a chain
+#pragma unroll 8
+      for (int t = 0; t < no; t++) in_old |= olds[t] == nid;
+      vn = vn && !in_old;
+    }
     const uint32_t bn = __ballot_sync(0xffffffffu, vn);
     int nn = __popc(bn);
     if (vn) news[__popc(bn & lanemask_lt())] = nid;

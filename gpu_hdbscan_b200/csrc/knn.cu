@@ -405,7 +405,12 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
     __syncwarp();
     // new \ old (:468-486)
-    for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
+    {
+      bool in_old = false;  // independent reads, not a chain
+#pragma unroll 8
+      for (int t = 0; t < no; t++) in_old |= ids[32 + t] == nid;
+      vn = vn && !in_old;
+    }
     uint32_t bn = __ballot_sync(0xffffffffu, vn);
     const int nn = __popc(bn);
     if (vn) ids[__popc(bn & lanemask_lt())] = nid;
@@ -529,6 +534,7 @@ struct JoinSmemBf16 {
 __global__ void k_col_sums(const float *__restrict__ X, int64_t n, int d, double *__restrict__ sums) {
   for (int j = threadIdx.x; j < d; j += blockDim.x) {
     double s = 0.0;
+#pragma unroll 8
     for (int64_t row = blockIdx.x; row < n; row += gridDim.x) s += (double)X[row * d + j];
     atomicAdd(&sums[j], s);
   }
@@ -626,7 +632,12 @@ __global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restri
     const int no = __popc(bo);
     if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
     __syncwarp();
-    for (int t = 0; t < no && vn; t++) vn = ids[32 + t] != nid;
+    {
+      bool in_old = false;  // independent reads, not a chain
+#pragma unroll 8
+      for (int t = 0; t < no; t++) in_old |= ids[32 + t] == nid;
+      vn = vn && !in_old;
+    }
     uint32_t bn = __ballot_sync(0xffffffffu, vn);
     const int nn = __popc(bn);
     if (vn) ids[__popc(bn & lanemask_lt())] = nid;
@@ -934,7 +945,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     Buf<double> csum(ctx, d);
     Buf<float> cmean(ctx, d);
     HDB_CUDA(cudaMemsetAsync(csum, 0, d * sizeof(double), st));
-    k_col_sums<<<2 * ctx->num_sms, 256, 0, st>>>(X, n, d, csum); ctx->launches++;
+    k_col_sums<<<16 * ctx->num_sms, 256, 0, st>>>(X, n, d, csum); ctx->launches++;
     k_col_mean<<<1, 256, 0, st>>>(csum, d, n, cmean); ctx->launches++;
     k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, cmean, Xb, nrm); ctx->launches++;
     HDB_CHECK_LAUNCH();
