@@ -145,16 +145,26 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist(const K *__restrict__
   counts[(int64_t)threadIdx.x * nblocks + blockIdx.x] = hist[threadIdx.x];
 }
 
+// Scatter of one 2048-key tile for one digit.  Keys are ranked per warp
+// (match_any), the tile is laid out in digit order in shared memory (stable:
+// input order within a digit), and each digit's run is then written by
+// consecutive threads to consecutive addresses.
 template <typename K, bool kVals>
 __global__ void __launch_bounds__(kSortThreads) radix_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, K *__restrict__ keys_out,
     uint32_t *__restrict__ vals_out, const uint32_t *__restrict__ offsets, int64_t n, int shift,
     uint32_t nblocks) {
   __shared__ uint32_t whist[kSortWarps][256];
+  __shared__ uint32_t dstart[256];  // first tile position of each digit
+  __shared__ uint32_t gofs[256];    // global position of the tile's first key of each digit
+  __shared__ uint32_t wsum[kSortWarps];
+  __shared__ K tk[kSortTile];
+  __shared__ uint32_t tv[kVals ? kSortTile : 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&whist[0][0])[i] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortItems);
+  const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
+  const int64_t base = tile0 + (int64_t)warp * (32 * kSortItems);
   K k[kSortItems];
   uint32_t v[kSortItems];
   uint32_t local[kSortItems];
@@ -179,22 +189,49 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(
   }
   __syncthreads();
   {
-    uint32_t d = threadIdx.x;  // one digit per thread (256 threads)
-    uint32_t run = offsets[(int64_t)d * nblocks + blockIdx.x];
+    // one digit per thread: warp prefixes, then the digit's count in the tile
+    const uint32_t d = threadIdx.x;
+    uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; w++) {
-      uint32_t c = whist[w][d];
+      const uint32_t c = whist[w][d];
       whist[w][d] = run;
       run += c;
     }
+    // exclusive scan of the 256 digit counts over the block
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int w = 0; w < warp; w++) wpre += wsum[w];
+    dstart[d] = wpre + x - run;
+    gofs[d] = offsets[(int64_t)d * nblocks + blockIdx.x];
   }
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
     if (dig[j] < 256u) {
-      uint32_t pos = whist[warp][dig[j]] + local[j];
-      keys_out[pos] = k[j];
-      if (kVals) vals_out[pos] = v[j];
+      const uint32_t pos = dstart[dig[j]] + whist[warp][dig[j]] + local[j];
+      tk[pos] = k[j];
+      if (kVals) tv[pos] = v[j];
+    }
+  }
+  __syncthreads();
+  const int64_t valid = n - tile0 < kSortTile ? n - tile0 : kSortTile;
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const int i = j * kSortThreads + threadIdx.x;
+    if (i < valid) {
+      const K key = tk[i];
+      const uint32_t d = (uint32_t)(key >> shift) & 0xffu;
+      const uint32_t pos = gofs[d] + (uint32_t)i - dstart[d];
+      keys_out[pos] = key;
+      if (kVals) vals_out[pos] = tv[i];
     }
   }
 }
