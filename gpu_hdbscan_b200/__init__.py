@@ -19,6 +19,7 @@ raise HdbError with the library's status and message.
 """
 from __future__ import annotations
 
+import numpy as np
 import ctypes as C
 from dataclasses import dataclass
 
@@ -123,6 +124,25 @@ class Context:
         _lib.check(self.L.hdb_bf16_distance_tiles(self.h, _ptr(X), X.shape[0], X.shape[1],
                                                   _ptr(ids), _ptr(counts), tiles, _ptr(out)))
         return out
+
+    def build_CoreSG(self, ids, dist, X, mst) -> EnhancedGraph:
+        """Core-SG (kNN graph + MST, Euclidean weights) of ids/dist [n, k], X and
+        the sorted MST (MST_EDGE records, e.g. buildMST's output)."""
+        torch = self._torch
+        ids = self._dev(ids, torch.int32)
+        dist = self._dev(dist, torch.float32)
+        X = self._dev(X, torch.float32)
+        if isinstance(mst, np.ndarray) and mst.dtype.names:  # MSTedge records
+            mst = mst.view(np.int32).reshape(-1, 3)
+        mst = self._dev(mst, torch.int32)
+        n, k = ids.shape
+        g = _lib.Graph()
+        _lib.check(self.L.hdb_core_sg(self.h, _ptr(ids), _ptr(dist), _ptr(X), n, X.shape[1], k,
+                                      _ptr(mst), C.byref(g)))
+        empty = torch.empty(0, dtype=torch.int32, device=self.device)
+        return EnhancedGraph(g.nodes, g.edges, self._view(g.nindex, g.nodes + 1, torch.int64),
+                             self._view(g.nlist, g.edges, torch.int32),
+                             self._view(g.eweight, g.edges, torch.float32), empty, g)
 
     def buildEnhancedKNNG(self, ids, dist, X) -> EnhancedGraph:
         torch = self._torch

@@ -24,7 +24,8 @@ HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
-           "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles")
+           "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
+           "hdb_core_sg")
 
 
 class HdbError(RuntimeError):
@@ -92,6 +93,7 @@ def load(path: str = LIB_PATH):
                                   C.POINTER(RunStats)]),
         "hdb_sort_edges_noalloc": (C.c_int, [_P, _I64, _P]),
         "hdb_bf16_distance_tiles": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _I64, _P]),
+        "hdb_core_sg": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, _P, C.POINTER(Graph)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

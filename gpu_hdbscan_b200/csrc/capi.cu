@@ -122,6 +122,20 @@ HDB_API hdb_status hdb_enhanced_knng(hdb_ctx *h, const int32_t *ids, const float
   });
 }
 
+HDB_API hdb_status hdb_core_sg(hdb_ctx *h, const int32_t *ids, const float *dist, const float *X,
+                               int64_t n, int32_t d, int32_t k, const hdb_mst_edge *mst,
+                               hdb_graph *graph) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(ids, "ids");
+    require_ptr(dist, "dist");
+    require_ptr(X, "X");
+    require_ptr(mst, "mst");
+    require_ptr(graph, "graph");
+    build_core_sg(ctx, ids, dist, X, n, d, k, mst, graph);
+  });
+}
+
 HDB_API hdb_status hdb_mst(hdb_ctx *h, const hdb_graph *graph, uint8_t *in_mst, hdb_mst_edge *mst,
                            int32_t *rounds) {
   return guard([&] {

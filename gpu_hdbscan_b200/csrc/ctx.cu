@@ -127,6 +127,9 @@ HDB_API hdb_status hdb_destroy(hdb_ctx *h) {
     cudaFree(c.g_nlist);
     cudaFree(c.g_eweight);
     cudaFree(c.g_antihubs);
+    cudaFree(c.sg_nindex);
+    cudaFree(c.sg_nlist);
+    cudaFree(c.sg_eweight);
     cudaFree(c.dev_err);
     if (c.pinned) cudaFreeHost(c.pinned);
     for (auto &e : c.ev)

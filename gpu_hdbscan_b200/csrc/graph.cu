@@ -315,6 +315,133 @@ __global__ void k_clique(const int32_t *__restrict__ ah, int32_t P, const float 
   }
 }
 
+// ---- Core-SG (HDBSCAN/core-sg/core-sg.cu) -------------------------------------
+// Euclidean distance (euclid_ref rounding) of m pairs (from[e], to[e]) of MST
+// edges: one warp per 32 edges, rows staged like k_core_sqrt.
+__global__ void __launch_bounds__(32 * kCoreWarps)
+    k_edge_euclid(const float *__restrict__ X, int d, const hdb_mst_edge *__restrict__ mst, int64_t m,
+                  float *__restrict__ out) {
+  __shared__ float stage[kCoreWarps][2][32 * kCoreLd];
+  const int lane = lane_id(), w = threadIdx.x >> 5;
+  float *sa = stage[w][0], *sb = stage[w][1];
+  for (int64_t e0 = ((int64_t)blockIdx.x * kCoreWarps + w) * 32; e0 < m;
+       e0 += (int64_t)gridDim.x * kCoreWarps * 32) {
+    const int64_t e = e0 + lane;
+    const bool active = e < m;
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    const int32_t a = active ? mst[e].from_node : 0, b = active ? mst[e].to_node : 0;
+    float soma = 0.0f;
+    for (int c0 = 0; c0 < d; c0 += kCoreCols) {
+      const int wd = min(kCoreCols, d - c0);
+      __syncwarp();
+      for (int i = 0; i < 32; i++) {
+        if (!((act >> i) & 1u)) continue;
+        const int32_t ai = __shfl_sync(0xffffffffu, a, i), bi = __shfl_sync(0xffffffffu, b, i);
+        if (lane < wd) {
+          sa[i * kCoreLd + lane] = X[(int64_t)ai * d + c0 + lane];
+          sb[i * kCoreLd + lane] = X[(int64_t)bi * d + c0 + lane];
+        }
+      }
+      __syncwarp();
+      if (active) {
+        const float *x = sa + lane * kCoreLd, *y = sb + lane * kCoreLd;
+        for (int j = 0; j < wd; j++) {
+          const float diff = __fsub_rn(x[j], y[j]);
+          const double sq = __dmul_rn((double)diff, (double)diff);
+          soma = __double2float_rn(__dadd_rn((double)soma, sq));
+        }
+      }
+    }
+    if (active) out[e] = __fsqrt_rn(soma);
+  }
+}
+
+// Endpoints in [0, n); incident-edge counts; the two row entries of every
+// edge (to_node's first: key = row, value = 2e or 2e + 1).
+__global__ void k_mst_entries(const hdb_mst_edge *__restrict__ mst, int64_t m, int64_t n,
+                              int32_t *__restrict__ mdeg, uint32_t *__restrict__ keys,
+                              uint32_t *__restrict__ vals, uint32_t *err) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = mst[e].from_node, b = mst[e].to_node;
+    if (a < 0 || a >= n || b < 0 || b >= n) {
+      atomicOr(err, DEVERR_ID_RANGE);
+      keys[2 * e] = 0; vals[2 * e] = 0xffffffffu;
+      keys[2 * e + 1] = 0; vals[2 * e + 1] = 0xffffffffu;
+      continue;
+    }
+    atomicAdd(&mdeg[b], 1);
+    atomicAdd(&mdeg[a], 1);
+    keys[2 * e] = (uint32_t)b;
+    vals[2 * e] = (uint32_t)(2 * e);
+    keys[2 * e + 1] = (uint32_t)a;
+    vals[2 * e + 1] = (uint32_t)(2 * e + 1);
+  }
+}
+
+// Reverse entries for Core-SG: key = target row, value = the source's flat
+// list index (source * k + slot), so the entry can carry dist[source][slot].
+__global__ void k_emit_reverse_flat(const int32_t *__restrict__ ids, const uint32_t *__restrict__ mutual,
+                                    const int64_t *__restrict__ off, int64_t n, int k,
+                                    uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  const uint32_t valid = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+  for (; row < n; row += stride) {
+    uint32_t nm = ~mutual[row] & valid;
+    if (lane < k && ((nm >> lane) & 1u)) {
+      int64_t p = off[row] + __popc(nm & lanemask_lt());
+      keys[p] = (uint32_t)ids[row * k + lane];
+      vals[p] = (uint32_t)(row * k + lane);
+    }
+  }
+}
+
+__global__ void k_row_sizes_sg(const int32_t *__restrict__ revcnt, const int32_t *__restrict__ mdeg,
+                               int64_t n, int k, int32_t *__restrict__ sizes) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    sizes[i] = k + revcnt[i] + mdeg[i];
+}
+
+// One warp per row: kNN ids with their distances, the non-mutual sources in
+// ascending order with the source's distance, then the MST neighbours in
+// edge order with the edge's Euclidean distance.
+__global__ void k_fill_sg(const int32_t *__restrict__ ids, const float *__restrict__ dist,
+                          const int64_t *__restrict__ nindex, const int32_t *__restrict__ revcnt,
+                          const int64_t *__restrict__ rev_off, const uint32_t *__restrict__ rev_flat,
+                          const int32_t *__restrict__ mdeg, const int64_t *__restrict__ m_off,
+                          const uint32_t *__restrict__ m_vals, const hdb_mst_edge *__restrict__ mst,
+                          const float *__restrict__ eu, int64_t n, int k,
+                          int32_t *__restrict__ nlist, float *__restrict__ eweight) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
+  for (; row < n; row += stride) {
+    const int64_t base = nindex[row];
+    if (lane < k) {
+      nlist[base + lane] = ids[row * k + lane];
+      eweight[base + lane] = dist[row * k + lane];
+    }
+    const int32_t rc = revcnt[row];
+    const int64_t ro = rev_off[row];
+    for (int t = lane; t < rc; t += 32) {
+      const uint32_t f = rev_flat[ro + t];
+      nlist[base + k + t] = (int32_t)(f / (uint32_t)k);
+      eweight[base + k + t] = dist[f];
+    }
+    const int32_t mc = mdeg[row];
+    const int64_t mo = m_off[row];
+    for (int t = lane; t < mc; t += 32) {
+      const uint32_t v = m_vals[mo + t];
+      const int64_t e = v >> 1;
+      nlist[base + k + rc + t] = (v & 1u) ? mst[e].to_node : mst[e].from_node;
+      eweight[base + k + rc + t] = eu[e];
+    }
+  }
+}
+
 int bits_for(int64_t n) {
   int b = 0;
   while (b < 63 && (int64_t(1) << b) < n) b++;
@@ -451,6 +578,89 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   out->eweight = ctx->g_eweight;
   out->num_antihubs = P;
   out->antihubs = ctx->g_antihubs;
+}
+
+
+void build_core_sg(Context *ctx, const int32_t *ids, const float *dist, const float *X, int64_t n,
+                   int32_t d, int32_t k, const hdb_mst_edge *mst, hdb_graph *out) {
+  HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "core-SG: bad n");
+  HDB_REQUIRE(k >= 1 && k <= 32 && k < n, HDB_ERR_ARG, "core-SG: k must be in [1, 32]");
+  HDB_REQUIRE(d >= 1, HDB_ERR_ARG, "core-SG: bad d");
+  HDB_REQUIRE(n * k < (int64_t(1) << 32) && 2 * (n - 1) < (int64_t(1) << 32), HDB_ERR_ARG,
+              "core-SG: n * k must stay below 2^32");
+  cudaStream_t st = ctx->stream;
+  const int gw = grid_for(ctx, n, kWarpsPerBlock);
+  const int ge = grid_for(ctx, n, 256);
+  const int64_t m = n - 1;
+
+  Buf<int32_t> deg(ctx, n);
+  HDB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(int32_t), st));
+  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  // MST entries (validated with the ids)
+  Buf<int32_t> mdeg(ctx, n);
+  Buf<uint32_t> mkeys(ctx, 2 * m), mvals(ctx, 2 * m);
+  HDB_CUDA(cudaMemsetAsync(mdeg, 0, n * sizeof(int32_t), st));
+  k_mst_entries<<<grid_for(ctx, m, 256), 256, 0, st>>>(mst, m, n, mdeg, mkeys, mvals, ctx->dev_err);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  uint32_t err = ctx->take_dev_err();
+  HDB_REQUIRE(!(err & DEVERR_ID_RANGE), HDB_ERR_ARG,
+              "core-SG: a kNN id or an MST endpoint lies outside [0, n)");
+  HDB_REQUIRE(!(err & DEVERR_SELF_ID), HDB_ERR_ARG, "kNN graph: a row lists its own id");
+  HDB_REQUIRE(!(err & DEVERR_DUP_ID), HDB_ERR_ARG, "kNN graph: an id repeats within a row");
+  radix_sort_u32(ctx, mkeys, mvals, 2 * m, 0, bits_for(n));  // stable: edge order within a row
+  Buf<int64_t> m_off(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, mdeg, m_off, n, m_off.get() + n);
+  Buf<float> eu(ctx, m);
+  k_edge_euclid<<<grid_for(ctx, (m + 31) / 32, kCoreWarps, 8), 32 * kCoreWarps, 0, st>>>(X, d, mst, m,
+                                                                                            eu);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+
+  // mutual flags, reverse entries sorted by target (stable: ascending source)
+  Buf<uint32_t> mutual(ctx, n);
+  Buf<int32_t> revcnt(ctx, n), nonmutual(ctx, n);
+  HDB_CUDA(cudaMemsetAsync(revcnt, 0, n * sizeof(int32_t), st));
+  k_mutual<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, mutual, revcnt, nonmutual); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  Buf<int64_t> roff(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, nonmutual, roff, n, roff.get() + n);
+  ensure_capacity(ctx, (void **)&ctx->sg_nindex, &ctx->sg_nindex_cap, (n + 1) * sizeof(int64_t));
+  {
+    Buf<int32_t> sizes(ctx, n);
+    k_row_sizes_sg<<<ge, 256, 0, st>>>(revcnt, mdeg, n, k, sizes); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    scan_exclusive_i32_i64(ctx, sizes, ctx->sg_nindex, n, ctx->sg_nindex + n);
+  }
+  int64_t *h = static_cast<int64_t *>(ctx->pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, roff.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  HDB_CUDA(cudaMemcpyAsync(h + 1, ctx->sg_nindex + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  const int64_t R = h[0], E = h[1];
+  Buf<uint32_t> rkeys(ctx, R), rvals(ctx, R);
+  k_emit_reverse_flat<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, mutual, roff, n, k, rkeys, rvals);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  radix_sort_u32(ctx, rkeys, rvals, R, 0, bits_for(n));
+  Buf<int64_t> rev_off(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, revcnt, rev_off, n, nullptr);
+
+  ensure_capacity(ctx, (void **)&ctx->sg_nlist, &ctx->sg_nlist_cap, (size_t)E * sizeof(int32_t));
+  ensure_capacity(ctx, (void **)&ctx->sg_eweight, &ctx->sg_eweight_cap, (size_t)E * sizeof(float));
+  k_fill_sg<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, dist, ctx->sg_nindex, revcnt, rev_off, rvals, mdeg,
+                                                m_off, mvals, mst, eu, n, k, ctx->sg_nlist,
+                                                ctx->sg_eweight);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  ctx->sync();
+  out->nodes = (int32_t)n;
+  out->edges = E;
+  out->nindex = ctx->sg_nindex;
+  out->nlist = ctx->sg_nlist;
+  out->eweight = ctx->sg_eweight;
+  out->num_antihubs = 0;
+  out->antihubs = nullptr;
 }
 
 }  // namespace hdb

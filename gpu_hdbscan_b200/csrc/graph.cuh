@@ -17,4 +17,10 @@ void core_distances(Context *ctx, const float *dist, const float *X, const int32
 void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, const float *X,
                          int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times);
 
+// Core-SG (build_CoreSG / Union_kNNG_MST, HDBSCAN/core-sg/core-sg.cu:292-571):
+// the kNN graph's CSR (own ids, non-mutual reverse entries) plus the edges
+// of the sorted MST, with Euclidean weights.  Output in context-owned buffers.
+void build_core_sg(Context *ctx, const int32_t *ids, const float *dist, const float *X, int64_t n,
+                   int32_t d, int32_t k, const hdb_mst_edge *mst, hdb_graph *out);
+
 }  // namespace hdb

@@ -119,6 +119,11 @@ struct Context {
   float *g_eweight = nullptr;
   int32_t *g_antihubs = nullptr;
   size_t g_nindex_cap = 0, g_nlist_cap = 0, g_eweight_cap = 0, g_antihubs_cap = 0;
+  // Persistent outputs of hdb_core_sg.
+  int64_t *sg_nindex = nullptr;
+  int32_t *sg_nlist = nullptr;
+  float *sg_eweight = nullptr;
+  size_t sg_nindex_cap = 0, sg_nlist_cap = 0, sg_eweight_cap = 0;
   cudaEvent_t ev[8] = {};
   // Kernel launches issued by this context (all stages count them).
   int64_t launches = 0;

@@ -142,6 +142,24 @@ HDB_API hdb_status hdb_enhanced_knng(hdb_ctx *ctx, const int32_t *ids, const flo
                                      const float *X, int64_t n, int32_t d, int32_t k,
                                      hdb_graph *graph);
 
+/* build_CoreSG / Union_kNNG_MST, HDBSCAN/core-sg/core-sg.cu:292-571 (the body
+ * of the reference's built hdbscan_ entry, new.cu:92): the core-SG of a kNN
+ * graph, i.e. its CSR (row i = its k kNN ids in list order, then every i'
+ * with a non-mutual edge i'->i in ascending i') joined with the n-1 edges
+ * of `mst`, the sorted MST of its enhanced kNN graph (hdb_mst's output):
+ * each MST edge adds from_node to to_node's row and to_node to from_node's
+ * row, in edge order, after the reverse entries.  eweight is the Euclidean
+ * weight the reference leaves in place: dist[i][j] for kNN and reverse
+ * entries (the distance as given, squared or not) and, for MST entries, the
+ * float-accumulated pow / sqrtf distance of calculates.cu:275-283.  The
+ * arrays are owned by the context (kept until the next hdb_core_sg call or
+ * hdb_destroy); num_antihubs = 0.  ids, dist, X and mst are device memory;
+ * ids are validated like hdb_enhanced_knng's, MST endpoints must lie in
+ * [0, n), and n * k must stay below 2^32 (HDB_ERR_ARG otherwise). */
+HDB_API hdb_status hdb_core_sg(hdb_ctx *ctx, const int32_t *ids, const float *dist, const float *X,
+                               int64_t n, int32_t d, int32_t k, const hdb_mst_edge *mst,
+                               hdb_graph *graph);
+
 /* cpuMST + buildMST, HDBSCAN/mst/mst.cuh:64,91 (mst.cu:34-78, 291-336): the
  * minimum spanning tree under the order (weight, CSR edge index) of the
  * entries whose target exceeds their row, written as MSTedge[n-1] already

@@ -515,6 +515,83 @@ int64_t orc_enhanced_knng(const int32_t *ids, const float *dist, const float *X,
   return E;
 }
 
+/*
+ * Core-SG, HDBSCAN/core-sg/core-sg.cu: the union of the kNN graph and the MST
+ * of the enhanced kNN graph, as build_CoreSG (:477-571) leaves it.
+ *  core_sg_calculate_nindex (:101-145): row i has its k kNN ids, one entry
+ *    i' for every non-mutual edge i'->i, and one entry per incident MST edge;
+ *  core_sg_calculate_nlist (:148-237): kNN ids in list order, then the
+ *    non-mutual sources in ascending order, then the MST neighbours in the
+ *    order of the (sorted, buildMST mst.cu:291-336) MST edge list, the
+ *    to_node row taking from_node before the from_node row takes to_node;
+ *  the weights finally held are the Euclidean ones (update_core_sg_weights,
+ *    :432-471, replaces the MRD weights by the vector written by
+ *    core_sg_calculate_MRD_mst :242-285): the kNN distance for kNN and
+ *    reverse entries (dist[i][j] of the listing row), and the float/pow
+ *    Euclidean distance (calculates.cu:275-283) for MST entries.
+ */
+int64_t orc_core_sg(const int32_t *ids, const float *dist, const float *X, int64_t n, int32_t d,
+                    int32_t k, const orc_mst_edge *mst, int64_t **nindex_out, int32_t **nlist_out,
+                    float **eweight_out) {
+  if (orc_validate_knn(ids, n, k) != ORC_OK) return -1;
+  int64_t *nindex = (int64_t *)calloc(n + 1, sizeof(int64_t));
+  int32_t *flag = (int32_t *)malloc(sizeof(int32_t) * n * k);
+  for (int64_t i = 0; i < n; i++) {
+    int64_t soma = 0;
+    for (int32_t j = 0; j < k; j++) {
+      int64_t neig = ids[i * k + j];
+      int32_t FLAG = 0;
+      for (int32_t t = 0; t < k; t++) FLAG += (ids[neig * k + t] == i);
+      flag[i * k + j] = FLAG;
+      if (FLAG > 1) { nindex[neig + 1] += FLAG - 1; nindex[i + 1] -= (FLAG - 1); }
+      nindex[neig + 1] += 1;
+      if (!FLAG) soma += 1;
+    }
+    nindex[i + 1] += soma;
+  }
+  for (int64_t e = 0; e < n - 1; e++) {
+    nindex[mst[e].to_node + 1] += 1;
+    nindex[mst[e].from_node + 1] += 1;
+  }
+  for (int64_t i = 1; i < n + 1; i++) nindex[i] = nindex[i - 1] + nindex[i];
+  int64_t E = nindex[n];
+  int32_t *nlist = (int32_t *)malloc(sizeof(int32_t) * (E > 0 ? E : 1));
+  float *ew = (float *)malloc(sizeof(float) * (E > 0 ? E : 1));
+  int64_t *aux = (int64_t *)calloc(n, sizeof(int64_t));
+  for (int64_t i = 0; i < n; i++) {
+    int64_t pos = nindex[i] + aux[i];
+    for (int32_t j = 0; j < k; j++) {
+      ew[pos] = dist[i * k + j];
+      nlist[pos++] = ids[i * k + j];
+      aux[i]++;
+    }
+  }
+  for (int64_t i = 0; i < n; i++)
+    for (int32_t j = 0; j < k; j++) {
+      int64_t neig = ids[i * k + j];
+      if (!flag[i * k + j]) {
+        int64_t p = nindex[neig] + aux[neig]++;
+        nlist[p] = (int32_t)i;
+        ew[p] = dist[i * k + j];
+      }
+    }
+  for (int64_t e = 0; e < n - 1; e++) {
+    int32_t to = mst[e].to_node, from = mst[e].from_node;
+    float eu = orc_euclid_ref(X + (int64_t)from * d, X + (int64_t)to * d, d);
+    int64_t pt = nindex[to] + aux[to]++, pf = nindex[from] + aux[from]++;
+    nlist[pt] = from;
+    ew[pt] = eu;
+    nlist[pf] = to;
+    ew[pf] = eu;
+  }
+  free(flag);
+  free(aux);
+  *nindex_out = nindex;
+  *nlist_out = nlist;
+  *eweight_out = ew;
+  return E;
+}
+
 /* ------------------------------------------------------------------------ */
 /* MST                                                                       */
 /* ------------------------------------------------------------------------ */

@@ -57,6 +57,10 @@ int32_t orc_select_antihubs(const int32_t *ids, const int32_t *deg, int64_t n, i
 int64_t orc_enhanced_knng(const int32_t *ids, const float *dist, const float *X, int64_t n,
                           int32_t d, int32_t k, int64_t **nindex_out, int32_t **nlist_out,
                           float **eweight_out, int32_t **antihubs_out, int32_t *num_antihubs_out);
+/* Core-SG (kNN graph + MST), core-sg.cu; returns the edge count or -1. */
+int64_t orc_core_sg(const int32_t *ids, const float *dist, const float *X, int64_t n, int32_t d,
+                    int32_t k, const orc_mst_edge *mst, int64_t **nindex_out, int32_t **nlist_out,
+                    float **eweight_out);
 
 /* ---- MST (HDBSCAN/mst/mst.cu, HDBSCAN/merge_sort/merge_sort.cu) ---- */
 int orc_kruskal(const int64_t *nindex, const int32_t *nlist, const float *eweight, int32_t nodes,

@@ -58,6 +58,7 @@ def lib():
             "orc_degrees": (None, [_P, _I64, _I32, _P]),
             "orc_select_antihubs": (_I32, [_P, _P, _I64, _I32, _P]),
             "orc_enhanced_knng": (_I64, [_P, _P, _P, _I64, _I32, _I32, _P, _P, _P, _P, _P]),
+            "orc_core_sg": (_I64, [_P, _P, _P, _I64, _I32, _I32, _P, _P, _P, _P]),
             "orc_kruskal": (C.c_int, [_P, _P, _P, _I32, _I64, _P]),
             "orc_build_mst": (C.c_int, [_P, _P, _P, _I32, _I64, _P, _P]),
             "orc_sort_edges": (None, [_P, _I64]),
@@ -191,6 +192,25 @@ def enhanced_knng(ids, dist, X):
     ew = _take(pw, E, C.c_float, None)
     ah = _take(pa, nah.value, C.c_int32, None)
     return nindex, nlist, ew, ah
+
+
+def core_sg(ids, dist, X, mst):
+    """Core-SG of a kNN graph and its sorted MST (MST_EDGE records, n-1):
+    (nindex int64[n+1], nlist int32[E], eweight float32[E])."""
+    ids = _c(ids, np.int32)
+    dist = _c(dist, np.float32)
+    X = _c(X, np.float32)
+    mst = np.ascontiguousarray(mst, dtype=MST_EDGE)
+    n, k = ids.shape
+    if len(mst) != n - 1:
+        raise ValueError("the MST must have n - 1 edges")
+    pn, pl, pw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    E = lib().orc_core_sg(_p(ids), _p(dist), _p(X), n, X.shape[1], k, _p(mst), C.byref(pn),
+                          C.byref(pl), C.byref(pw))
+    if E < 0:
+        raise ValueError("invalid kNN graph (id out of range, self id or duplicate id)")
+    return (_take(pn, n + 1, C.c_int64, None), _take(pl, E, C.c_int32, None),
+            _take(pw, E, C.c_float, None))
 
 
 def kruskal(nindex, nlist, eweight):
