@@ -235,6 +235,39 @@ class Context:
         _lib.check(self.L.hdb_run(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels), C.byref(st)))
         return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
 
+    def hdbscan_batched(self, Xs, k=32, mpts=32, sample_num=16, iterations=6,
+                        precision=HDB_PREC_FP32, distance=HDB_DIST_SQRT,
+                        stability=HDB_STAB_FP32, want_graphs=False):
+        """Independent runs of the whole path on every array of Xs in shared
+        launches (hdb_run_batched).  Host arrays run with host_io=1 (copies
+        inside the call); CUDA tensors give device results.
+        -> (labels per instance, cluster counts, stats[, kNN graphs [n, k, 2]
+        with instance-local ids])."""
+        torch = self._torch
+        host = not (isinstance(Xs[0], torch.Tensor) and Xs[0].is_cuda)
+        dev = None if host else self.device
+        Xs = [torch.as_tensor(X, dtype=torch.float32).contiguous() if host
+              else X.to(torch.float32).contiguous() for X in Xs]
+        labels = [torch.empty(X.shape[0], dtype=torch.int32, device=dev) for X in Xs]
+        graphs = [torch.empty((X.shape[0], k, 2), dtype=torch.int32, device=dev) for X in Xs] \
+            if want_graphs else None
+        insts = (_lib.Instance * len(Xs))()
+        for i, X in enumerate(Xs):
+            insts[i].X = X.data_ptr()
+            insts[i].n = X.shape[0]
+            insts[i].d = X.shape[1]
+            insts[i].labels = labels[i].data_ptr()
+            insts[i].G = graphs[i].data_ptr() if want_graphs else None
+        p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
+                        stability, 1 if host else 0)
+        st = _lib.RunStats()
+        _lib.check(self.L.hdb_run_batched(self.h, insts, len(Xs), C.byref(p), C.byref(st)))
+        stats = {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
+        ncl = [insts[i].num_clusters for i in range(len(Xs))]
+        if want_graphs:
+            return labels, ncl, stats, graphs
+        return labels, ncl, stats
+
     def hdbscan_from_knn(self, G, X, k=32, mpts=32, distance=HDB_DIST_SQRT,
                          stability=HDB_STAB_FP32):
         """The stages after the kNN graph (hdb_run_knn): G [n, k, 2] NNDElement rows,

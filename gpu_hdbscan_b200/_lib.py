@@ -25,7 +25,7 @@ EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_se
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
-           "hdb_core_sg")
+           "hdb_core_sg", "hdb_run_batched")
 
 
 class HdbError(RuntimeError):
@@ -58,6 +58,11 @@ class RunStats(C.Structure):
                 ("join_ms", C.c_float), ("join_launches", C.c_int32),
                 ("join_rows_gathered", C.c_int64), ("join_candidates", C.c_int64),
                 ("gpu_launches", C.c_int64)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("X", C.c_void_p), ("n", C.c_int64), ("d", C.c_int32),
+                ("num_clusters", C.c_int32), ("labels", C.c_void_p), ("G", C.c_void_p)]
 
 
 _L = None
@@ -94,6 +99,8 @@ def load(path: str = LIB_PATH):
         "hdb_sort_edges_noalloc": (C.c_int, [_P, _I64, _P]),
         "hdb_bf16_distance_tiles": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _I64, _P]),
         "hdb_core_sg": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, _P, C.POINTER(Graph)]),
+        "hdb_run_batched": (C.c_int, [_P, C.POINTER(Instance), _I32, C.POINTER(Params),
+                                      C.POINTER(RunStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,5 +1,6 @@
 // extern "C" entry points of libhdb_b200 (include/hdb/hdb.h) and the
 // end-to-end pipeline in the reference's HDBSCAN/_new.cu order.
+#include <map>
 #include <vector>
 
 #include "graph.cuh"
@@ -200,22 +201,25 @@ void check_run_params(const hdb_params &p) {
 
 // The stages after the kNN graph (HDBSCAN/_new.cu:243-347) on device arrays:
 // ids [n, k] decoded, core [n], X [n, d] -> labels [n].  Records ev[3..5].
+// With seg, every instance separately; inst_clusters (host) gets the counts.
 void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X, int64_t n,
-                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st) {
+                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st,
+                   const Segments &seg = Segments{}, int32_t *inst_clusters = nullptr) {
   cudaStream_t s = ctx->stream;
   hdb_graph g;
-  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr);
+  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr, seg);
   HDB_CUDA(cudaEventRecord(ctx->ev[3], s));
   int32_t rounds = 0;
-  Buf<hdb_mst_edge> mst(ctx, n - 1);
-  boruvka_mst(ctx, &g, nullptr, mst, &rounds);
+  const int64_t m = n - (seg.count > 0 ? seg.count : 1);
+  Buf<hdb_mst_edge> mst(ctx, m);
+  boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg);
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   int32_t ncl = 0;
   {
-    Buf<hdb_linkage_node> hier(ctx, n - 1);
-    linkage_tree(ctx, mst, n, hier);
+    Buf<hdb_linkage_node> hier(ctx, m);
+    linkage_tree(ctx, mst, n, hier, seg);
     condense_select(ctx, hier, n, p.mpts, p.stability, labels, &ncl, nullptr, nullptr, nullptr,
-                    nullptr);
+                    nullptr, seg, inst_clusters);
   }
   HDB_CUDA(cudaEventRecord(ctx->ev[5], s));
   st->edges = g.edges;
@@ -231,6 +235,145 @@ void fill_times(Context *ctx, hdb_run_stats *st, bool with_knn) {
   st->ms_mst = elapsed(ev[3], ev[4]);
   st->ms_tree = elapsed(ev[4], ev[5]);
   st->ms_total = elapsed(ev[0], ev[6]);
+}
+
+// ---- hdb_run_batched: instances of one d laid back to back -----------------
+// Row-major [rows, d] blocks of several instances copied into one array.
+__global__ void k_pack_rows(const float *const *__restrict__ src, Segments seg, int d,
+                            float *__restrict__ dst) {
+  const int64_t total = seg.off[seg.count] * d;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.of_point(i / d);
+    dst[i] = src[t][i - seg.off[t] * d];
+  }
+}
+
+__global__ void k_unpack_labels(const int32_t *__restrict__ src, Segments seg,
+                                int32_t *const *__restrict__ dst) {
+  const int64_t total = seg.off[seg.count];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.of_point(i);
+    dst[t][i - seg.off[t]] = src[i];
+  }
+}
+
+// Batch ids -> instance-local ids, keeping the old/new sign encoding.
+__global__ void k_local_ids(hdb_nnd_element *__restrict__ G, int k, Segments seg) {
+  const int64_t total = seg.off[seg.count] * k;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t base = seg.off[seg.of_point(i / k)];
+    const int32_t lab = G[i].label_;
+    const int32_t id = lab < 0 ? -lab - 1 : lab;
+    const int32_t local = (int32_t)(id - base);
+    G[i].label_ = lab < 0 ? -local - 1 : local;
+  }
+}
+
+// Runs the instances `idx` (all of dimension d) as one batch.
+void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_t> &idx, int32_t d,
+                     const hdb_params &p, hdb_run_stats *acc, JoinStats *js_acc) {
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t *ev = ctx->ev;
+  const int32_t k = p.knn.k;
+  const int32_t T = (int32_t)idx.size();
+  std::vector<int64_t> off((size_t)T + 1, 0);
+  for (int32_t t = 0; t < T; t++) off[t + 1] = off[t] + insts[idx[t]].n;
+  const int64_t n = off[T];
+  HDB_REQUIRE(n < (int64_t(1) << 30), HDB_ERR_ARG,
+              "hdb_run_batched: the instances of one d must hold fewer than 2^30 points");
+  Buf<int64_t> doff(ctx, T + 1);
+  HDB_CUDA(cudaMemcpyAsync(doff, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  Segments seg;
+  seg.off = doff;
+  seg.host_off = off.data();
+  seg.count = T;
+
+  // inputs: one [n, d] array (used in place when the instances already are one)
+  HDB_CUDA(cudaEventRecord(ev[1], st));
+  bool contiguous = !p.host_io;
+  for (int32_t t = 1; t < T && contiguous; t++)
+    contiguous = insts[idx[t]].X == insts[idx[0]].X + off[t] * d;
+  Buf<float> Xpack;
+  const float *X = insts[idx[0]].X;
+  std::vector<void *> ptrs((size_t)T);
+  Buf<void *> dptrs(ctx, T);
+  if (!contiguous) {
+    Xpack = Buf<float>(ctx, (size_t)n * d);
+    if (p.host_io) {
+      for (int32_t t = 0; t < T; t++)
+        HDB_CUDA(cudaMemcpyAsync(Xpack.get() + off[t] * d, insts[idx[t]].X,
+                                 (size_t)(off[t + 1] - off[t]) * d * sizeof(float),
+                                 cudaMemcpyHostToDevice, st));
+    } else {
+      for (int32_t t = 0; t < T; t++) ptrs[t] = const_cast<float *>(insts[idx[t]].X);
+      HDB_CUDA(cudaMemcpyAsync(dptrs, ptrs.data(), T * sizeof(void *), cudaMemcpyHostToDevice, st));
+      k_pack_rows<<<grid_for(ctx, n * d, 256), 256, 0, st>>>(
+          reinterpret_cast<const float *const *>(dptrs.get()), seg, d, Xpack); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+    }
+    X = Xpack;
+  }
+
+  int64_t dropped = 0;
+  JoinStats js;
+  Buf<int32_t> ids(ctx, (size_t)n * k), labels(ctx, n);
+  Buf<float> core(ctx, n);
+  Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
+  nndescent(ctx, X, n, d, p.knn, G, &dropped, &js, seg);
+  HDB_CUDA(cudaEventRecord(ev[2], st));
+  {
+    Buf<float> dist;
+    if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
+    knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
+    core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, core);
+  }
+  std::vector<int32_t> ncl((size_t)T, 0);
+  hdb_run_stats rs = {};
+  run_after_knn(ctx, ids, core, X, n, d, k, p, labels, &rs, seg, ncl.data());
+
+  // outputs
+  if (p.host_io) {
+    for (int32_t t = 0; t < T; t++)
+      HDB_CUDA(cudaMemcpyAsync(insts[idx[t]].labels, labels.get() + off[t],
+                               (off[t + 1] - off[t]) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  } else {
+    for (int32_t t = 0; t < T; t++) ptrs[t] = insts[idx[t]].labels;
+    HDB_CUDA(cudaMemcpyAsync(dptrs, ptrs.data(), T * sizeof(void *), cudaMemcpyHostToDevice, st));
+    k_unpack_labels<<<grid_for(ctx, n, 256), 256, 0, st>>>(
+        labels, seg, reinterpret_cast<int32_t *const *>(dptrs.get())); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
+  bool want_graph = false;
+  for (int32_t t = 0; t < T; t++) want_graph = want_graph || insts[idx[t]].G != nullptr;
+  if (want_graph) {
+    k_local_ids<<<grid_for(ctx, n * k, 256), 256, 0, st>>>(G, k, seg); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    for (int32_t t = 0; t < T; t++) {
+      hdb_instance &in = insts[idx[t]];
+      if (!in.G) continue;
+      HDB_CUDA(cudaMemcpyAsync(in.G, G.get() + off[t] * k,
+                               (size_t)(off[t + 1] - off[t]) * k * sizeof(hdb_nnd_element),
+                               p.host_io ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  ctx->sync();
+  for (int32_t t = 0; t < T; t++) insts[idx[t]].num_clusters = ncl[t];
+  acc->edges += rs.edges;
+  acc->num_antihubs += rs.num_antihubs;
+  acc->num_clusters += rs.num_clusters;
+  acc->mst_rounds = rs.mst_rounds > acc->mst_rounds ? rs.mst_rounds : acc->mst_rounds;
+  acc->knn_dropped += dropped;
+  acc->ms_knn += elapsed(ev[1], ev[2]);
+  acc->ms_graph += elapsed(ev[2], ev[3]);
+  acc->ms_mst += elapsed(ev[3], ev[4]);
+  acc->ms_tree += elapsed(ev[4], ev[5]);
+  js_acc->ms += js.ms;
+  js_acc->launches += js.launches;
+  js_acc->rows_gathered += js.rows_gathered;
+  js_acc->candidates += js.candidates;
 }
 
 }  // namespace
@@ -286,6 +429,45 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
     if (stats) {
       rs.knn_dropped = dropped;
       fill_times(ctx, &rs, true);
+      rs.join_ms = (float)js.ms;
+      rs.join_launches = (int32_t)js.launches;
+      rs.join_rows_gathered = js.rows_gathered;
+      rs.join_candidates = js.candidates;
+      rs.gpu_launches = ctx->launches - launches0;
+      *stats = rs;
+    }
+  });
+}
+
+HDB_API hdb_status hdb_run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count,
+                                   const hdb_params *params, hdb_run_stats *stats) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(insts, "insts");
+    require_ptr(params, "params");
+    HDB_REQUIRE(count >= 1, HDB_ERR_ARG, "hdb_run_batched: need at least one instance");
+    const hdb_params &p = *params;
+    check_run_params(p);
+    const int32_t k = p.knn.k;
+    // instances grouped by d (ascending), each group in instance order
+    std::map<int32_t, std::vector<int32_t>> groups;
+    for (int32_t i = 0; i < count; i++) {
+      const hdb_instance &in = insts[i];
+      require_ptr(in.X, "instance X");
+      require_ptr(in.labels, "instance labels");
+      HDB_REQUIRE(in.n > k && in.n < (int64_t(1) << 30) && in.d >= 1, HDB_ERR_ARG,
+                  "hdb_run_batched: every instance needs k < n < 2^30 and d >= 1");
+      groups[in.d].push_back(i);
+    }
+    const int64_t launches0 = ctx->launches;
+    hdb_run_stats rs = {};
+    JoinStats js;
+    HDB_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    for (auto &g : groups) run_batch_group(ctx, insts, g.second, g.first, p, &rs, &js);
+    HDB_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
+    ctx->sync();
+    if (stats) {
+      rs.ms_total = elapsed(ctx->ev[0], ctx->ev[6]);
       rs.join_ms = (float)js.ms;
       rs.join_launches = (int32_t)js.launches;
       rs.join_rows_gathered = js.rows_gathered;

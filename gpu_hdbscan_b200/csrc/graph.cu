@@ -8,6 +8,8 @@
 // calculate_coreDistance_antihubs (:412-446).  The reference does these as
 // serial host loops plus sharded 3-GPU kernels; here every step is a
 // single-device pass over HBM-resident arrays.
+#include <vector>
+
 #include "hdb_internal.cuh"
 #include "graph.cuh"
 
@@ -34,16 +36,23 @@ __device__ __forceinline__ float euclid_ref(const float *__restrict__ a,
 
 // One warp per row: validate the row (range, self, duplicates) and count
 // in-degrees (countValues, count.cu:10-19).
-__global__ void k_degrees(const int32_t *__restrict__ ids, int64_t n, int k,
+// With instances, ids must stay inside the row's instance.
+__global__ void k_degrees(const int32_t *__restrict__ ids, int64_t n, int k, Segments seg,
                           int32_t *__restrict__ deg, uint32_t *err) {
   const int lane = lane_id();
   int64_t row = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   const int64_t stride = (int64_t)gridDim.x * kWarpsPerBlock;
   for (; row < n; row += stride) {
     int32_t v = lane < k ? ids[row * k + lane] : -1 - lane;
+    int64_t lo = 0, hi = n;
+    if (seg.count > 0) {
+      const int32_t t = seg.of_point(row);
+      lo = seg.off[t];
+      hi = seg.off[t + 1];
+    }
     uint32_t bad = 0;
     if (lane < k) {
-      if (v < 0 || v >= n) bad |= DEVERR_ID_RANGE;
+      if (v < lo || v >= hi) bad |= DEVERR_ID_RANGE;
       else if (v == row) bad |= DEVERR_SELF_ID;
     }
     uint32_t peers = __match_any_sync(0xffffffffu, v);
@@ -140,6 +149,111 @@ __global__ void k_compact_flags(const int32_t *__restrict__ flag, const int64_t 
     if (flag[i]) out[pos[i]] = (int32_t)i;
 }
 
+// ---- antihubs of independent instances -----------------------------------
+// Every instance takes its own floor(sqrt(n_t)) lowest in-degrees, ties at the
+// threshold by (score, index) -- the set the single-instance selection picks
+// on that instance alone, since that order is (degree, score, index).
+// Sort key: instance << 32 | degree, value: point.  The stable sort keeps
+// equal keys in index order.
+__global__ void k_seg_deg_keys(const int32_t *__restrict__ deg, int64_t n, Segments seg,
+                               uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = ((uint64_t)seg.of_point(i) << 32) | (uint32_t)deg[i];
+    vals[i] = (uint32_t)i;
+  }
+}
+
+struct AhRun {
+  int64_t lb, ub;   // sorted positions of the instance's threshold-degree run
+  int64_t missing;  // how many of the run are antihubs
+  int32_t ties;     // 1: the run is longer than that -> (score, index) tie-break
+  int32_t pad;
+};
+
+// One thread per instance t: P_t = ah_off[t+1] - ah_off[t] antihubs; the P_t-th
+// smallest key of the instance's sorted range [off[t], off[t+1]) fixes the
+// threshold degree and its run [lb, ub).
+__global__ void k_seg_threshold(const uint64_t *__restrict__ keys, Segments seg,
+                                const int64_t *__restrict__ ah_off, AhRun *__restrict__ run) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < seg.count;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = seg.off[t], b = seg.off[t + 1];
+    const int64_t P = ah_off[t + 1] - ah_off[t];
+    const uint64_t kT = keys[a + P - 1];
+    int64_t lo = a, hi = a + P - 1;  // first position with key == kT
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < kT) lo = mid + 1; else hi = mid;
+    }
+    const int64_t lb = lo;
+    lo = a + P - 1;
+    hi = b;  // first position with key > kT
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] <= kT) lo = mid + 1; else hi = mid;
+    }
+    AhRun r;
+    r.lb = lb;
+    r.ub = lo;
+    r.missing = P - (lb - a);
+    r.ties = (lo - lb) > r.missing ? 1 : 0;
+    r.pad = 0;
+    run[t] = r;
+  }
+}
+
+// Per sorted position: below the run -> antihub; in a run that fits -> antihub;
+// in a run that does not -> a tie, decided by (score, index).
+__global__ void k_seg_mark(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                           int64_t n, const AhRun *__restrict__ run, int32_t *__restrict__ is_ah,
+                           int32_t *__restrict__ tie) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const AhRun r = run[keys[p] >> 32];
+    const bool in_run = p >= r.lb && p < r.ub;
+    is_ah[vals[p]] = (p < r.lb || (in_run && !r.ties)) ? 1 : 0;
+    tie[p] = in_run && r.ties;
+  }
+}
+
+// Tied points in sorted-position order with calculateScore's tie score
+// (calculates.cu:21-36), as k_tie_keys computes it.
+__global__ void k_seg_tie_keys(const uint32_t *__restrict__ vals, const int32_t *__restrict__ tie,
+                               const int64_t *__restrict__ tpos, int64_t n,
+                               const int32_t *__restrict__ deg, const int32_t *__restrict__ ids,
+                               int k, uint64_t *__restrict__ tkeys, uint32_t *__restrict__ tvals) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    if (!tie[p]) continue;
+    const uint32_t i = vals[p];
+    int32_t score = 0;
+    for (int j = 0; j < k; j++) score += deg[ids[(int64_t)i * k + j]];
+    tkeys[tpos[p]] = ((uint64_t)(uint32_t)score << 32) | (uint64_t)i;
+    tvals[tpos[p]] = i;
+  }
+}
+
+__global__ void k_seg_tie_inst(const uint32_t *__restrict__ tvals, int64_t cnt, Segments seg,
+                               uint32_t *__restrict__ tinst) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+       q += (int64_t)gridDim.x * blockDim.x)
+    tinst[q] = (uint32_t)seg.of_point(tvals[q]);
+}
+
+// Ties sorted by (instance, score, index): the first `missing` of each
+// instance's run are antihubs.  The run of instance t starts where its first
+// tie sits in the position-ordered tie list.
+__global__ void k_seg_tie_select(const uint32_t *__restrict__ tinst, const uint32_t *__restrict__ tvals,
+                                 int64_t cnt, const AhRun *__restrict__ run,
+                                 const int64_t *__restrict__ tpos, int32_t *__restrict__ is_ah) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const AhRun r = run[tinst[q]];
+    if (q - tpos[r.lb] < r.missing) is_ah[tvals[q]] = 1;
+  }
+}
+
 // One warp per row i: which of i's neighbours list i back (findKNNlist,
 // getters.cu:41-49).  Non-mutual edges i->v become reverse entries of v.
 __global__ void k_mutual(const int32_t *__restrict__ ids, int64_t n, int k,
@@ -175,11 +289,24 @@ __global__ void k_mutual(const int32_t *__restrict__ ids, int64_t n, int k,
   }
 }
 
+// Row length: k own ids, the reverse entries, and for an antihub the other
+// antihubs of its instance.
 __global__ void k_row_sizes(const int32_t *__restrict__ revcnt, const int32_t *__restrict__ is_ah,
-                            int64_t n, int k, int32_t P, int32_t *__restrict__ sizes) {
+                            int64_t n, int k, int32_t P, Segments seg,
+                            const int64_t *__restrict__ ah_off, int32_t *__restrict__ sizes) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    sizes[i] = k + revcnt[i] + (is_ah[i] ? P - 1 : 0);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t clique = 0;
+    if (is_ah[i]) {
+      if (seg.count > 0) {
+        const int32_t t = seg.of_point(i);
+        clique = (int32_t)(ah_off[t + 1] - ah_off[t]) - 1;
+      } else {
+        clique = P - 1;
+      }
+    }
+    sizes[i] = k + revcnt[i] + clique;
+  }
 }
 
 // Emits (v, i) for every non-mutual edge i->v in (i, j) order.
@@ -290,22 +417,30 @@ __global__ void k_gather_rows(const float *__restrict__ X, const int32_t *__rest
     out[t] = X[(int64_t)rows[t / d] * d + (t % d)];
 }
 
-// One block per antihub row: the other antihubs in ascending order with
-// max(MRD, sqrt-L2) weights (calculate_nlist :392-407 and
-// calculate_coreDistance_antihubs :412-446).
-__global__ void k_clique(const int32_t *__restrict__ ah, int32_t P, const float *__restrict__ Xah,
+// One block per antihub row: the other antihubs (of its instance) in
+// ascending order with max(MRD, sqrt-L2) weights (calculate_nlist :392-407
+// and calculate_coreDistance_antihubs :412-446).
+__global__ void k_clique(const int32_t *__restrict__ ah, int32_t P, Segments seg,
+                         const int64_t *__restrict__ ah_off, const float *__restrict__ Xah,
                          int d, const float *__restrict__ core, const int64_t *__restrict__ nindex,
                          const int32_t *__restrict__ revcnt, int k, int32_t *__restrict__ nlist,
                          float *__restrict__ eweight) {
   extern __shared__ float xa[];
-  const int r = blockIdx.x;
+  const int64_t r = blockIdx.x;
   const int32_t a = ah[r];
-  for (int t = threadIdx.x; t < d; t += blockDim.x) xa[t] = Xah[(int64_t)r * d + t];
+  int64_t lo = 0, cnt = P;
+  if (seg.count > 0) {
+    const int32_t t = seg.of_point(a);
+    lo = ah_off[t];
+    cnt = ah_off[t + 1] - lo;
+  }
+  const int64_t rr = r - lo;
+  for (int t = threadIdx.x; t < d; t += blockDim.x) xa[t] = Xah[r * d + t];
   __syncthreads();
   const int64_t base = nindex[a] + k + revcnt[a];
   const float ca = core[a];
-  for (int t = threadIdx.x; t < P - 1; t += blockDim.x) {
-    int o = t < r ? t : t + 1;
+  for (int64_t t = threadIdx.x; t < cnt - 1; t += blockDim.x) {
+    const int64_t o = lo + (t < rr ? t : t + 1);
     int32_t b = ah[o];
     float w = mrd(ca, core[b]);
     float eu = euclid_ref(xa, Xah + (int64_t)o * d, d);
@@ -462,8 +597,46 @@ void core_distances(Context *ctx, const float *dist, const float *X, const int32
   HDB_CHECK_LAUNCH();
 }
 
+// Antihubs of every instance (is_ah[i] = 1 for the chosen points); see
+// k_seg_deg_keys.  ah_off: device prefix sums of the per-instance counts.
+static void select_antihubs_segmented(Context *ctx, const int32_t *deg, const int32_t *ids,
+                                      int64_t n, int32_t k, const Segments &seg,
+                                      const int64_t *ah_off, int32_t *is_ah) {
+  cudaStream_t st = ctx->stream;
+  const int ge = grid_for(ctx, n, 256);
+  Buf<uint64_t> keys(ctx, n);
+  Buf<uint32_t> vals(ctx, n);
+  k_seg_deg_keys<<<ge, 256, 0, st>>>(deg, n, seg, keys, vals); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  radix_sort_u64(ctx, keys, vals, n, 0, 32 + bits_for(seg.count));
+  Buf<AhRun> run(ctx, seg.count);
+  k_seg_threshold<<<grid_for(ctx, seg.count, 128), 128, 0, st>>>(keys, seg, ah_off, run); ctx->launches++;
+  Buf<int32_t> tie(ctx, n);
+  k_seg_mark<<<ge, 256, 0, st>>>(keys, vals, n, run, is_ah, tie); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  Buf<int64_t> tpos(ctx, n + 1);
+  scan_exclusive_i32_i64(ctx, tie, tpos, n, tpos.get() + n);
+  int64_t *h = static_cast<int64_t *>(ctx->pinned);
+  HDB_CUDA(cudaMemcpyAsync(h, tpos.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  const int64_t nt = h[0];
+  if (nt == 0) return;
+  Buf<uint64_t> tkeys(ctx, nt);
+  Buf<uint32_t> tvals(ctx, nt), tinst(ctx, nt);
+  k_seg_tie_keys<<<ge, 256, 0, st>>>(vals, tie, tpos, n, deg, ids, k, tkeys, tvals); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  radix_sort_u64(ctx, tkeys, tvals, nt, 0, 64);
+  const int gt = grid_for(ctx, nt, 256);
+  k_seg_tie_inst<<<gt, 256, 0, st>>>(tvals, nt, seg, tinst); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  radix_sort_u32(ctx, tinst, tvals, nt, 0, bits_for(seg.count));
+  k_seg_tie_select<<<gt, 256, 0, st>>>(tinst, tvals, nt, run, tpos, is_ah); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+}
+
 void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, const float *X,
-                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times) {
+                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times,
+                         const Segments &seg) {
   HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "enhanced kNN graph: bad n");
   HDB_REQUIRE(k >= 1 && k <= 32 && k < n, HDB_ERR_ARG, "enhanced kNN graph: k must be in [1, 32]");
   HDB_REQUIRE(d >= 1, HDB_ERR_ARG, "enhanced kNN graph: bad d");
@@ -474,51 +647,76 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   // 1. in-degrees + validation
   Buf<int32_t> deg(ctx, n);
   HDB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(int32_t), st));
-  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err); ctx->launches++;
+  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, seg, deg, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   uint32_t err = ctx->take_dev_err();
-  HDB_REQUIRE(!(err & DEVERR_ID_RANGE), HDB_ERR_ARG, "kNN graph: neighbour id outside [0, n)");
+  HDB_REQUIRE(!(err & DEVERR_ID_RANGE), HDB_ERR_ARG,
+              seg.count > 0 ? "kNN graph: neighbour id outside its instance"
+                            : "kNN graph: neighbour id outside [0, n)");
   HDB_REQUIRE(!(err & DEVERR_SELF_ID), HDB_ERR_ARG, "kNN graph: a row lists its own id");
   HDB_REQUIRE(!(err & DEVERR_DUP_ID), HDB_ERR_ARG, "kNN graph: an id repeats within a row");
 
   // 2. antihubs: the P = (int)sqrt(n) lowest degrees (get_NumThreshold,
-  //    getters.cu:6-9); ties at the threshold by (score, index).
-  const int32_t P = (int32_t)sqrt((double)n);
-  Buf<uint32_t> hist(ctx, kDegHistBins);
-  Buf<int64_t> thr(ctx, 4);
-  HDB_CUDA(cudaMemsetAsync(hist, 0, kDegHistBins * sizeof(uint32_t), st));
-  k_degree_hist<<<ge, 256, 0, st>>>(deg, n, hist); ctx->launches++;
-  HDB_CHECK_LAUNCH();
-  k_find_threshold<<<1, 1024, 0, st>>>(hist, P, thr); ctx->launches++;
-  HDB_CHECK_LAUNCH();
+  //    getters.cu:6-9); ties at the threshold by (score, index).  With
+  //    instances, floor(sqrt(n_t)) of each.
   int64_t *h = static_cast<int64_t *>(ctx->pinned);
-  HDB_CUDA(cudaMemcpyAsync(h, thr, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  ctx->sync();
-  const int64_t T = h[0], below = h[1], at = h[2];
-  HDB_REQUIRE(T >= 0 && T < kDegHistBins - 1, HDB_ERR_INTERNAL,
-              "antihub threshold degree out of histogram range");
-  const int64_t missing = P - below;
+  int32_t P = (int32_t)sqrt((double)n);
   Buf<int32_t> is_ah(ctx, n);
   Buf<int64_t> pos(ctx, n + 1);
-  Buf<int32_t> flag(ctx, n);
-  k_flag_below<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, is_ah, at == missing ? 1 : 0); ctx->launches++;
-  HDB_CHECK_LAUNCH();
-  if (at > missing) {
-    k_flag_eq<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, flag); ctx->launches++;
+  Buf<int64_t> ah_off;
+  int64_t P_total = P;
+  if (seg.count > 0) {
+    std::vector<int64_t> ho((size_t)seg.count + 1, 0);
+    for (int32_t t = 0; t < seg.count; t++) {
+      const int64_t nt = seg.host_off[t + 1] - seg.host_off[t];
+      HDB_REQUIRE(nt > k, HDB_ERR_ARG, "enhanced kNN graph: every instance needs more than k points");
+      ho[t + 1] = ho[t] + (int64_t)sqrt((double)nt);
+    }
+    P_total = ho[seg.count];
+    ah_off = Buf<int64_t>(ctx, seg.count + 1);
+    HDB_CUDA(cudaMemcpyAsync(ah_off, ho.data(), ho.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                             st));
+    select_antihubs_segmented(ctx, deg, ids, n, k, seg, ah_off, is_ah);
+    P = 0;  // per instance from ah_off
+  } else {
+    Buf<uint32_t> hist(ctx, kDegHistBins);
+    Buf<int64_t> thr(ctx, 4);
+    HDB_CUDA(cudaMemsetAsync(hist, 0, kDegHistBins * sizeof(uint32_t), st));
+    k_degree_hist<<<ge, 256, 0, st>>>(deg, n, hist); ctx->launches++;
     HDB_CHECK_LAUNCH();
-    scan_exclusive_i32_i64(ctx, flag, pos, n, nullptr);
-    Buf<uint64_t> keys(ctx, at);
-    k_tie_keys<<<ge, 256, 0, st>>>(deg, flag, pos, ids, n, k, keys); ctx->launches++;
+    k_find_threshold<<<1, 1024, 0, st>>>(hist, P, thr); ctx->launches++;
     HDB_CHECK_LAUNCH();
-    radix_sort_u64(ctx, keys, nullptr, at, 0, 64);
-    k_mark_selected_ties<<<grid_for(ctx, missing, 256), 256, 0, st>>>(keys, missing, is_ah); ctx->launches++;
+    HDB_CUDA(cudaMemcpyAsync(h, thr, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    const int64_t T = h[0], below = h[1], at = h[2];
+    HDB_REQUIRE(T >= 0 && T < kDegHistBins - 1, HDB_ERR_INTERNAL,
+                "antihub threshold degree out of histogram range");
+    const int64_t missing = P - below;
+    Buf<int32_t> flag(ctx, n);
+    k_flag_below<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, is_ah, at == missing ? 1 : 0); ctx->launches++;
     HDB_CHECK_LAUNCH();
+    if (at > missing) {
+      k_flag_eq<<<ge, 256, 0, st>>>(deg, n, (int32_t)T, flag); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+      scan_exclusive_i32_i64(ctx, flag, pos, n, nullptr);
+      Buf<uint64_t> keys(ctx, at);
+      k_tie_keys<<<ge, 256, 0, st>>>(deg, flag, pos, ids, n, k, keys); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+      radix_sort_u64(ctx, keys, nullptr, at, 0, 64);
+      k_mark_selected_ties<<<grid_for(ctx, missing, 256), 256, 0, st>>>(keys, missing, is_ah); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+    }
   }
   ensure_capacity(ctx, (void **)&ctx->g_antihubs, &ctx->g_antihubs_cap,
-                  (size_t)(P > 0 ? P : 1) * sizeof(int32_t));
+                  (size_t)(P_total > 0 ? P_total : 1) * sizeof(int32_t));
   scan_exclusive_i32_i64(ctx, is_ah, pos, n, pos.get() + n);
   k_compact_flags<<<ge, 256, 0, st>>>(is_ah, pos, n, ctx->g_antihubs); ctx->launches++;
   HDB_CHECK_LAUNCH();
+  if (seg.count > 0) {
+    HDB_CUDA(cudaMemcpyAsync(h, pos.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ctx->sync();
+    HDB_REQUIRE(h[0] == P_total, HDB_ERR_INTERNAL, "antihub selection: wrong count");
+  }
   if (times) HDB_CUDA(cudaEventRecord(times->after_antihubs, st));
 
   // 3. mutual flags and reverse counts
@@ -532,7 +730,7 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   ensure_capacity(ctx, (void **)&ctx->g_nindex, &ctx->g_nindex_cap, (n + 1) * sizeof(int64_t));
   {
     Buf<int32_t> sizes(ctx, n);
-    k_row_sizes<<<ge, 256, 0, st>>>(revcnt, is_ah, n, k, P, sizes); ctx->launches++;
+    k_row_sizes<<<ge, 256, 0, st>>>(revcnt, is_ah, n, k, P, seg, ah_off.get(), sizes); ctx->launches++;
     HDB_CHECK_LAUNCH();
     scan_exclusive_i32_i64(ctx, sizes, ctx->g_nindex, n, ctx->g_nindex + n);
   }
@@ -561,13 +759,14 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   k_fill<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, core, ctx->g_nindex, revcnt, rev_off, rvals, n,
                                              k, ctx->g_nlist, ctx->g_eweight); ctx->launches++;
   HDB_CHECK_LAUNCH();
-  if (P > 1) {
-    Buf<float> Xah(ctx, (size_t)P * d);
-    k_gather_rows<<<grid_for(ctx, (int64_t)P * d, 256), 256, 0, st>>>(X, ctx->g_antihubs, P, d,
-                                                                        Xah); ctx->launches++;
+  if (P_total > (seg.count > 0 ? seg.count : 1)) {  // some clique has two or more members
+    Buf<float> Xah(ctx, (size_t)P_total * d);
+    k_gather_rows<<<grid_for(ctx, P_total * d, 256), 256, 0, st>>>(X, ctx->g_antihubs, P_total, d,
+                                                                     Xah); ctx->launches++;
     HDB_CHECK_LAUNCH();
-    k_clique<<<P, 256, d * sizeof(float), st>>>(ctx->g_antihubs, P, Xah, d, core, ctx->g_nindex,
-                                                revcnt, k, ctx->g_nlist, ctx->g_eweight); ctx->launches++;
+    k_clique<<<(unsigned)P_total, 256, d * sizeof(float), st>>>(
+        ctx->g_antihubs, P, seg, ah_off.get(), Xah, d, core, ctx->g_nindex, revcnt, k,
+        ctx->g_nlist, ctx->g_eweight); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   ctx->sync();
@@ -576,7 +775,7 @@ void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, co
   out->nindex = ctx->g_nindex;
   out->nlist = ctx->g_nlist;
   out->eweight = ctx->g_eweight;
-  out->num_antihubs = P;
+  out->num_antihubs = (int32_t)P_total;
   out->antihubs = ctx->g_antihubs;
 }
 
@@ -595,7 +794,7 @@ void build_core_sg(Context *ctx, const int32_t *ids, const float *dist, const fl
 
   Buf<int32_t> deg(ctx, n);
   HDB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(int32_t), st));
-  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, deg, ctx->dev_err); ctx->launches++;
+  k_degrees<<<gw, 32 * kWarpsPerBlock, 0, st>>>(ids, n, k, Segments{}, deg, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   // MST entries (validated with the ids)
   Buf<int32_t> mdeg(ctx, n);

@@ -14,8 +14,11 @@ struct GraphTimes {
 void core_distances(Context *ctx, const float *dist, const float *X, const int32_t *ids,
                     int64_t n, int32_t d, int32_t k, int32_t mode, float *core);
 
+// seg: independent instances (antihubs and clique per instance); ids must
+// stay inside their row's instance.  Empty for one instance.
 void build_enhanced_knng(Context *ctx, const int32_t *ids, const float *core, const float *X,
-                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times);
+                         int64_t n, int32_t d, int32_t k, hdb_graph *out, GraphTimes *times,
+                         const Segments &seg = Segments{});
 
 // Core-SG (build_CoreSG / Union_kNNG_MST, HDBSCAN/core-sg/core-sg.cu:292-571):
 // the kNN graph's CSR (own ids, non-mutual reverse entries) plus the edges

@@ -171,6 +171,37 @@ inline int grid_for(const Context *ctx, int64_t work, int per_block, int blocks_
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Independent clustering instances laid out back to back in one set of
+// arrays (hdb_run_batched): points [off[t], off[t+1]) belong to instance t.
+// count == 0 is the single-instance case (off unused).  Instance t holds at
+// least two points; its MST edges, and so its linkage-tree ranks, occupy
+// [off[t] - t, off[t+1] - t - 1) of the batch's sorted MST.
+struct Segments {
+  const int64_t *off = nullptr;       // device [count + 1]
+  const int64_t *host_off = nullptr;  // the same offsets in host memory
+  int32_t count = 0;
+#ifdef __CUDACC__
+  // Instance of point p: the largest t with off[t] <= p.
+  __device__ __forceinline__ int32_t of_point(int64_t p) const {
+    int32_t lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int32_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(off + mid) <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+  }
+  // Instance of MST / linkage rank r: the largest t with off[t] - t <= r.
+  __device__ __forceinline__ int32_t of_rank(int64_t r) const {
+    int32_t lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int32_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(off + mid) - mid <= r) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+  }
+#endif
+};
+
 // ---------------------------------------------------------------------------
 // Device helpers
 // ---------------------------------------------------------------------------

@@ -112,7 +112,10 @@ __device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int
   return s;
 }
 
-__global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
+// With instances (seg.count > 0) every row draws from its own instance with
+// the instance-local position and size, so an instance starts from the graph
+// a run on that instance alone starts from.
+__global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Segments seg,
                        int32_t *__restrict__ gid, float *__restrict__ gdist,
                        float *__restrict__ worst) {
   extern __shared__ float smem_stage[];
@@ -121,17 +124,25 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k,
   float *sm = smem_stage + (threadIdx.x >> 5) * kStageFloats;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
+    int64_t base = 0, cnt = n;
+    if (seg.count > 0) {
+      const int32_t t = seg.of_point(row);
+      base = seg.off[t];
+      cnt = seg.off[t + 1] - base;
+    }
+    const int64_t lrow = row - base;
     // InitKNNGraphIndexKernel (nndescent.cu:1673-1692): xorshift64star(pos) % n,
     // advanced past the row itself -- and here also past ids already taken.
-    int64_t label = (int64_t)(xorshift64star((uint64_t)(row * k + lane)) % (uint64_t)n);
+    int64_t label = (int64_t)(xorshift64star((uint64_t)(lrow * k + lane)) % (uint64_t)cnt);
     for (int t = 0; t < k; t++) {
       while (true) {
         int64_t c = __shfl_sync(0xffffffffu, label, t);
         bool dup = (lane < t) && (label == c);
-        if (c != row && __ballot_sync(0xffffffffu, dup) == 0) break;
-        if (lane == t) label = (label + 1) % n;
+        if (c != lrow && __ballot_sync(0xffffffffu, dup) == 0) break;
+        if (lane == t) label = (label + 1) % cnt;
       }
     }
+    label += base;
     const float ds = diffsum_staged(X, d, row, (int32_t)label, lane < k, sm);
     uint64_t key = ~0ull;
     if (lane < k) key = pack(ds, (int32_t)label);
@@ -880,7 +891,7 @@ static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
 }
 
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
-               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js) {
+               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js, const Segments &seg) {
   const int k = p.k, S = p.sample_num;
   HDB_REQUIRE(k >= 1 && k <= kMaxK, HDB_ERR_ARG, "NN-Descent: k must be in [1, 32]");
   HDB_REQUIRE(S >= 1 && 2 * S <= k, HDB_ERR_ARG,
@@ -918,7 +929,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
-  k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, gid, gdist, worst); ctx->launches++;
+  k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, seg, gid, gdist, worst); ctx->launches++;
   HDB_CHECK_LAUNCH();
   const int dp = (d & 1) ? d : d + 1;
   const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);

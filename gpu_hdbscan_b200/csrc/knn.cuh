@@ -11,8 +11,11 @@ struct JoinStats {
   int64_t launches = 0, rows_gathered = 0, candidates = 0;
 };
 
+// seg: independent instances in one run (each row's neighbours stay inside
+// its instance); empty for one instance.  Every instance needs more than k rows.
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
-               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr);
+               hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr,
+               const Segments &seg = Segments{});
 // BF16 tensor-core distances for explicit slot lists (hdb_bf16_distance_tiles).
 void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
                          const int32_t *counts, int64_t tiles, float *out);

@@ -228,6 +228,15 @@ __global__ void k_edge_keys(const hdb_mst_edge *__restrict__ e, int64_t m, uint3
   }
 }
 
+__global__ void k_edge_instance(const hdb_mst_edge *__restrict__ e, int64_t m, Segments seg,
+                                uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    keys[t] = (uint32_t)seg.of_point(e[t].from_node);
+    vals[t] = (uint32_t)t;
+  }
+}
+
 __global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint32_t *__restrict__ idx,
                                 int64_t m, hdb_mst_edge *__restrict__ out) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
@@ -238,9 +247,11 @@ __global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint3
 }  // namespace
 
 void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
-                 int32_t *rounds_out) {
+                 int32_t *rounds_out, const Segments &seg) {
   const int64_t n = g->nodes;
   HDB_REQUIRE(n >= 2, HDB_ERR_ARG, "MST: need at least 2 nodes");
+  // one tree per instance: n - (number of instances) edges
+  const int64_t me = n - (seg.count > 0 ? seg.count : 1);
   HDB_REQUIRE(g->edges < (int64_t(1) << 32), HDB_ERR_ARG, "MST: 2^32 or more edges");
   cudaStream_t st = ctx->stream;
   const int gw = grid_for(ctx, n, kWarps);
@@ -280,7 +291,7 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
     const int gr = grid_for(ctx, nr, 256);
     k_min_edge<<<ge, 256, 0, st>>>(ep, m, minkey); ctx->launches++;
     k_winner<<<ge, 256, 0, st>>>(ep, m, minkey, other); ctx->launches++;
-    k_hook<<<gr, 256, 0, st>>>(rp, nr, minkey, other, parent, keys, counters, n - 1); ctx->launches++;
+    k_hook<<<gr, 256, 0, st>>>(rp, nr, minkey, other, parent, keys, counters, me); ctx->launches++;
     k_reset_minkey<<<gr, 256, 0, st>>>(rp, nr, minkey); ctx->launches++;
     k_jump<<<gr, 256, 0, st>>>(rp, nr, parent, ctx->dev_err); ctx->launches++;
     HDB_CUDA(cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(unsigned long long), st));
@@ -301,12 +312,28 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
     HDB_CUDA(cudaMemcpyAsync(h, counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ctx->sync();
   }
-  HDB_REQUIRE((rounds == 0 ? h[0] : chosen) == n - 1, HDB_ERR_DISCONNECTED,
-              "MST does not have n-1 edges: the enhanced kNN graph is disconnected");
-  radix_sort_u64(ctx, keys, nullptr, n - 1, 0, 64);
+  HDB_REQUIRE((rounds == 0 ? h[0] : chosen) == me, HDB_ERR_DISCONNECTED,
+              seg.count > 0
+                  ? "MST forest does not have n - instances edges: an instance's enhanced kNN "
+                    "graph is disconnected"
+                  : "MST does not have n-1 edges: the enhanced kNN graph is disconnected");
+  radix_sort_u64(ctx, keys, nullptr, me, 0, 64);
   if (in_mst) HDB_CUDA(cudaMemsetAsync(in_mst, 0, g->edges, st));
-  k_gather_mst<<<grid_for(ctx, n - 1, 256), 256, 0, st>>>(keys, n - 1, g->nindex, g->nlist,
-                                                          g->eweight, n, mst, in_mst); ctx->launches++;
+  const int gm = grid_for(ctx, me, 256);
+  if (seg.count > 1) {
+    // each instance's edges together, in (weight, edge index) order inside it
+    Buf<hdb_mst_edge> tmp(ctx, me);
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, me, g->nindex, g->nlist, g->eweight, n, tmp, in_mst); ctx->launches++;
+    Buf<uint32_t> ikeys(ctx, me), idx(ctx, me);
+    k_edge_instance<<<gm, 256, 0, st>>>(tmp, me, seg, ikeys, idx); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    int bits = 1;
+    while (bits < 31 && (int64_t(1) << bits) < seg.count) bits++;
+    radix_sort_u32(ctx, ikeys, idx, me, 0, bits);
+    k_permute_edges<<<gm, 256, 0, st>>>(tmp, idx, me, mst); ctx->launches++;
+  } else {
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, me, g->nindex, g->nlist, g->eweight, n, mst, in_mst); ctx->launches++;
+  }
   HDB_CHECK_LAUNCH();
   ctx->sync();
   if (rounds_out) *rounds_out = rounds;

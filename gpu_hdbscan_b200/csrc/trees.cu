@@ -183,12 +183,22 @@ __global__ void k_link_out(const hdb_mst_edge *__restrict__ mst, const int32_t *
 // ---------------------------------------------------------------------------
 enum : int8_t { KIND_SPLIT = 0, KIND_BOTHSMALL = 1, KIND_LEFTBIG = 2, KIND_RIGHTBIG = 3 };
 
+// A single-linkage tree, or a forest with one tree per instance (seg):
+// internal node n + r for rank r < m, where m = n - (number of trees).
 struct TreeView {
   const hdb_linkage_node *h;
   int64_t n;  // points
+  int64_t m;  // internal nodes
   int32_t mpts;
+  Segments seg;
   __device__ __forceinline__ int32_t sz(int64_t x) const {
     return x < n ? 1 : h[x - n].node_size;
+  }
+  // Root of its tree: the last rank of the tree's instance.
+  __device__ __forceinline__ bool is_root(int64_t r) const {
+    if (seg.count == 0) return r == m - 1;
+    const int32_t t = seg.of_rank(r);
+    return r == seg.off[t + 1] - t - 2;
   }
 };
 
@@ -200,7 +210,7 @@ __device__ __forceinline__ float lambda_of(float w) {
 // Hierarchy input check: children are earlier nodes and sizes add up, so
 // parent pointers always go to larger ids (every upward walk ends at the root).
 __global__ void k_validate_hier(TreeView t, uint32_t *err) {
-  const int64_t m = t.n - 1;
+  const int64_t m = t.m;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     hdb_linkage_node h = t.h[r];
@@ -216,7 +226,7 @@ __global__ void k_validate_hier(TreeView t, uint32_t *err) {
 __global__ void k_nodes(TreeView t, int32_t *__restrict__ par, int8_t *__restrict__ side,
                         int8_t *__restrict__ kind, int8_t *__restrict__ visited,
                         float *__restrict__ lam) {
-  const int64_t m = t.n - 1;
+  const int64_t m = t.m;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     hdb_linkage_node h = t.h[r];
@@ -227,7 +237,7 @@ __global__ void k_nodes(TreeView t, int32_t *__restrict__ par, int8_t *__restric
     side[h.right_node] = 1;
     bool lb = t.sz(h.left_node) >= t.mpts, rb = t.sz(h.right_node) >= t.mpts;
     kind[r] = (lb && rb) ? KIND_SPLIT : (!lb && !rb) ? KIND_BOTHSMALL : lb ? KIND_LEFTBIG : KIND_RIGHTBIG;
-    visited[r] = (r == m - 1) || h.node_size >= t.mpts;
+    visited[r] = t.is_root(r) || h.node_size >= t.mpts;
     lam[r] = lambda_of(h.weight);
   }
 }
@@ -238,12 +248,12 @@ __global__ void k_path_init(TreeView t, const int32_t *__restrict__ par, const i
                             const int8_t *__restrict__ kind, const int8_t *__restrict__ visited,
                             int32_t *__restrict__ jmp, int64_t *__restrict__ dep,
                             int64_t *__restrict__ pre, int32_t *__restrict__ head) {
-  const int64_t m = t.n - 1;
+  const int64_t m = t.m;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     if (!visited[r]) { jmp[r] = -1; head[r] = -1; continue; }
     int64_t x = t.n + r;
-    if (r == m - 1) {  // root
+    if (t.is_root(r)) {
       jmp[r] = -1; dep[r] = 0; pre[r] = 0; head[r] = (int32_t)r;
       continue;
     }
@@ -313,15 +323,48 @@ __global__ void k_split_emit(int64_t m, const int32_t *__restrict__ flag, const 
 
 // Cluster ids: root = n; the t-th split node in BFS order gives n+1+2t (left)
 // and n+2+2t (right).  cid is indexed by internal-node rank r (-1 otherwise).
+// A forest numbers its clusters tree after tree: the splits are sorted by
+// (instance, BFS order), split q of instance s gives indices s+1+2q and
+// s+2+2q, and instance s's root the index just before its first split's.
 __global__ void k_assign_cids(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
-                              int32_t *__restrict__ cid, int32_t *__restrict__ split_rank) {
+                              const uint32_t *__restrict__ split_inst, int32_t *__restrict__ cid,
+                              int32_t *__restrict__ split_rank) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ns;
        q += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = split_nodes[q];
+    const int64_t base = split_inst ? split_inst[q] : 0;
     hdb_linkage_node h = t.h[r];
-    cid[h.left_node - t.n] = (int32_t)(t.n + 1 + 2 * q);
-    cid[h.right_node - t.n] = (int32_t)(t.n + 2 + 2 * q);
+    cid[h.left_node - t.n] = (int32_t)(t.n + base + 1 + 2 * q);
+    cid[h.right_node - t.n] = (int32_t)(t.n + base + 2 + 2 * q);
     split_rank[r] = (int32_t)q;
+  }
+}
+
+__global__ void k_split_inst(const uint32_t *__restrict__ split_nodes, int64_t ns, Segments seg,
+                             uint32_t *__restrict__ inst) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ns;
+       q += (int64_t)gridDim.x * blockDim.x)
+    inst[q] = (uint32_t)seg.of_rank(split_nodes[q]);
+}
+
+// One thread per instance s: its root's cluster index croot[s] = s + 2 *
+// (splits of earlier instances), the root node's cid, and cseg of the root.
+__global__ void k_forest_roots(TreeView t, const uint32_t *__restrict__ split_inst, int64_t ns,
+                               int32_t *__restrict__ cid, int32_t *__restrict__ croot,
+                               int32_t *__restrict__ cseg, int64_t C) {
+  const int32_t T = t.seg.count;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= T;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    if (s == T) { croot[T] = (int32_t)C; continue; }
+    int64_t lo = 0, hi = ns;  // first split of an instance >= s
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if ((int64_t)split_inst[mid] < s) lo = mid + 1; else hi = mid;
+    }
+    const int64_t c = s + 2 * lo;
+    croot[s] = (int32_t)c;
+    cseg[c] = (int32_t)s;
+    cid[t.seg.off[s + 1] - s - 2] = (int32_t)(t.n + c);
   }
 }
 
@@ -335,14 +378,17 @@ __global__ void k_node_cluster(int64_t m, int64_t n, const int8_t *__restrict__ 
 }
 
 __global__ void k_cluster_info(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
+                               const uint32_t *__restrict__ split_inst,
                                const int32_t *__restrict__ ncl, const float *__restrict__ lam,
                                float *__restrict__ birth, int32_t *__restrict__ cparent,
-                               int32_t *__restrict__ ckid0) {
+                               int32_t *__restrict__ ckid0, int32_t *__restrict__ cseg) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ns;
        q += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = split_nodes[q];
     int32_t pc = ncl[r];  // cluster whose chain ends at this split
-    int32_t c0 = (int32_t)(1 + 2 * q), c1 = (int32_t)(2 + 2 * q);
+    const int32_t base = split_inst ? (int32_t)split_inst[q] : 0;
+    int32_t c0 = (int32_t)(base + 1 + 2 * q), c1 = c0 + 1;
+    if (cseg) cseg[c0] = cseg[c1] = base;
     birth[c0] = lam[r];
     birth[c1] = lam[r];
     cparent[c0] = pc - (int32_t)t.n;
@@ -543,14 +589,15 @@ __global__ void k_stability(int64_t C, const int64_t *__restrict__ seg_start,
 }
 
 // Excess of mass, bottom-up: the last of two siblings to finish continues
-// with their parent (get_clusters, tree.cu:692-725).  Index 0 is the root,
-// which the reference never evaluates.
+// with their parent (get_clusters, tree.cu:692-725).  Roots (the clusters
+// without a parent: index 0, or one per tree of a forest) are never
+// evaluated, as in the reference.
 __global__ void k_eom(int64_t C, const int32_t *__restrict__ ckid0, const int32_t *__restrict__ cparent,
                       const float *__restrict__ stab, const double *__restrict__ stab64, int fp64,
                       float *sub, double *sub64, int8_t *self_sel, int32_t *arrive) {
   for (int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < C;
        c0 += (int64_t)gridDim.x * blockDim.x) {
-    if (c0 == 0 || ckid0[c0] >= 0) continue;  // start from leaf clusters
+    if (cparent[c0] < 0 || ckid0[c0] >= 0) continue;  // start from leaf clusters
     int64_t c = c0;
     // leaf: no children -> subtree stability 0, never above its own
     volatile float *vsub = sub;
@@ -560,7 +607,7 @@ __global__ void k_eom(int64_t C, const int32_t *__restrict__ ckid0, const int32_
     self_sel[c] = 1;
     for (int64_t guard = 0; guard < C; guard++) {
       int64_t p = cparent[c];
-      if (p <= 0) break;  // parent is the root
+      if (p < 0 || cparent[p] < 0) break;  // parent is a root
       __threadfence();
       if (atomicAdd(&arrive[p], 1) == 0) break;  // sibling not done yet
       __threadfence();
@@ -583,13 +630,13 @@ __global__ void k_eom(int64_t C, const int32_t *__restrict__ ckid0, const int32_
   }
 }
 
-// Nearest self-selected proper ancestor (root excluded) by doubling.
+// Nearest self-selected proper ancestor (roots excluded) by doubling.
 __global__ void k_sel_init(int64_t C, const int32_t *__restrict__ cparent, const int8_t *__restrict__ self_sel,
                            int32_t *__restrict__ jmp, int8_t *__restrict__ anc) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
        c += (int64_t)gridDim.x * blockDim.x) {
-    int32_t p = c == 0 ? -1 : cparent[c];
-    if (p <= 0) { jmp[c] = -1; anc[c] = 0; }
+    int32_t p = cparent[c];
+    if (p < 0 || cparent[p] < 0) { jmp[c] = -1; anc[c] = 0; }
     else { jmp[c] = p; anc[c] = self_sel[p]; }
   }
 }
@@ -606,11 +653,12 @@ __global__ void k_sel_jump(int64_t C, const int32_t *__restrict__ jmp, const int
   }
 }
 
-__global__ void k_selected(int64_t C, const int8_t *__restrict__ self_sel, const int8_t *__restrict__ anc,
+__global__ void k_selected(int64_t C, const int32_t *__restrict__ cparent,
+                           const int8_t *__restrict__ self_sel, const int8_t *__restrict__ anc,
                            int32_t *__restrict__ sel) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
        c += (int64_t)gridDim.x * blockDim.x)
-    sel[c] = (c > 0 && self_sel[c] && !anc[c]) ? 1 : 0;
+    sel[c] = (cparent[c] >= 0 && self_sel[c] && !anc[c]) ? 1 : 0;
 }
 
 // Selected cluster covering each cluster (itself or nearest selected ancestor).
@@ -620,8 +668,8 @@ __global__ void k_cover_init(int64_t C, const int32_t *__restrict__ cparent, con
        c += (int64_t)gridDim.x * blockDim.x) {
     if (sel[c]) { cover[c] = (int32_t)c; jmp[c] = -1; continue; }
     cover[c] = -1;
-    int32_t p = c == 0 ? -1 : cparent[c];
-    jmp[c] = p > 0 ? p : -1;
+    int32_t p = cparent[c];
+    jmp[c] = (p >= 0 && cparent[p] >= 0) ? p : -1;
   }
 }
 
@@ -663,11 +711,21 @@ __global__ void k_points(TreeView t, const int32_t *__restrict__ par, const int3
   }
 }
 
+// Label of a selected cluster: its rank among the selected clusters of its
+// tree (a forest restarts the count at each instance's root).
 __global__ void k_label_map(int64_t C, const int32_t *__restrict__ sel, const int32_t *__restrict__ pos,
+                            const int32_t *__restrict__ cseg, const int32_t *__restrict__ croot,
                             int32_t *__restrict__ label_of) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < C;
        c += (int64_t)gridDim.x * blockDim.x)
-    label_of[c] = sel[c] ? pos[c] : -1;
+    label_of[c] = sel[c] ? pos[c] - (cseg ? pos[croot[cseg[c]]] : 0) : -1;
+}
+
+__global__ void k_inst_clusters(int32_t T, const int32_t *__restrict__ pos,
+                                const int32_t *__restrict__ croot, int32_t *__restrict__ out) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < T;
+       s += (int64_t)gridDim.x * blockDim.x)
+    out[s] = pos[croot[s + 1]] - pos[croot[s]];
 }
 
 __global__ void k_condensed_rows(TreeView t, const uint32_t *__restrict__ split_nodes, int64_t ns,
@@ -742,10 +800,11 @@ int bits_for(int64_t v) {
 
 }  // namespace
 
-void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_node *out) {
+void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_node *out,
+                  const Segments &seg) {
   HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 30), HDB_ERR_ARG, "linkage tree: bad n");
   cudaStream_t st = ctx->stream;
-  const int64_t m = n - 1, total = 2 * n - 1;
+  const int64_t m = n - (seg.count > 0 ? seg.count : 1), total = n + m;
   Buf<int32_t> la(ctx, m), lb(ctx, m), ufp(ctx, total), maxr(ctx, total), seen(ctx, total),
       acc(ctx, total), size(ctx, total);
   const int gm = grid_for(ctx, m, 256), gt = grid_for(ctx, total, 256);
@@ -775,12 +834,17 @@ void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_
 void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t mpts,
                      int32_t stab_mode, int32_t *labels, int32_t *num_clusters,
                      hdb_condensed_node *condensed, int64_t *condensed_size,
-                     hdb_stability *stability, int64_t *num_stability) {
+                     hdb_stability *stability, int64_t *num_stability, const Segments &seg,
+                     int32_t *inst_clusters) {
   HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 30), HDB_ERR_ARG, "condensed tree: bad n");
   HDB_REQUIRE(mpts >= 2, HDB_ERR_ARG, "condensed tree: mpts (min cluster size) must be >= 2");
+  const bool forest = seg.count > 0;
+  HDB_REQUIRE(!forest || (!condensed && !stability), HDB_ERR_ARG,
+              "condensed tree: condensed rows and stabilities are per single tree");
   cudaStream_t st = ctx->stream;
-  const int64_t m = n - 1, total = 2 * n - 1;
-  TreeView t{h, n, mpts};
+  const int64_t trees = forest ? seg.count : 1;
+  const int64_t m = n - trees, total = n + m;
+  TreeView t{h, n, m, mpts, seg};
   const int gm = grid_for(ctx, m, 256), gn = grid_for(ctx, n, 256);
   int64_t *hp = static_cast<int64_t *>(ctx->pinned);
   int32_t *hflag = reinterpret_cast<int32_t *>(hp + 8);
@@ -836,20 +900,35 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   HDB_CUDA(cudaMemcpyAsync(hp, pos.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   ctx->sync();
   const int64_t ns = hp[0];
-  const int64_t C = 1 + 2 * ns;
+  const int64_t C = trees + 2 * ns;
   Buf<uint64_t> skeys(ctx, ns > 0 ? ns : 1);
-  Buf<uint32_t> snodes(ctx, ns > 0 ? ns : 1);
-  Buf<int32_t> cid(ctx, m), split_rank(ctx, m);
+  Buf<uint32_t> snodes(ctx, ns > 0 ? ns : 1), sinst;
+  Buf<int32_t> cid(ctx, m), split_rank(ctx, m), cseg, croot;
   HDB_CUDA(cudaMemsetAsync(cid, 0xff, m * sizeof(int32_t), st));
+  if (forest) {
+    sinst = Buf<uint32_t>(ctx, ns > 0 ? ns : 1);
+    cseg = Buf<int32_t>(ctx, C);
+    croot = Buf<int32_t>(ctx, trees + 1);
+  }
   if (ns > 0) {
     k_split_emit<<<gm, 256, 0, st>>>(m, flag, pos, d0, p0, skeys, snodes); ctx->launches++;
     HDB_CHECK_LAUNCH();
     radix_sort_u64(ctx, skeys, snodes, ns, 0, 64);
-    k_assign_cids<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, cid, split_rank); ctx->launches++;
+    if (forest) {  // (instance, BFS order)
+      k_split_inst<<<grid_for(ctx, ns, 256), 256, 0, st>>>(snodes, ns, seg, sinst); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+      radix_sort_u32(ctx, sinst, snodes, ns, 0, bits_for(seg.count));
+    }
+    k_assign_cids<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, sinst.get(), cid,
+                                                           split_rank); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
-  // root cluster id
-  {
+  // root cluster ids
+  if (forest) {
+    k_forest_roots<<<grid_for(ctx, trees + 1, 256), 256, 0, st>>>(t, sinst, ns, cid, croot, cseg,
+                                                                   C); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  } else {
     int32_t root_cid = (int32_t)n;
     HDB_CUDA(cudaMemcpyAsync(cid.get() + (m - 1), &root_cid, sizeof(int32_t),
                              cudaMemcpyHostToDevice, st));
@@ -870,8 +949,8 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
   HDB_CUDA(cudaMemsetAsync(arrive, 0, C * sizeof(int32_t), st));
   HDB_CUDA(cudaMemsetAsync(self_sel, 0, C, st));
   if (ns > 0) {
-    k_cluster_info<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, ncl, lam, birth,
-                                                            cparent, ckid0); ctx->launches++;
+    k_cluster_info<<<grid_for(ctx, ns, 256), 256, 0, st>>>(t, snodes, ns, sinst.get(), ncl, lam,
+                                                            birth, cparent, ckid0, cseg.get()); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
 
@@ -930,12 +1009,12 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
       std::swap(aa, ab);
       if (!hflag[0]) break;
     }
-    k_selected<<<gc, 128, 0, st>>>(C, self_sel, aa, sel); ctx->launches++;
+    k_selected<<<gc, 128, 0, st>>>(C, cparent, self_sel, aa, sel); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   Buf<int32_t> selpos(ctx, C + 1), label_of(ctx, C);
   scan_exclusive_i32_i32(ctx, sel, selpos, C, selpos.get() + C);
-  k_label_map<<<gc, 128, 0, st>>>(C, sel, selpos, label_of); ctx->launches++;
+  k_label_map<<<gc, 128, 0, st>>>(C, sel, selpos, cseg.get(), croot.get(), label_of); ctx->launches++;
   k_cover_init<<<gc, 128, 0, st>>>(C, cparent, sel, cj, cover); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int32_t *cov_final = cover;
@@ -965,6 +1044,13 @@ void condense_select(Context *ctx, const hdb_linkage_node *h, int64_t n, int32_t
                                condensed ? pcl.get() : nullptr, condensed ? plam.get() : nullptr); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemcpyAsync(hflag, selpos.get() + C, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  Buf<int32_t> icl;
+  if (forest && inst_clusters) {
+    icl = Buf<int32_t>(ctx, trees);
+    k_inst_clusters<<<grid_for(ctx, trees, 256), 256, 0, st>>>(seg.count, selpos, croot, icl); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    HDB_CUDA(cudaMemcpyAsync(inst_clusters, icl, trees * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  }
   if (condensed) {
     const int64_t rows = n + 2 * ns;
     Buf<hdb_condensed_node> tmp(ctx, rows);

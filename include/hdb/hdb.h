@@ -204,6 +204,30 @@ HDB_API hdb_status hdb_run_knn(hdb_ctx *ctx, const hdb_nnd_element *G, const flo
                                int32_t d, const hdb_params *params, int32_t *labels,
                                hdb_run_stats *stats);
 
+/* One clustering instance of hdb_run_batched. */
+typedef struct {
+  const float *X;          /* [n, d] float32 row-major */
+  int64_t n;               /* points; n > params->knn.k */
+  int32_t d;
+  int32_t num_clusters;    /* out: clusters found in this instance */
+  int32_t *labels;         /* out: [n], -1 = noise, clusters 0.. per instance */
+  hdb_nnd_element *G;      /* optional out (NULL to skip): [n, k] final kNN rows,
+                              ids local to the instance, flags as hdb_nndescent */
+} hdb_instance;
+
+/* hdb_run_batched -- many independent HDBSCAN runs (the hdbscan_ flow of
+ * HDBSCAN/_new.cu on each instance) in shared kernel launches: instances of
+ * equal d are laid back to back and every stage runs once over all of them,
+ * each instance's kNN lists, antihubs, clique, MST tree, condensed tree and
+ * cluster selection staying inside the instance.  Per instance the result is
+ * what hdb_run computes on that instance alone from the same kNN graph (the
+ * NN-Descent initial graph is the same too: ids are drawn with
+ * instance-local positions).  insts is a HOST array of `count` descriptors;
+ * X, labels and G are device pointers, or host pointers with
+ * params->host_io = 1.  stats (optional) sums the stages over all instances. */
+HDB_API hdb_status hdb_run_batched(hdb_ctx *ctx, hdb_instance *insts, int32_t count,
+                                   const hdb_params *params, hdb_run_stats *stats);
+
 /* hdb_bf16_distance_tiles -- a diagnostic with no counterpart in the
  * reference: the distances the BF16 tensor-core local join of hdb_nndescent
  * computes, for given slot lists instead of NN-Descent's samples.  Tile t
