@@ -41,7 +41,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="blobs_20m_d128")
-    ap.add_argument("--precision", choices=["fp32", "bf16"], default="bf16")
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default=None,
+                    help="form (default: bf16; fp32 for the batched workloads)")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="batched workloads: only the first N instances (0: all)")
+    ap.add_argument("--loop-instances", type=int, default=256,
+                    help="batched workloads: instances timed in the per-instance loop comparison")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the other form (plain FP32 vs BF16-TC)")
     ap.add_argument("--recall-queries", type=int, default=1000)
@@ -392,9 +397,212 @@ def run_ours(args, w):
         dist.destroy_process_group()
 
 
+def batch_cpu_sample(bw, layout, min_points=50_000):
+    """The first instances of the layout up to `min_points` points, built on
+    the host (numpy) for the CPU timing."""
+    from gpu_hdbscan_b200 import synth
+    Xs, tot = [], 0
+    for i, (n, d, b) in enumerate(layout):
+        Xs.append(synth.generate(synth.batch_instance(bw, i, n, d, b)))
+        tot += n
+        if tot >= min_points:
+            break
+    return Xs
+
+
+def cpu_batch_run(bw, Xs):
+    """The reference algorithm per instance on the host cores (oracle port);
+    an instance whose graph is disconnected is timed up to its failure, as
+    the reference stops there."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    for X in Xs:
+        ids, _ = O.nndescent(X, bw.k, bw.sample_num, bw.iterations)
+        try:
+            O.hdbscan_from_knn(ids, O.fix_distances(X, ids), X, bw.mpts)
+        except RuntimeError:
+            pass
+    dt = time.perf_counter() - t0
+    npts = sum(len(X) for X in Xs)
+    return {"value": npts / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"the first {len(Xs)} instance(s) of {bw.name} ({npts} points, d in "
+                      f"{sorted({X.shape[1] for X in Xs})}, k={bw.k}, mpts={bw.mpts}), one run "
+                      f"each, oracle port (NN-Descent + enhanced kNNG + Kruskal + trees)"}
+
+
+def run_reference_batch(args, bw):
+    from gpu_hdbscan_b200 import synth
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    layout = synth.batch_layout(bw, args.instances or None)
+    Xs = batch_cpu_sample(bw, layout)
+    vals = [cpu_batch_run(bw, Xs) for _ in range(max(1, args.steps))]
+    cb = vals[-1]
+    cb["value"] = statistics.median(v["value"] for v in vals)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": bw.name, "instances": len(layout),
+                                             "k": bw.k, "mpts": bw.mpts},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_batch(args, bw):
+    """Many independent instances (hdb_run_batched) against a per-instance
+    loop of hdb_run over the first --loop-instances of them."""
+    import torch
+    import torch.distributed as dist
+
+    import gpu_hdbscan_b200 as g
+    from gpu_hdbscan_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
+    rbw = synth.BatchWorkload(**{**bw.__dict__, "seed": bw.seed + 1000 * rank})
+    views, layout = synth.generate_batch_torch(rbw, device=dev, count=args.instances or None)
+    n_total = sum(n for n, _, _ in layout)
+    ctx = g.Context(local)
+    kw = dict(k=bw.k, mpts=bw.mpts, sample_num=bw.sample_num, iterations=bw.iterations,
+              precision=prec)
+    kw_b = {**kw, "strict": False}
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        out = []
+        e0.record(stream)
+        for _ in range(steps):
+            out.append(fn())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1), dev), out
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_max, outs = timed(lambda: ctx.hdbscan_batched(views, **kw_b), args.steps, args.warmup)
+    clk = clocks.stop()
+    stats = [o[2] for o in outs]
+    value = whole_job_rate(n_total, args.steps, world, ms_max)
+    failed = sum(1 for s_ in stats[-1]["instance_status"] if s_ != 0)
+
+    # per-instance loop (hdb_run per instance) against the batch on the same
+    # instances; the loop skips the instances the batch found disconnected
+    # (hdb_run stops on them, as the reference does)
+    m = min(args.loop_instances, len(views))
+    sub = [v for v, s_ in zip(views[:m], stats[-1]["instance_status"][:m]) if s_ == 0]
+    n_sub = sum(len(v) for v in sub)
+    lms, _ = timed(lambda: [ctx.hdbscan(v, **kw) for v in sub], 1, 1)
+    bms, _ = timed(lambda: ctx.hdbscan_batched(sub, **kw_b), 1, 1)
+    loop = {"instances": len(sub), "points": n_sub,
+            "loop_points_per_s": round(n_sub / (lms / 1e3), 1), "loop_ms": round(lms, 3),
+            "batched_points_per_s": round(n_sub / (bms / 1e3), 1), "batched_ms": round(bms, 3),
+            "speedup": round(lms / bms, 3)}
+
+    e2e = None
+    if not args.no_e2e:
+        hosts = [v.cpu() for v in views]
+        try:
+            hosts = [h.pin_memory() for h in hosts]
+            pinned = True
+        except RuntimeError:
+            pinned = False
+        ctx.hdbscan_batched(hosts, **kw_b)
+        te, _ = timed(lambda: ctx.hdbscan_batched(hosts, **kw_b), args.steps, 0)
+        e2e = {"value": whole_job_rate(n_total, args.steps, world, te), "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(v.numel() for v in views) * 4),
+               "d2h_bytes_per_step": int(n_total * 4), "pinned_inputs": pinned}
+        del hosts
+
+    if rank == 0:
+        hbm, _, peak_kind = measured_peaks()
+        last = stats[-1]
+        S = bw.sample_num
+        launches = max(1, last["join_launches"])
+        per_d = {}
+        for n, d, _ in layout:
+            per_d[d] = per_d.get(d, 0) + n
+        if prec == g.HDB_PREC_BF16:
+            row_bytes = {d: ((d + 63) // 64 * 64) * 2 for d in per_d}
+            jkernel = "k_join_tc"
+        else:
+            row_bytes = {d: d * 4 for d in per_d}
+            jkernel = "k_join"
+        # gathered rows are not split by d in the stats: weight the row size by points
+        mean_row = sum(row_bytes[d] * c for d, c in per_d.items()) / n_total
+        join_bytes = (last["join_rows_gathered"] * mean_row
+                      + bw.iterations * n_total * (2 * 2 * S * 4 + 2 * 4 + 2 * 1)
+                      + last["join_candidates"] * (8 + 4 + 4))
+        achieved = join_bytes / (last["join_ms"] / 1e3) / 1e9
+        roofline = {"kernel": jkernel + " (NN-Descent local join, all batches)", "bound": "hbm",
+                    "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                    "algorithmic_bytes_per_launch": round(join_bytes / launches),
+                    "avg_launch_ms": round(last["join_ms"] / launches, 4)}
+        cb = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cb = cpu_batch_run(rbw, batch_cpu_sample(rbw, layout))
+            except Exception as e:
+                cb = {"error": f"{type(e).__name__}: {e}"}
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if prec == g.HDB_PREC_FP32 else "bf16", "data": "synthetic",
+                "config": {"workload": bw.name, "instances": len(layout), "n_total": n_total,
+                           "points_per_d": {str(d): c for d, c in sorted(per_d.items())},
+                           "k": bw.k, "mpts": bw.mpts, "sample_num": bw.sample_num,
+                           "iterations": bw.iterations, "form": args.precision,
+                           "parallelism": f"replicas{world}",
+                           "l2": f"inputs larger than L2 ({sum(v.numel() for v in views) * 4 / 1e9:.1f} GB)",
+                           "stage_ms": {s_: round(last[f"ms_{s_}"], 3) for s_ in
+                                        ("knn", "graph", "mst", "tree", "total")},
+                           "num_clusters": last["num_clusters"], "edges": last["edges"],
+                           "knn_dropped": last["knn_dropped"],
+                           "disconnected_instances": failed, "per_instance_loop": loop},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+                "gpu_launches": int(sum(s_["gpu_launches"] for s_ in stats))}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     from gpu_hdbscan_b200 import synth
+    if args.workload in synth.BATCH_WORKLOADS:
+        bw = synth.BATCH_WORKLOADS[args.workload]
+        if args.precision is None:
+            args.precision = "fp32"
+        if args.impl == "reference":
+            run_reference_batch(args, bw)
+        else:
+            run_ours_batch(args, bw)
+        return
+    if args.precision is None:
+        args.precision = "bf16"
     w = synth.WORKLOADS[args.workload]
     if args.n and args.n != w.n:
         blobs = max(1, round(w.blobs * args.n / w.n))

@@ -237,32 +237,54 @@ class Context:
 
     def hdbscan_batched(self, Xs, k=32, mpts=32, sample_num=16, iterations=6,
                         precision=HDB_PREC_FP32, distance=HDB_DIST_SQRT,
-                        stability=HDB_STAB_FP32, want_graphs=False):
+                        stability=HDB_STAB_FP32, want_graphs=False, strict=True):
         """Independent runs of the whole path on every array of Xs in shared
         launches (hdb_run_batched).  Host arrays run with host_io=1 (copies
         inside the call); CUDA tensors give device results.
         -> (labels per instance, cluster counts, stats[, kNN graphs [n, k, 2]
-        with instance-local ids])."""
+        with instance-local ids]).  stats["instance_status"] holds each
+        instance's status; an instance whose enhanced kNN graph is disconnected
+        raises HdbError when strict, else keeps labels -1 and status
+        HDB_ERR_DISCONNECTED while the others complete."""
+        p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
+                        stability, 0)
+        return self._batched(self.L.hdb_run_batched, Xs, None, k, p, want_graphs, strict)
+
+    def hdbscan_batched_from_knn(self, Gs, Xs, k=32, mpts=32, distance=HDB_DIST_SQRT,
+                                 stability=HDB_STAB_FP32, strict=True):
+        """The stages after the kNN graph on many instances in shared launches
+        (hdb_run_knn_batched): Gs[i] [n_i, k, 2] NNDElement rows with
+        instance-local ids, Xs[i] [n_i, d_i].  -> (labels, cluster counts, stats)."""
+        p = _lib.Params(_lib.KnnParams(k, max(1, k // 2), 0, HDB_PREC_FP32), mpts, distance,
+                        stability, 0)
+        return self._batched(self.L.hdb_run_knn_batched, Xs, Gs, k, p, False, strict)
+
+    def _batched(self, fn, Xs, Gs, k, p, want_graphs, strict):
         torch = self._torch
         host = not (isinstance(Xs[0], torch.Tensor) and Xs[0].is_cuda)
         dev = None if host else self.device
+        p.host_io = 1 if host else 0
         Xs = [torch.as_tensor(X, dtype=torch.float32).contiguous() if host
               else X.to(torch.float32).contiguous() for X in Xs]
+        if Gs is not None:
+            Gs = [torch.as_tensor(G).to(dtype=torch.int32).contiguous() if host
+                  else G.to(device=self.device, dtype=torch.int32).contiguous() for G in Gs]
         labels = [torch.empty(X.shape[0], dtype=torch.int32, device=dev) for X in Xs]
         graphs = [torch.empty((X.shape[0], k, 2), dtype=torch.int32, device=dev) for X in Xs] \
-            if want_graphs else None
+            if want_graphs else Gs
         insts = (_lib.Instance * len(Xs))()
         for i, X in enumerate(Xs):
             insts[i].X = X.data_ptr()
             insts[i].n = X.shape[0]
             insts[i].d = X.shape[1]
             insts[i].labels = labels[i].data_ptr()
-            insts[i].G = graphs[i].data_ptr() if want_graphs else None
-        p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
-                        stability, 1 if host else 0)
+            insts[i].G = graphs[i].data_ptr() if graphs is not None else None
         st = _lib.RunStats()
-        _lib.check(self.L.hdb_run_batched(self.h, insts, len(Xs), C.byref(p), C.byref(st)))
+        rc = fn(self.h, insts, len(Xs), C.byref(p), C.byref(st))
+        if rc != _lib.HDB_OK and (strict or rc != _lib.HDB_ERR_DISCONNECTED):
+            _lib.check(rc)
         stats = {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
+        stats["instance_status"] = [insts[i].status for i in range(len(Xs))]
         ncl = [insts[i].num_clusters for i in range(len(Xs))]
         if want_graphs:
             return labels, ncl, stats, graphs

@@ -25,7 +25,7 @@ EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_se
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
-           "hdb_core_sg", "hdb_run_batched")
+           "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched")
 
 
 class HdbError(RuntimeError):
@@ -62,7 +62,8 @@ class RunStats(C.Structure):
 
 class Instance(C.Structure):
     _fields_ = [("X", C.c_void_p), ("n", C.c_int64), ("d", C.c_int32),
-                ("num_clusters", C.c_int32), ("labels", C.c_void_p), ("G", C.c_void_p)]
+                ("num_clusters", C.c_int32), ("labels", C.c_void_p), ("G", C.c_void_p),
+                ("status", C.c_int32), ("reserved", C.c_int32)]
 
 
 _L = None
@@ -101,6 +102,8 @@ def load(path: str = LIB_PATH):
         "hdb_core_sg": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, _P, C.POINTER(Graph)]),
         "hdb_run_batched": (C.c_int, [_P, C.POINTER(Instance), _I32, C.POINTER(Params),
                                       C.POINTER(RunStats)]),
+        "hdb_run_knn_batched": (C.c_int, [_P, C.POINTER(Instance), _I32, C.POINTER(Params),
+                                          C.POINTER(RunStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

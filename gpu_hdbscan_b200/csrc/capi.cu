@@ -201,25 +201,22 @@ void check_run_params(const hdb_params &p) {
 
 // The stages after the kNN graph (HDBSCAN/_new.cu:243-347) on device arrays:
 // ids [n, k] decoded, core [n], X [n, d] -> labels [n].  Records ev[3..5].
-// With seg, every instance separately; inst_clusters (host) gets the counts.
 void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X, int64_t n,
-                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st,
-                   const Segments &seg = Segments{}, int32_t *inst_clusters = nullptr) {
+                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st) {
   cudaStream_t s = ctx->stream;
   hdb_graph g;
-  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr, seg);
+  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr);
   HDB_CUDA(cudaEventRecord(ctx->ev[3], s));
   int32_t rounds = 0;
-  const int64_t m = n - (seg.count > 0 ? seg.count : 1);
-  Buf<hdb_mst_edge> mst(ctx, m);
-  boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg);
+  Buf<hdb_mst_edge> mst(ctx, n - 1);
+  boruvka_mst(ctx, &g, nullptr, mst, &rounds);
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   int32_t ncl = 0;
   {
-    Buf<hdb_linkage_node> hier(ctx, m);
-    linkage_tree(ctx, mst, n, hier, seg);
+    Buf<hdb_linkage_node> hier(ctx, n - 1);
+    linkage_tree(ctx, mst, n, hier);
     condense_select(ctx, hier, n, p.mpts, p.stability, labels, &ncl, nullptr, nullptr, nullptr,
-                    nullptr, seg, inst_clusters);
+                    nullptr);
   }
   HDB_CUDA(cudaEventRecord(ctx->ev[5], s));
   st->edges = g.edges;
@@ -259,6 +256,138 @@ __global__ void k_unpack_labels(const int32_t *__restrict__ src, Segments seg,
   }
 }
 
+__global__ void k_pack_graph(const hdb_nnd_element *const *__restrict__ src, Segments seg, int k,
+                             hdb_nnd_element *__restrict__ dst) {
+  const int64_t total = seg.off[seg.count] * k;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.of_point(i / k);
+    dst[i] = src[t][i - seg.off[t] * k];
+  }
+}
+
+// Instance-local ids -> batch ids, keeping the old/new sign encoding; an id
+// outside its instance becomes n (outside every instance), which the graph
+// validation then rejects.
+__global__ void k_global_ids(hdb_nnd_element *__restrict__ G, int k, Segments seg) {
+  const int64_t n = seg.off[seg.count];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * k;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.of_point(i / k);
+    const int64_t base = seg.off[t], cnt = seg.off[t + 1] - base;
+    const int32_t lab = G[i].label_;
+    const int64_t id = lab < 0 ? -(int64_t)lab - 1 : (int64_t)lab;
+    const int64_t gid = id < cnt ? base + id : n;
+    G[i].label_ = (int32_t)(lab < 0 ? -gid - 1 : gid);
+  }
+}
+
+// MST edges of the connected instances only, their points renumbered without
+// the dropped instances' (pshift[t]: points of dropped instances before t;
+// eshift[t]: their MST edges).  The edges come grouped by instance.
+__global__ void k_compact_mst(const hdb_mst_edge *__restrict__ in, int64_t m, Segments seg,
+                              const int32_t *__restrict__ keep, const int64_t *__restrict__ pshift,
+                              const int64_t *__restrict__ eshift, hdb_mst_edge *__restrict__ out) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    hdb_mst_edge x = in[e];
+    const int32_t t = seg.of_point(x.from_node);
+    if (!keep[t]) continue;
+    x.from_node -= (int32_t)pshift[t];
+    x.to_node -= (int32_t)pshift[t];
+    out[e - eshift[t]] = x;
+  }
+}
+
+__global__ void k_expand_labels(const int32_t *__restrict__ kept_labels, Segments seg,
+                                const int32_t *__restrict__ keep, const int64_t *__restrict__ pshift,
+                                int32_t *__restrict__ labels) {
+  const int64_t total = seg.off[seg.count];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.of_point(i);
+    labels[i] = keep[t] ? kept_labels[i - pshift[t]] : -1;
+  }
+}
+
+// The stages after the kNN graph for a batch: enhanced graph, MST forest,
+// then the trees of the instances whose graph is connected (the others get
+// status HDB_ERR_DISCONNECTED and labels -1).  Records ev[3..5].
+void batch_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X,
+                     int64_t n, int32_t d, int32_t k, const hdb_params &p, int32_t *labels,
+                     hdb_run_stats *st, const Segments &seg, int32_t *ncl, int32_t *status) {
+  cudaStream_t s = ctx->stream;
+  const int32_t T = seg.count;
+  hdb_graph g;
+  build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr, seg);
+  HDB_CUDA(cudaEventRecord(ctx->ev[3], s));
+  int32_t rounds = 0;
+  Buf<hdb_mst_edge> mst(ctx, n - T);
+  std::vector<int32_t> iedges((size_t)T);
+  const int64_t chosen = boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg, iedges.data());
+  HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
+  std::vector<int32_t> keep((size_t)T);
+  std::vector<int64_t> pshift((size_t)T), eshift((size_t)T), off2(1, 0);
+  int64_t dp = 0, de = 0;
+  for (int32_t t = 0; t < T; t++) {
+    const int64_t nt = seg.host_off[t + 1] - seg.host_off[t];
+    keep[t] = iedges[t] == nt - 1;
+    pshift[t] = dp;
+    eshift[t] = de;
+    status[t] = keep[t] ? HDB_OK : HDB_ERR_DISCONNECTED;
+    if (keep[t]) {
+      off2.push_back(off2.back() + nt);
+    } else {
+      dp += nt;
+      de += iedges[t];
+    }
+  }
+  const int32_t K = (int32_t)off2.size() - 1;
+  std::vector<int32_t> ncl2((size_t)K, 0);
+  int32_t total_cl = 0;
+  if (K == T) {
+    Buf<hdb_linkage_node> hier(ctx, n - T);
+    linkage_tree(ctx, mst, n, hier, seg);
+    condense_select(ctx, hier, n, p.mpts, p.stability, labels, &total_cl, nullptr, nullptr,
+                    nullptr, nullptr, seg, ncl2.data());
+  } else {
+    const int64_t n2 = off2[K];
+    Buf<int32_t> dkeep(ctx, T);
+    Buf<int64_t> dps(ctx, T), des(ctx, T), doff2(ctx, K + 1);
+    HDB_CUDA(cudaMemcpyAsync(dkeep, keep.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    HDB_CUDA(cudaMemcpyAsync(dps, pshift.data(), T * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    HDB_CUDA(cudaMemcpyAsync(des, eshift.data(), T * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    HDB_CUDA(cudaMemcpyAsync(doff2, off2.data(), (K + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                             s));
+    Buf<int32_t> lab2(ctx, n2 > 0 ? n2 : 1);
+    if (K > 0) {
+      Buf<hdb_mst_edge> mst2(ctx, n2 - K);
+      if (chosen > 0) {
+        k_compact_mst<<<grid_for(ctx, chosen, 256), 256, 0, s>>>(mst, chosen, seg, dkeep, dps, des,
+                                                                mst2); ctx->launches++;
+        HDB_CHECK_LAUNCH();
+      }
+      Segments seg2;
+      seg2.off = doff2;
+      seg2.host_off = off2.data();
+      seg2.count = K;
+      Buf<hdb_linkage_node> hier(ctx, n2 - K);
+      linkage_tree(ctx, mst2, n2, hier, seg2);
+      condense_select(ctx, hier, n2, p.mpts, p.stability, lab2, &total_cl, nullptr, nullptr,
+                      nullptr, nullptr, seg2, ncl2.data());
+    }
+    k_expand_labels<<<grid_for(ctx, n, 256), 256, 0, s>>>(lab2, seg, dkeep, dps, labels); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    ctx->sync();
+  }
+  for (int32_t t = 0, j = 0; t < T; t++) ncl[t] = keep[t] ? ncl2[j++] : 0;
+  HDB_CUDA(cudaEventRecord(ctx->ev[5], s));
+  st->edges = g.edges;
+  st->num_antihubs = g.num_antihubs;
+  st->num_clusters = total_cl;
+  st->mst_rounds = rounds;
+}
+
 // Batch ids -> instance-local ids, keeping the old/new sign encoding.
 __global__ void k_local_ids(hdb_nnd_element *__restrict__ G, int k, Segments seg) {
   const int64_t total = seg.off[seg.count] * k;
@@ -272,9 +401,10 @@ __global__ void k_local_ids(hdb_nnd_element *__restrict__ G, int k, Segments seg
   }
 }
 
-// Runs the instances `idx` (all of dimension d) as one batch.
+// Runs the instances `idx` (all of dimension d) as one batch.  from_knn: the
+// instances' G are input kNN graphs (hdb_run_knn_batched) instead of outputs.
 void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_t> &idx, int32_t d,
-                     const hdb_params &p, hdb_run_stats *acc, JoinStats *js_acc) {
+                     const hdb_params &p, hdb_run_stats *acc, JoinStats *js_acc, bool from_knn) {
   cudaStream_t st = ctx->stream;
   cudaEvent_t *ev = ctx->ev;
   const int32_t k = p.knn.k;
@@ -322,7 +452,24 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
   Buf<int32_t> ids(ctx, (size_t)n * k), labels(ctx, n);
   Buf<float> core(ctx, n);
   Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
-  nndescent(ctx, X, n, d, p.knn, G, &dropped, &js, seg);
+  if (from_knn) {
+    if (p.host_io) {
+      for (int32_t t = 0; t < T; t++)
+        HDB_CUDA(cudaMemcpyAsync(G.get() + off[t] * k, insts[idx[t]].G,
+                                 (size_t)(off[t + 1] - off[t]) * k * sizeof(hdb_nnd_element),
+                                 cudaMemcpyHostToDevice, st));
+    } else {
+      for (int32_t t = 0; t < T; t++) ptrs[t] = insts[idx[t]].G;
+      HDB_CUDA(cudaMemcpyAsync(dptrs, ptrs.data(), T * sizeof(void *), cudaMemcpyHostToDevice, st));
+      k_pack_graph<<<grid_for(ctx, n * k, 256), 256, 0, st>>>(
+          reinterpret_cast<const hdb_nnd_element *const *>(dptrs.get()), seg, k, G); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+    }
+    k_global_ids<<<grid_for(ctx, n * k, 256), 256, 0, st>>>(G, k, seg); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  } else {
+    nndescent(ctx, X, n, d, p.knn, G, &dropped, &js, seg);
+  }
   HDB_CUDA(cudaEventRecord(ev[2], st));
   {
     Buf<float> dist;
@@ -330,9 +477,9 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
     knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
     core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, core);
   }
-  std::vector<int32_t> ncl((size_t)T, 0);
+  std::vector<int32_t> ncl((size_t)T, 0), status((size_t)T, HDB_OK);
   hdb_run_stats rs = {};
-  run_after_knn(ctx, ids, core, X, n, d, k, p, labels, &rs, seg, ncl.data());
+  batch_after_knn(ctx, ids, core, X, n, d, k, p, labels, &rs, seg, ncl.data(), status.data());
 
   // outputs
   if (p.host_io) {
@@ -347,7 +494,7 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
     HDB_CHECK_LAUNCH();
   }
   bool want_graph = false;
-  for (int32_t t = 0; t < T; t++) want_graph = want_graph || insts[idx[t]].G != nullptr;
+  for (int32_t t = 0; t < T && !from_knn; t++) want_graph = want_graph || insts[idx[t]].G != nullptr;
   if (want_graph) {
     k_local_ids<<<grid_for(ctx, n * k, 256), 256, 0, st>>>(G, k, seg); ctx->launches++;
     HDB_CHECK_LAUNCH();
@@ -360,7 +507,10 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
     }
   }
   ctx->sync();
-  for (int32_t t = 0; t < T; t++) insts[idx[t]].num_clusters = ncl[t];
+  for (int32_t t = 0; t < T; t++) {
+    insts[idx[t]].num_clusters = ncl[t];
+    insts[idx[t]].status = status[t];
+  }
   acc->edges += rs.edges;
   acc->num_antihubs += rs.num_antihubs;
   acc->num_clusters += rs.num_clusters;
@@ -439,8 +589,12 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
   });
 }
 
-HDB_API hdb_status hdb_run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count,
-                                   const hdb_params *params, hdb_run_stats *stats) {
+}  // extern "C"
+
+namespace {
+
+hdb_status run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count, const hdb_params *params,
+                       hdb_run_stats *stats, bool from_knn) {
   return guard([&] {
     Context *ctx = C(h);
     require_ptr(insts, "insts");
@@ -452,18 +606,37 @@ HDB_API hdb_status hdb_run_batched(hdb_ctx *h, hdb_instance *insts, int32_t coun
     // instances grouped by d (ascending), each group in instance order
     std::map<int32_t, std::vector<int32_t>> groups;
     for (int32_t i = 0; i < count; i++) {
-      const hdb_instance &in = insts[i];
+      hdb_instance &in = insts[i];
       require_ptr(in.X, "instance X");
       require_ptr(in.labels, "instance labels");
+      if (from_knn) require_ptr(in.G, "instance G");
       HDB_REQUIRE(in.n > k && in.n < (int64_t(1) << 30) && in.d >= 1, HDB_ERR_ARG,
                   "hdb_run_batched: every instance needs k < n < 2^30 and d >= 1");
+      in.status = HDB_OK;
+      in.num_clusters = 0;
       groups[in.d].push_back(i);
     }
     const int64_t launches0 = ctx->launches;
     hdb_run_stats rs = {};
     JoinStats js;
     HDB_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
-    for (auto &g : groups) run_batch_group(ctx, insts, g.second, g.first, p, &rs, &js);
+    // consecutive instances of one d, up to kBatchPoints points per batch
+    // (bounds the per-point working memory of NN-Descent, ~1.5 KB a point)
+    constexpr int64_t kBatchPoints = int64_t(1) << 25;
+    for (auto &g : groups) {
+      std::vector<int32_t> part;
+      int64_t pts = 0;
+      for (int32_t i : g.second) {
+        if (!part.empty() && pts + insts[i].n > kBatchPoints) {
+          run_batch_group(ctx, insts, part, g.first, p, &rs, &js, from_knn);
+          part.clear();
+          pts = 0;
+        }
+        part.push_back(i);
+        pts += insts[i].n;
+      }
+      run_batch_group(ctx, insts, part, g.first, p, &rs, &js, from_knn);
+    }
     HDB_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
     ctx->sync();
     if (stats) {
@@ -475,7 +648,26 @@ HDB_API hdb_status hdb_run_batched(hdb_ctx *h, hdb_instance *insts, int32_t coun
       rs.gpu_launches = ctx->launches - launches0;
       *stats = rs;
     }
+    int32_t failed = 0;
+    for (int32_t i = 0; i < count; i++) failed += insts[i].status != HDB_OK;
+    HDB_REQUIRE(failed == 0, HDB_ERR_DISCONNECTED,
+                std::to_string(failed) + " instance(s) with a disconnected enhanced kNN graph "
+                "(status HDB_ERR_DISCONNECTED, labels -1); the others are complete");
   });
+}
+
+}  // namespace
+
+extern "C" {
+
+HDB_API hdb_status hdb_run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count,
+                                   const hdb_params *params, hdb_run_stats *stats) {
+  return run_batched(h, insts, count, params, stats, false);
+}
+
+HDB_API hdb_status hdb_run_knn_batched(hdb_ctx *h, hdb_instance *insts, int32_t count,
+                                       const hdb_params *params, hdb_run_stats *stats) {
+  return run_batched(h, insts, count, params, stats, true);
 }
 
 HDB_API hdb_status hdb_run_knn(hdb_ctx *h, const hdb_nnd_element *G, const float *X, int64_t n,

@@ -237,6 +237,15 @@ __global__ void k_edge_instance(const hdb_mst_edge *__restrict__ e, int64_t m, S
   }
 }
 
+// Chosen MST edges per instance (the key's low half is the CSR edge index).
+__global__ void k_count_inst_edges(const uint64_t *__restrict__ keys, int64_t m,
+                                   const int64_t *__restrict__ nindex, int64_t n, Segments seg,
+                                   int32_t *__restrict__ cnt) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[seg.of_point(row_of(nindex, n, (uint32_t)keys[t]))], 1);
+}
+
 __global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint32_t *__restrict__ idx,
                                 int64_t m, hdb_mst_edge *__restrict__ out) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
@@ -246,8 +255,8 @@ __global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint3
 
 }  // namespace
 
-void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
-                 int32_t *rounds_out, const Segments &seg) {
+int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
+                    int32_t *rounds_out, const Segments &seg, int32_t *inst_edges) {
   const int64_t n = g->nodes;
   HDB_REQUIRE(n >= 2, HDB_ERR_ARG, "MST: need at least 2 nodes");
   // one tree per instance: n - (number of instances) edges
@@ -307,36 +316,56 @@ void boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge
     std::swap(ep, ep2);
     std::swap(rp, rp2);
   }
-  const int64_t chosen = h[0];
   if (rounds == 0) {
     HDB_CUDA(cudaMemcpyAsync(h, counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ctx->sync();
   }
-  HDB_REQUIRE((rounds == 0 ? h[0] : chosen) == me, HDB_ERR_DISCONNECTED,
-              seg.count > 0
-                  ? "MST forest does not have n - instances edges: an instance's enhanced kNN "
-                    "graph is disconnected"
-                  : "MST does not have n-1 edges: the enhanced kNN graph is disconnected");
-  radix_sort_u64(ctx, keys, nullptr, me, 0, 64);
+  const int64_t chosen = h[0];
+  if (inst_edges && seg.count > 0) {
+    // a forest that may miss edges: report each instance's count instead
+    HDB_REQUIRE(chosen <= me, HDB_ERR_INTERNAL, "MST: more edges than points");
+    Buf<int32_t> cnt(ctx, seg.count);
+    HDB_CUDA(cudaMemsetAsync(cnt, 0, seg.count * sizeof(int32_t), st));
+    if (chosen > 0) {
+      k_count_inst_edges<<<grid_for(ctx, chosen, 256), 256, 0, st>>>(keys, chosen, g->nindex, n,
+                                                                      seg, cnt); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+    }
+    HDB_CUDA(cudaMemcpyAsync(inst_edges, cnt, seg.count * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             st));
+    ctx->sync();
+  } else {
+    HDB_REQUIRE(chosen == me, HDB_ERR_DISCONNECTED,
+                seg.count > 0
+                    ? "MST forest does not have n - instances edges: an instance's enhanced kNN "
+                      "graph is disconnected"
+                    : "MST does not have n-1 edges: the enhanced kNN graph is disconnected");
+  }
   if (in_mst) HDB_CUDA(cudaMemsetAsync(in_mst, 0, g->edges, st));
-  const int gm = grid_for(ctx, me, 256);
+  if (chosen == 0) {
+    if (rounds_out) *rounds_out = rounds;
+    return 0;
+  }
+  radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
+  const int gm = grid_for(ctx, chosen, 256);
   if (seg.count > 1) {
     // each instance's edges together, in (weight, edge index) order inside it
-    Buf<hdb_mst_edge> tmp(ctx, me);
-    k_gather_mst<<<gm, 256, 0, st>>>(keys, me, g->nindex, g->nlist, g->eweight, n, tmp, in_mst); ctx->launches++;
-    Buf<uint32_t> ikeys(ctx, me), idx(ctx, me);
-    k_edge_instance<<<gm, 256, 0, st>>>(tmp, me, seg, ikeys, idx); ctx->launches++;
+    Buf<hdb_mst_edge> tmp(ctx, chosen);
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, tmp, in_mst); ctx->launches++;
+    Buf<uint32_t> ikeys(ctx, chosen), idx(ctx, chosen);
+    k_edge_instance<<<gm, 256, 0, st>>>(tmp, chosen, seg, ikeys, idx); ctx->launches++;
     HDB_CHECK_LAUNCH();
     int bits = 1;
     while (bits < 31 && (int64_t(1) << bits) < seg.count) bits++;
-    radix_sort_u32(ctx, ikeys, idx, me, 0, bits);
-    k_permute_edges<<<gm, 256, 0, st>>>(tmp, idx, me, mst); ctx->launches++;
+    radix_sort_u32(ctx, ikeys, idx, chosen, 0, bits);
+    k_permute_edges<<<gm, 256, 0, st>>>(tmp, idx, chosen, mst); ctx->launches++;
   } else {
-    k_gather_mst<<<gm, 256, 0, st>>>(keys, me, g->nindex, g->nlist, g->eweight, n, mst, in_mst); ctx->launches++;
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, mst, in_mst); ctx->launches++;
   }
   HDB_CHECK_LAUNCH();
   ctx->sync();
   if (rounds_out) *rounds_out = rounds;
+  return chosen;
 }
 
 void sort_mst_edges(Context *ctx, hdb_mst_edge *edges, int64_t m) {

@@ -127,3 +127,75 @@ def generate_torch(w: Workload, device="cuda"):
     X[row:].uniform_(generator=g).mul_(hi - lo).add_(lo)
     perm = torch.randperm(w.n, generator=g, device=device)
     return X[perm].contiguous()
+
+
+# ---- many independent instances (hdb_run_batched) ---------------------------
+@dataclass(frozen=True)
+class BatchWorkload:
+    name: str
+    count: int         # instances
+    n_lo: int          # sizes log-uniform in [n_lo, n_hi]
+    n_hi: int
+    dims: tuple        # d drawn uniformly from these per instance
+    blobs_lo: int      # blobs per instance, uniform in [blobs_lo, blobs_hi]
+    blobs_hi: int
+    center_lo: float
+    center_hi: float
+    sigma: float
+    noise: float
+    k: int
+    mpts: int
+    sample_num: int
+    iterations: int
+    seed: int
+
+
+BATCH_WORKLOADS = {
+    # 4096 instances, n log-uniform in [1000, 200000], d in {8, 12, 32, 64},
+    # 3-50 isotropic blobs (centres in [-10, 10], sigma 1) + 5 % noise each,
+    # k = mpts = 16 (SAMPLE_NUM 8).  Expected total n = 4096 * 199000 / ln(200)
+    # ~ 154M points (4096 times the size's geometric mean, 14142, is 58M).
+    "batch_4096": BatchWorkload("batch_4096", 4096, 1000, 200_000, (8, 12, 32, 64), 3, 50,
+                                -10.0, 10.0, 1.0, 0.05, 16, 16, 8, 6, 4),
+}
+
+
+def batch_layout(bw: BatchWorkload, count: int | None = None):
+    """Per instance (n, d, blobs), seeded; the first `count` instances."""
+    rng = np.random.default_rng(bw.seed)
+    c = bw.count
+    n = np.exp(rng.uniform(np.log(bw.n_lo), np.log(bw.n_hi), size=c)).astype(np.int64)
+    d = rng.choice(np.asarray(bw.dims), size=c)
+    b = rng.integers(bw.blobs_lo, bw.blobs_hi + 1, size=c)
+    m = c if count is None else count
+    return [(int(n[i]), int(d[i]), int(b[i])) for i in range(m)]
+
+
+def batch_instance(bw: BatchWorkload, i: int, n: int, d: int, blobs: int) -> Workload:
+    """Instance i as a single workload (its own seed)."""
+    return Workload(f"{bw.name}_i{i}", n, d, blobs, bw.center_lo, bw.center_hi, bw.sigma,
+                    bw.sigma, False, 0.0, bw.noise, bw.k, bw.mpts, bw.sample_num, bw.iterations,
+                    bw.seed * 1_000_003 + i)
+
+
+def generate_batch_torch(bw: BatchWorkload, device="cuda", count: int | None = None):
+    """The instances on `device`: one [sum n, d] array per d with the instances
+    of that d back to back (in instance order), and per instance a view into
+    it, in instance order.  -> (views, layout)."""
+    import torch
+
+    layout = batch_layout(bw, count)
+    by_d = {}
+    for i, (n, d, b) in enumerate(layout):
+        by_d.setdefault(d, []).append(i)
+    views = [None] * len(layout)
+    for d, idx in by_d.items():
+        total = sum(layout[i][0] for i in idx)
+        buf = torch.empty((total, d), dtype=torch.float32, device=device)
+        row = 0
+        for i in idx:
+            n, _, b = layout[i]
+            buf[row:row + n] = generate_torch(batch_instance(bw, i, n, d, b), device=device)
+            views[i] = buf[row:row + n]
+            row += n
+    return views, layout

@@ -212,21 +212,37 @@ typedef struct {
   int32_t num_clusters;    /* out: clusters found in this instance */
   int32_t *labels;         /* out: [n], -1 = noise, clusters 0.. per instance */
   hdb_nnd_element *G;      /* optional out (NULL to skip): [n, k] final kNN rows,
-                              ids local to the instance, flags as hdb_nndescent */
+                              ids local to the instance, flags as hdb_nndescent
+                              (the input graph for hdb_run_knn_batched) */
+  int32_t status;          /* out: HDB_OK, or HDB_ERR_DISCONNECTED when the
+                              instance's enhanced kNN graph is disconnected (its
+                              labels are then all -1 and num_clusters 0) */
+  int32_t reserved;
 } hdb_instance;
 
 /* hdb_run_batched -- many independent HDBSCAN runs (the hdbscan_ flow of
- * HDBSCAN/_new.cu on each instance) in shared kernel launches: instances of
- * equal d are laid back to back and every stage runs once over all of them,
+ * HDBSCAN/_new.cu on each instance) in shared kernel launches: consecutive
+ * instances of equal d (up to 2^25 points at a time) are laid back to back
+ * and every stage runs once over all of them,
  * each instance's kNN lists, antihubs, clique, MST tree, condensed tree and
  * cluster selection staying inside the instance.  Per instance the result is
  * what hdb_run computes on that instance alone from the same kNN graph (the
  * NN-Descent initial graph is the same too: ids are drawn with
  * instance-local positions).  insts is a HOST array of `count` descriptors;
  * X, labels and G are device pointers, or host pointers with
- * params->host_io = 1.  stats (optional) sums the stages over all instances. */
+ * params->host_io = 1.  stats (optional) sums the stages over all instances.
+ * Where hdb_run fails on a disconnected graph, only that instance fails here:
+ * the call then returns HDB_ERR_DISCONNECTED with every other instance's
+ * outputs complete (see hdb_instance.status). */
 HDB_API hdb_status hdb_run_batched(hdb_ctx *ctx, hdb_instance *insts, int32_t count,
                                    const hdb_params *params, hdb_run_stats *stats);
+
+/* hdb_run_knn_batched -- hdb_run_knn (the HDBSCAN/_new.cu flow from finished
+ * .kgraph files) on many instances in shared launches: insts[i].G is the
+ * INPUT kNN graph [n, params->knn.k] of instance i, ids local to the
+ * instance (flags allowed); everything else as hdb_run_batched. */
+HDB_API hdb_status hdb_run_knn_batched(hdb_ctx *ctx, hdb_instance *insts, int32_t count,
+                                       const hdb_params *params, hdb_run_stats *stats);
 
 /* hdb_bf16_distance_tiles -- a diagnostic with no counterpart in the
  * reference: the distances the BF16 tensor-core local join of hdb_nndescent

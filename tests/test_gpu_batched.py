@@ -109,3 +109,81 @@ def test_batched_argument_errors(ctx):
         ctx.hdbscan_batched(Xs, k=16, mpts=17, sample_num=8)
     labels, ncl, _ = ctx.hdbscan_batched(Xs[:2], k=16, mpts=16, sample_num=8)
     assert len(labels) == 2  # the context still works
+
+
+def _two_group_graph():
+    """kNN lists that stay inside two groups of 50 points; every antihub falls
+    in the first group (equal degrees, ties by index), so the second group is
+    unreachable: the reference stops on it with "MST montada incorretamente"
+    (mst.cu:317-323)."""
+    n, k = 100, 4
+    ids = np.zeros((n, k), np.int32)
+    for g0 in (0, 50):
+        for i in range(50):
+            ids[g0 + i] = [g0 + (i + s) % 50 for s in (1, 2, 3, 4)]
+    X = np.random.default_rng(0).normal(size=(n, 2)).astype(np.float32)
+    G = np.zeros((n, k, 2), np.int32)
+    G[..., 0] = np.ones((n, k), np.float32).view(np.int32)
+    G[..., 1] = ids
+    return G, X
+
+
+def test_batched_disconnected_instance_fails_alone(ctx, oracle):
+    """An instance with a disconnected enhanced kNN graph gets status
+    HDB_ERR_DISCONNECTED and labels -1; the other instances of the batch
+    complete with the oracle's labels."""
+    Xs, Gs = [], []
+    for i, n in enumerate((300, 0, 500, 0, 250)):
+        if n == 0:
+            G, X = _two_group_graph()
+        else:
+            X = blobs(n, 2, seed=40 + i, spread=2.5)
+            G = ctx.NNDescent(X, k=4, sample_num=2).cpu().numpy()
+        Xs.append(X)
+        Gs.append(G)
+    kw = dict(k=4, mpts=4)
+    with pytest.raises(g.HdbError, match="DISCONNECTED"):
+        ctx.hdbscan_batched_from_knn(Gs, Xs, **kw)
+    labels, ncl, st = ctx.hdbscan_batched_from_knn(Gs, Xs, strict=False, **kw)
+    D = g._lib.HDB_ERR_DISCONNECTED
+    assert st["instance_status"] == [0, D, 0, D, 0]
+    for i, (G, X) in enumerate(zip(Gs, Xs)):
+        ids = np.where(G[..., 1] < 0, -G[..., 1] - 1, G[..., 1]).astype(np.int32)
+        if st["instance_status"][i]:
+            assert (labels[i].numpy() == -1).all() and ncl[i] == 0
+            with pytest.raises(RuntimeError):
+                oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 4)
+            continue
+        _, ref, rnc = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 4)
+        np.testing.assert_array_equal(labels[i].numpy(), ref)
+        assert ncl[i] == rnc
+
+
+def test_batched_from_knn_reproduces_reference_golden_labels(ctx):
+    """The reference's own fixtures (tests/golden) as one batch through
+    hdb_run_knn_batched: every instance's labels equal the reference's."""
+    import glob
+    import json
+    import os
+    files = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+    if not files:
+        pytest.skip("no golden fixtures")
+    fx = [(dict(np.load(f)), json.load(open(f[:-4] + ".json"))) for f in files]
+    batches = 0
+    for mpts in sorted({v for _, m in fx for v in m["mpts"]}):
+        Gs, Xs, refs = [], [], []
+        for d, m in fx:
+            if mpts not in m["mpts"]:
+                continue
+            G = np.zeros(d["ids"].shape + (2,), np.int32)
+            G[..., 0] = d["dist"].view(np.int32)
+            G[..., 1] = d["ids"]
+            Gs.append(G)
+            Xs.append(d["X"])
+            refs.append(d[f"labels_{mpts}"])
+        labels, _, _ = ctx.hdbscan_batched_from_knn(Gs, Xs, k=32, mpts=mpts,
+                                                     distance=g.HDB_DIST_SQUARED)
+        for lab, ref in zip(labels, refs):
+            np.testing.assert_array_equal(lab.numpy(), ref)
+        batches += len(Gs) > 1
+    assert batches >= 1  # at least one mpts shared by several fixtures
