@@ -512,12 +512,24 @@ def run_ours_batch(args, bw):
     m = min(args.loop_instances, len(views))
     sub = [v for v, s_ in zip(views[:m], stats[-1]["instance_status"][:m]) if s_ == 0]
     n_sub = sum(len(v) for v in sub)
-    lms, _ = timed(lambda: [ctx.hdbscan(v, **kw) for v in sub], 1, 1)
+    loop_failed = []
+
+    def loop_once():
+        loop_failed.clear()
+        for v in sub:
+            try:
+                ctx.hdbscan(v, **kw)
+            except g.HdbError as e:  # its own graph may fall apart where the batch's did not
+                if e.status != g._lib.HDB_ERR_DISCONNECTED:
+                    raise
+                loop_failed.append(1)
+
+    lms, _ = timed(loop_once, 1, 1)
     bms, _ = timed(lambda: ctx.hdbscan_batched(sub, **kw_b), 1, 1)
     loop = {"instances": len(sub), "points": n_sub,
             "loop_points_per_s": round(n_sub / (lms / 1e3), 1), "loop_ms": round(lms, 3),
             "batched_points_per_s": round(n_sub / (bms / 1e3), 1), "batched_ms": round(bms, 3),
-            "speedup": round(lms / bms, 3)}
+            "speedup": round(lms / bms, 3), "loop_disconnected": len(loop_failed)}
 
     e2e = None
     if not args.no_e2e:
