@@ -679,6 +679,75 @@ void orc_sort_edges(orc_mst_edge *e, int64_t m) {
   free(tmp);
 }
 
+/* The mst_gpu = 1 MST of build_CoreSG (core-sg.cu:533-540).
+ *  - GetMinDistanceFromKNNG (tools/filetool.hpp:312-347): the smallest
+ *    positive first-neighbour distance of the .kgraph rows (start 999.0; row
+ *    0's distance replaces it outright when positive); first_dist[i] is row
+ *    i's first distance.
+ *  - buildGPUgraph (core-sg.cu:8-44): multiplier m = ceil(-log10|min|) + 2,
+ *    integer weights (int)(10^m * w).  A product outside the int range takes
+ *    the value x86's truncating conversion gives it, INT_MIN.
+ *  - gpuMST (mst.cu:210-288): Boruvka over the entries j with nlist[j] > row,
+ *    keyed by ((uint32)q << 32 | j) -- unique keys, so the tree is Kruskal's
+ *    under that order.
+ *  - buildMST_gpu (mst.cu:338-380): chosen edges in CSR order with weight
+ *    (float)(q / 10^m), then sort_edges (stable by weight).
+ * Returns ORC_ERR_DISCONNECTED when the tree has fewer than nodes-1 edges. */
+typedef struct { uint64_t key; int32_t a, b; } orc_qedge;
+static int cmp_qedge(const void *x, const void *y) {
+  uint64_t a = ((const orc_qedge *)x)->key, b = ((const orc_qedge *)y)->key;
+  return a < b ? -1 : a > b;
+}
+
+int orc_mst_quantised(const int64_t *nindex, const int32_t *nlist, const float *eweight,
+                      int32_t nodes, int64_t edges, const float *first_dist, orc_mst_edge *out,
+                      int32_t *mult_out) {
+  double min_value = 999.0;
+  for (int32_t i = 0; i < nodes; i++) {
+    double d = (double)first_dist[i];
+    if (i == 0 && d > 0.0) min_value = d;
+    else if (min_value > d && d > 0.0) min_value = d;
+  }
+  int32_t m = (int32_t)(ceil(-log10(fabs(min_value))) + 2);
+  double p10 = pow(10.0, m);
+  int32_t *q = (int32_t *)malloc(sizeof(int32_t) * (edges > 0 ? edges : 1));
+  for (int64_t j = 0; j < edges; j++) {
+    double v = p10 * (double)eweight[j] / 1;
+    q[j] = (v < 2147483648.0 && v > -2147483649.0) ? (int32_t)v : INT32_MIN;
+  }
+  int64_t cnt = 0;
+  for (int32_t i = 0; i < nodes; i++)
+    for (int64_t j = nindex[i]; j < nindex[i + 1]; j++) cnt += (nlist[j] > i);
+  orc_qedge *list = (orc_qedge *)malloc(sizeof(orc_qedge) * (cnt > 0 ? cnt : 1));
+  cnt = 0;
+  for (int32_t i = 0; i < nodes; i++)
+    for (int64_t j = nindex[i]; j < nindex[i + 1]; j++)
+      if (nlist[j] > i)
+        list[cnt++] = (orc_qedge){((uint64_t)(uint32_t)q[j] << 32) | (uint64_t)j, i, nlist[j]};
+  qsort(list, cnt, sizeof(orc_qedge), cmp_qedge);
+  int32_t *parent = (int32_t *)malloc(sizeof(int32_t) * nodes);
+  for (int32_t i = 0; i < nodes; i++) parent[i] = i;
+  uint8_t *in = (uint8_t *)calloc(edges > 0 ? edges : 1, 1);
+  int32_t left = nodes - 1;
+  for (int64_t p = 0; p < cnt && left > 0; p++) {
+    int32_t ar = serial_find(list[p].a, parent), br = serial_find(list[p].b, parent);
+    if (ar != br) {
+      in[(uint32_t)list[p].key] = 1;
+      if (ar > br) parent[br] = ar; else parent[ar] = br;
+      left--;
+    }
+  }
+  int64_t soma = 0;
+  for (int32_t i = 0; i < nodes && left == 0; i++)
+    for (int64_t j = nindex[i]; j < nindex[i + 1]; j++)
+      if (in[j]) out[soma++] = (orc_mst_edge){i, nlist[j], (float)((1.0 * q[j]) / p10)};
+  free(list); free(parent); free(in); free(q);
+  if (left != 0) return ORC_ERR_DISCONNECTED;
+  orc_sort_edges(out, nodes - 1);
+  if (mult_out) *mult_out = m;
+  return ORC_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Trees                                                                     */
 /* ------------------------------------------------------------------------ */

@@ -67,6 +67,12 @@ int orc_kruskal(const int64_t *nindex, const int32_t *nlist, const float *eweigh
                 int64_t edges, uint8_t *in_mst);
 int orc_build_mst(const int64_t *nindex, const int32_t *nlist, const float *eweight,
                   int32_t nodes, int64_t edges, const uint8_t *in_mst, orc_mst_edge *out);
+/* mst_gpu = 1 (core-sg.cu:8-44, mst.cu:210-288, 338-380): int-quantised MST,
+ * dequantised weights, stably sorted.  first_dist[i]: row i's first kNN
+ * distance as the .kgraph holds it. */
+int orc_mst_quantised(const int64_t *nindex, const int32_t *nlist, const float *eweight,
+                      int32_t nodes, int64_t edges, const float *first_dist, orc_mst_edge *out,
+                      int32_t *mult_out);
 void orc_sort_edges(orc_mst_edge *edges, int64_t m);
 
 /* ---- trees (HDBSCAN/trees/tree.cu) ---- */

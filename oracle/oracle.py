@@ -61,6 +61,7 @@ def lib():
             "orc_core_sg": (_I64, [_P, _P, _P, _I64, _I32, _I32, _P, _P, _P, _P]),
             "orc_kruskal": (C.c_int, [_P, _P, _P, _I32, _I64, _P]),
             "orc_build_mst": (C.c_int, [_P, _P, _P, _I32, _I64, _P, _P]),
+            "orc_mst_quantised": (C.c_int, [_P, _P, _P, _I32, _I64, _P, _P, _P]),
             "orc_sort_edges": (None, [_P, _I64]),
             "orc_linkage_tree": (None, [_P, _I64, _P]),
             "orc_condensed_tree": (_I64, [_P, _I64, _I32, _P]),
@@ -237,6 +238,22 @@ def build_mst(nindex, nlist, eweight, inmst):
     if rc:
         raise RuntimeError("MST has the wrong number of edges")
     return out
+
+
+def mst_quantised(nindex, nlist, eweight, first_dist):
+    """The reference's mst_gpu = 1 MST: (sorted MST_EDGE[n-1], multiplier)."""
+    nindex = _c(nindex, np.int64)
+    nlist = _c(nlist, np.int32)
+    eweight = _c(eweight, np.float32)
+    first_dist = _c(first_dist, np.float32)
+    n = len(nindex) - 1
+    out = np.zeros(n - 1, MST_EDGE)
+    mult = C.c_int32(0)
+    rc = lib().orc_mst_quantised(_p(nindex), _p(nlist), _p(eweight), n, len(nlist), _p(first_dist),
+                                 _p(out), C.byref(mult))
+    if rc:
+        raise RuntimeError("graph is disconnected")
+    return out, mult.value
 
 
 def sort_edges(edges):

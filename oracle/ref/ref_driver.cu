@@ -13,7 +13,9 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <cstring>
+#include <string>
 
 #include "HDBSCAN/calculates/calculates.cuh"
 #include "HDBSCAN/counts/count.cuh"
@@ -25,6 +27,7 @@
 #include "HDBSCAN/trees/tree.cuh"
 #include "HDBSCAN/graphs/graph.cuh"
 #include "gpuknn/nndescent.cuh"
+#include "tools/filetool.hpp"
 
 // ---- stand-ins for the reference's fixed-path file helpers (build_kNNG.cu) ----
 static const float *g_vectors = nullptr;
@@ -41,6 +44,19 @@ float *jesus(int *antihubs, int num_antihubs, int *paz) {
 }
 // write_bool_dict (build_kNNG.cu:79-87) only persists the mutual flags.
 void write_bool_dict(int *, long, long) {}
+
+// The other fixed-path helpers of build_kNNG.cu that core-sg.cu links against
+// serve only build_CoreSG's own file flow, which this driver never enters.
+static void not_in_driver(const char *what) {
+  fprintf(stderr, "%s is not available in the reference driver\n", what);
+  abort();
+}
+float *ReadObjects(long *) { not_in_driver("ReadObjects"); return nullptr; }
+NNDElement *ReadkNNGgraph() { not_in_driver("ReadkNNGgraph"); return nullptr; }
+int *read_bool_dict() { not_in_driver("read_bool_dict"); return nullptr; }
+float *read_euclidean_distance_vecs() { not_in_driver("read_euclidean_distance_vecs"); return nullptr; }
+void write_euclidean_distance_vecs(float *, long) { not_in_driver("write_euclidean_distance_vecs"); }
+
 
 static int check(const char *what) {
   cudaError_t e = cudaDeviceSynchronize();
@@ -215,6 +231,48 @@ int ref_nndescent(const float *X, long n, int d, int iterations, NNDElement *G_o
   memcpy(G_out, G, n * NEIGHB_NUM_PER_LIST * sizeof(NNDElement));
   delete[] G;
   cudaFree(Xd);
+  return 0;
+}
+
+// The mst_gpu = 1 branch of build_CoreSG (core-sg.cu:533-540): buildGPUgraph,
+// gpuMST(g, INT_MAX), buildMST_gpu (dequantised weights, sort_edges).
+// buildGPUgraph (core-sg.cu:8-44) itself is not called: it hands
+// FileTool::GetMinDistanceFromKNNG an uninitialised `long` for the row width,
+// of which the reader fills only 4 bytes (filetool.hpp:321), so it works only
+// when that stack slot happens to be zero.  Here the same reader runs with the
+// long zeroed, and buildGPUgraph's scaling (multiplier ceil(-log10|min|) + 2,
+// weights (int)(10^m * w)) is repeated line for line; gpuMST and buildMST_gpu
+// are the reference's.
+int ref_mst_gpu(const long *nindex, const int *nlist, const float *ew, long n,
+                const char *kgraph_path, MSTedge *mst_out, int *mult_out) {
+  NNDElement *row = nullptr;
+  long knng_num = 0, knng_dim = 0;
+  double min_dist = FileTool::GetMinDistanceFromKNNG(std::string(kgraph_path), &row, &knng_num,
+                                                     &knng_dim);
+  delete[] row;
+  int multiplica = ceil(-log10(fabs(min_dist))) + 2;
+  GPUECLgraph gg;
+  gg.nodes = (int)n;
+  gg.edges = (int)nindex[n];
+  gg.nindex = new int[n + 1];
+  gg.nlist = new int[gg.edges];
+  gg.eweight = new int[gg.edges];
+  for (long i = 0; i <= n; i++) gg.nindex[i] = (int)nindex[i];
+  for (long i = 0; i < gg.edges; i++) {
+    gg.nlist[i] = nlist[i];
+    gg.eweight[i] = (int)(pow(10.0, multiplica) * (double)ew[i] / 1);
+  }
+  bool *edges = gpuMST(gg, INT_MAX);
+  MSTedge *mst = buildMST_gpu(gg, edges, multiplica);
+  if (check("buildMST_gpu")) return 1;
+  memcpy(mst_out, mst, (n - 1) * sizeof(MSTedge));
+  *mult_out = multiplica;
+  delete[] gg.nindex;
+  delete[] gg.nlist;
+  delete[] gg.eweight;
+  gg.nindex = nullptr;
+  gg.nlist = nullptr;
+  gg.eweight = nullptr;
   return 0;
 }
 

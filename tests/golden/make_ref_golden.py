@@ -7,6 +7,11 @@ Needs a GPU (the reference's tree stages allocate managed memory and launch
 fill kernels).  Usage on a GPU box, from the repository root:
 
     python tests/golden/make_ref_golden.py OUTDIR
+    python tests/golden/make_ref_golden.py --add-mst-gpu OUTDIR
+
+The second form adds the reference's mst_gpu = 1 MST (int-quantised weights,
+gpuMST, buildMST_gpu) of every committed fixture's enhanced graph as
+`mstgpu` / `mstgpu_mult`, leaving the fixture's other arrays as they are.
 
 The kNN graphs fed to the reference come from the oracle's NN-Descent (with
 fix_distances applied), so every later stage sees one shared input.  The
@@ -52,8 +57,36 @@ def load_ref():
     L.ref_mst_trees.argtypes = [P, P, P, C.c_long, C.c_int, P, P, P, P, P, P, P]
     L.ref_nndescent.restype = C.c_int
     L.ref_nndescent.argtypes = [P, C.c_long, C.c_int, C.c_int, P]
+    L.ref_mst_gpu.restype = C.c_int
+    L.ref_mst_gpu.argtypes = [P, P, P, C.c_long, C.c_char_p, P, P]
     L.ref_free.argtypes = [P]
     return L
+
+
+def write_kgraph(path, ids, dist):
+    """The .kgraph layout (tools/filetool.hpp WriteBinaryVecs of NNDElement):
+    per row int32 k, then k (float distance, int32 label) pairs."""
+    n, k = ids.shape
+    rows = np.empty((n, 1 + 2 * k), np.int32)
+    rows[:, 0] = k
+    rows[:, 1::2] = np.ascontiguousarray(dist, np.float32).view(np.int32)
+    rows[:, 2::2] = ids
+    rows.tofile(path)
+
+
+def ref_mst_gpu(L, nindex, nlist, ew, ids, dist, outdir, name):
+    """The reference's mst_gpu = 1 MST; the multiplier comes from a .kgraph
+    holding the graph's distances, as build_CoreSG reads it."""
+    n = len(nindex) - 1
+    kg = os.path.join(outdir, f"_{name}.kgraph")
+    write_kgraph(kg, ids, dist)
+    mst = np.zeros(n - 1, MST_EDGE)
+    mult = C.c_int(0)
+    rc = L.ref_mst_gpu(p(np.ascontiguousarray(nindex, np.int64)), p(nlist), p(ew), n,
+                       kg.encode(), p(mst), C.byref(mult))
+    os.remove(kg)
+    assert rc == 0, "reference gpuMST failed"
+    return mst, mult.value
 
 
 def p(a):
@@ -83,6 +116,8 @@ def run_case(L, name, n, d, nblobs, noise, seed, mpts_list, outdir):
     ah = take(L, pa, nah.value, C.c_int)
     out = dict(X=X, ids=ids, dist=dist, nindex=nindex, nlist=nlist, eweight=ew, antihubs=ah)
     meta = {"name": name, "n": n, "d": d, "k": 32, "edges": int(E), "mpts": mpts_list}
+    out["mstgpu"], mult = ref_mst_gpu(L, nindex, nlist, ew, ids, dist, outdir, name)
+    out["mstgpu_mult"] = np.array([mult], np.int32)
     for mpts in mpts_list:
         mst = np.zeros(n - 1, MST_EDGE)
         hier = np.zeros(n - 1, LINK)
@@ -114,11 +149,27 @@ def run_case(L, name, n, d, nblobs, noise, seed, mpts_list, outdir):
     print(name, meta, flush=True)
 
 
+def add_mst_gpu(L, outdir):
+    import glob
+    for f in sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "ref_*.npz"))):
+        d = dict(np.load(f))
+        name = os.path.basename(f)[4:-4]
+        d["mstgpu"], mult = ref_mst_gpu(L, d["nindex"], d["nlist"], d["eweight"], d["ids"],
+                                        d["dist"], outdir, name)
+        d["mstgpu_mult"] = np.array([mult], np.int32)
+        np.savez_compressed(os.path.join(outdir, os.path.basename(f)), **d)
+        print(name, "mst_gpu multiplier", mult, flush=True)
+
+
 def main():
-    outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    outdir = args[0] if args else os.path.join(ROOT, "tests", "golden")
     os.makedirs(outdir, exist_ok=True)
     O.build()
     L = load_ref()
+    if "--add-mst-gpu" in sys.argv:
+        add_mst_gpu(L, outdir)
+        return
     for case in CASES:
         run_case(L, *case, outdir)
 
