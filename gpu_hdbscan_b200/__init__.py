@@ -182,6 +182,21 @@ class Context:
                                   C.byref(rounds)))
         return mst, inm, rounds.value
 
+    def buildMST_quantised(self, graph: EnhancedGraph, dist, with_in_mst=False):
+        """The reference's mst_gpu = 1 MST (hdb_mst_quantised): dist [n, k] the
+        kNN distances the graph was built from (its first column sets the
+        scale).  -> (mst [n-1, 3] int32 view of MSTedge, in_mst or None,
+        multiplier m, Boruvka rounds)."""
+        torch = self._torch
+        n = graph.nodes
+        dist = self._dev(dist, torch.float32)
+        mst = torch.empty((n - 1, 3), dtype=torch.int32, device=self.device)
+        inm = torch.empty(graph.edges, dtype=torch.uint8, device=self.device) if with_in_mst else None
+        rounds, mult = C.c_int32(0), C.c_int32(0)
+        _lib.check(self.L.hdb_mst_quantised(self.h, C.byref(graph.raw), _ptr(dist), dist.shape[1],
+                                            _ptr(inm), _ptr(mst), C.byref(mult), C.byref(rounds)))
+        return mst, inm, mult.value, rounds.value
+
     def sort_edges(self, mst):
         """In place: stable ascending sort of MSTedge rows by weight."""
         _lib.check(self.L.hdb_sort_edges(self.h, _ptr(mst), mst.shape[0]))
@@ -215,7 +230,7 @@ class Context:
         return labels, ncl.value, cond, stab
 
     def hdbscan(self, X, k=32, mpts=32, sample_num=16, iterations=6, precision=HDB_PREC_FP32,
-                distance=HDB_DIST_SQRT, stability=HDB_STAB_FP32, labels_out=None):
+                distance=HDB_DIST_SQRT, stability=HDB_STAB_FP32, labels_out=None, mst_gpu=0):
         """The whole path (hdb_run).  X on the host (numpy / CPU tensor) runs with
         host_io=1: the H2D copy of X and the D2H copy of the labels are inside
         the call.  X on the device returns device labels."""
@@ -230,14 +245,14 @@ class Context:
                 X.shape[0], dtype=torch.int32, device=self.device)
         n, d = X.shape
         p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
-                        stability, 1 if host else 0)
+                        stability, 1 if host else 0, mst_gpu)
         st = _lib.RunStats()
         _lib.check(self.L.hdb_run(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels), C.byref(st)))
         return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
 
     def hdbscan_batched(self, Xs, k=32, mpts=32, sample_num=16, iterations=6,
                         precision=HDB_PREC_FP32, distance=HDB_DIST_SQRT,
-                        stability=HDB_STAB_FP32, want_graphs=False, strict=True):
+                        stability=HDB_STAB_FP32, want_graphs=False, strict=True, mst_gpu=0):
         """Independent runs of the whole path on every array of Xs in shared
         launches (hdb_run_batched).  Host arrays run with host_io=1 (copies
         inside the call); CUDA tensors give device results.
@@ -247,16 +262,16 @@ class Context:
         raises HdbError when strict, else keeps labels -1 and status
         HDB_ERR_DISCONNECTED while the others complete."""
         p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
-                        stability, 0)
+                        stability, 0, mst_gpu)
         return self._batched(self.L.hdb_run_batched, Xs, None, k, p, want_graphs, strict)
 
     def hdbscan_batched_from_knn(self, Gs, Xs, k=32, mpts=32, distance=HDB_DIST_SQRT,
-                                 stability=HDB_STAB_FP32, strict=True):
+                                 stability=HDB_STAB_FP32, strict=True, mst_gpu=0):
         """The stages after the kNN graph on many instances in shared launches
         (hdb_run_knn_batched): Gs[i] [n_i, k, 2] NNDElement rows with
         instance-local ids, Xs[i] [n_i, d_i].  -> (labels, cluster counts, stats)."""
         p = _lib.Params(_lib.KnnParams(k, max(1, k // 2), 0, HDB_PREC_FP32), mpts, distance,
-                        stability, 0)
+                        stability, 0, mst_gpu)
         return self._batched(self.L.hdb_run_knn_batched, Xs, Gs, k, p, False, strict)
 
     def _batched(self, fn, Xs, Gs, k, p, want_graphs, strict):
@@ -291,7 +306,7 @@ class Context:
         return labels, ncl, stats
 
     def hdbscan_from_knn(self, G, X, k=32, mpts=32, distance=HDB_DIST_SQRT,
-                         stability=HDB_STAB_FP32):
+                         stability=HDB_STAB_FP32, mst_gpu=0):
         """The stages after the kNN graph (hdb_run_knn): G [n, k, 2] NNDElement rows,
         X [n, d].  Device tensors -> device labels; host arrays -> host labels
         (host_io: copies inside the call)."""
@@ -307,7 +322,7 @@ class Context:
             labels = torch.empty(X.shape[0], dtype=torch.int32, device=self.device)
         n, d = X.shape
         p = _lib.Params(_lib.KnnParams(k, max(1, k // 2), 0, HDB_PREC_FP32), mpts, distance,
-                        stability, 1 if host else 0)
+                        stability, 1 if host else 0, mst_gpu)
         st = _lib.RunStats()
         _lib.check(self.L.hdb_run_knn(self.h, _ptr(G), _ptr(X), n, d, C.byref(p), _ptr(labels),
                                       C.byref(st)))

@@ -25,7 +25,7 @@ EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_se
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
-           "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched")
+           "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised")
 
 
 class HdbError(RuntimeError):
@@ -41,7 +41,7 @@ class KnnParams(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [("knn", KnnParams), ("mpts", C.c_int32), ("distance", C.c_int32),
-                ("stability", C.c_int32), ("host_io", C.c_int32)]
+                ("stability", C.c_int32), ("host_io", C.c_int32), ("mst_gpu", C.c_int32)]
 
 
 class Graph(C.Structure):
@@ -57,7 +57,8 @@ class RunStats(C.Structure):
                 ("ms_mst", C.c_float), ("ms_tree", C.c_float), ("ms_total", C.c_float),
                 ("join_ms", C.c_float), ("join_launches", C.c_int32),
                 ("join_rows_gathered", C.c_int64), ("join_candidates", C.c_int64),
-                ("gpu_launches", C.c_int64)]
+                ("gpu_launches", C.c_int64), ("mst_multiplier", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class Instance(C.Structure):
@@ -90,6 +91,8 @@ def load(path: str = LIB_PATH):
         "hdb_fix_distances": (C.c_int, [_P, _P, _I64, _I32, _P, _I32, _P]),
         "hdb_enhanced_knng": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, C.POINTER(Graph)]),
         "hdb_mst": (C.c_int, [_P, C.POINTER(Graph), _P, _P, C.POINTER(_I32)]),
+        "hdb_mst_quantised": (C.c_int, [_P, C.POINTER(Graph), _P, _I32, _P, _P, C.POINTER(_I32),
+                                        C.POINTER(_I32)]),
         "hdb_sort_edges": (C.c_int, [_P, _P, _I64]),
         "hdb_linkage_tree": (C.c_int, [_P, _P, _I64, _P]),
         "hdb_condense_select": (C.c_int, [_P, _P, _I64, _I32, _I32, _P, C.POINTER(_I32), _P,

@@ -5,9 +5,11 @@
 //
 // Exactly four positional arguments, otherwise it prints "NUM_VALUES NOT
 // SETTED" and exits 1; mpts must not exceed k (assert(k >= mpts)).  `shards`
-// and `mst_gpu` are accepted for compatibility: the path runs on one GPU and
-// its MST is always the GPU Boruvka (bit-identical to the reference's
-// cpuMST).  The stages run in the reference's order, one library call each:
+// is accepted for compatibility (the path runs on one GPU); mst_gpu selects
+// the MST as in the reference: 0 = the float MST of cpuMST, 1 = the
+// int-quantised GPU MST of buildGPUgraph + gpuMST + buildMST_gpu (both run
+// as GPU Boruvka here).  The stages run in the reference's order, one library
+// call each:
 // kNN graph (built, or read from a .kgraph), fix_distances, enhanced kNN
 // graph, MST, linkage tree, condensed tree / stability / clusters.  Instead
 // of the reference's hard-coded /nndescent/... paths the files are options:
@@ -237,8 +239,14 @@ int main(int argc, char **argv) {
     return fail("hdb_enhanced_knng");
   const double t_graph = secs_since(t);
   t = std::chrono::steady_clock::now();
-  int32_t rounds = 0;
-  if (hdb_mst(ctx, &g, nullptr, mst, &rounds) != HDB_OK) return fail("hdb_mst");
+  int32_t rounds = 0, mult = 0;
+  if (mst_gpu) {
+    if (hdb_mst_quantised(ctx, &g, dist, k, nullptr, mst, &mult, &rounds) != HDB_OK)
+      return fail("hdb_mst_quantised");
+    printf("MST WEIGHT MULTIPLIER: 10^%d\n", mult);
+  } else if (hdb_mst(ctx, &g, nullptr, mst, &rounds) != HDB_OK) {
+    return fail("hdb_mst");
+  }
   const double t_mst = secs_since(t);
   t = std::chrono::steady_clock::now();
   int32_t ncl = 0;

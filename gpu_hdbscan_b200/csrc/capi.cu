@@ -147,6 +147,23 @@ HDB_API hdb_status hdb_mst(hdb_ctx *h, const hdb_graph *graph, uint8_t *in_mst, 
   });
 }
 
+HDB_API hdb_status hdb_mst_quantised(hdb_ctx *h, const hdb_graph *graph, const float *dist,
+                                     int32_t k, uint8_t *in_mst, hdb_mst_edge *mst,
+                                     int32_t *multiplier, int32_t *rounds) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(graph, "graph");
+    require_ptr(dist, "dist");
+    require_ptr(mst, "mst");
+    HDB_REQUIRE(k >= 1 && graph->nodes >= 2, HDB_ERR_ARG, "hdb_mst_quantised: bad k or graph");
+    Buf<double> p10(ctx, 1);
+    int32_t mult = 0;
+    quant_scales(ctx, dist, k, graph->nodes, Segments{}, p10, &mult);
+    boruvka_mst(ctx, graph, in_mst, mst, rounds, Segments{}, nullptr, p10);
+    if (multiplier) *multiplier = mult;
+  });
+}
+
 HDB_API hdb_status hdb_sort_edges(hdb_ctx *h, hdb_mst_edge *edges, int64_t m) {
   return guard([&] {
     Context *ctx = C(h);
@@ -191,6 +208,7 @@ namespace {
 
 void check_run_params(const hdb_params &p) {
   check_knn_params(&p.knn);
+  HDB_REQUIRE(p.mst_gpu == 0 || p.mst_gpu == 1, HDB_ERR_ARG, "mst_gpu must be 0 or 1");
   const int32_t k = p.knn.k;
   HDB_REQUIRE(p.mpts >= 2 && p.mpts <= k, HDB_ERR_ARG, "mpts must satisfy 2 <= mpts <= k");
   HDB_REQUIRE(p.distance == HDB_DIST_SQRT || p.distance == HDB_DIST_SQUARED, HDB_ERR_ARG,
@@ -201,15 +219,22 @@ void check_run_params(const hdb_params &p) {
 
 // The stages after the kNN graph (HDBSCAN/_new.cu:243-347) on device arrays:
 // ids [n, k] decoded, core [n], X [n, d] -> labels [n].  Records ev[3..5].
+// first (p.mst_gpu only): every row's first-neighbour distance.
 void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X, int64_t n,
-                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st) {
+                   int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st,
+                   const float *first) {
   cudaStream_t s = ctx->stream;
   hdb_graph g;
   build_enhanced_knng(ctx, ids, core, X, n, d, k, &g, nullptr);
   HDB_CUDA(cudaEventRecord(ctx->ev[3], s));
   int32_t rounds = 0;
   Buf<hdb_mst_edge> mst(ctx, n - 1);
-  boruvka_mst(ctx, &g, nullptr, mst, &rounds);
+  Buf<double> p10;
+  if (p.mst_gpu) {
+    p10 = Buf<double>(ctx, 1);
+    quant_scales(ctx, first, 1, n, Segments{}, p10, &st->mst_multiplier);
+  }
+  boruvka_mst(ctx, &g, nullptr, mst, &rounds, Segments{}, nullptr, p10.get());
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   int32_t ncl = 0;
   {
@@ -315,7 +340,8 @@ __global__ void k_expand_labels(const int32_t *__restrict__ kept_labels, Segment
 // status HDB_ERR_DISCONNECTED and labels -1).  Records ev[3..5].
 void batch_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X,
                      int64_t n, int32_t d, int32_t k, const hdb_params &p, int32_t *labels,
-                     hdb_run_stats *st, const Segments &seg, int32_t *ncl, int32_t *status) {
+                     hdb_run_stats *st, const Segments &seg, int32_t *ncl, int32_t *status,
+                     const float *first) {
   cudaStream_t s = ctx->stream;
   const int32_t T = seg.count;
   hdb_graph g;
@@ -324,7 +350,12 @@ void batch_after_knn(Context *ctx, const int32_t *ids, const float *core, const 
   int32_t rounds = 0;
   Buf<hdb_mst_edge> mst(ctx, n - T);
   std::vector<int32_t> iedges((size_t)T);
-  const int64_t chosen = boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg, iedges.data());
+  Buf<double> p10;
+  if (p.mst_gpu) {  // every instance's own scale, as its own run would take it
+    p10 = Buf<double>(ctx, T);
+    quant_scales(ctx, first, 1, n, seg, p10, nullptr);
+  }
+  const int64_t chosen = boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg, iedges.data(), p10.get());
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   std::vector<int32_t> keep((size_t)T);
   std::vector<int64_t> pshift((size_t)T), eshift((size_t)T), off2(1, 0);
@@ -450,7 +481,7 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
   int64_t dropped = 0;
   JoinStats js;
   Buf<int32_t> ids(ctx, (size_t)n * k), labels(ctx, n);
-  Buf<float> core(ctx, n);
+  Buf<float> core(ctx, n), first;
   Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
   if (from_knn) {
     if (p.host_io) {
@@ -476,10 +507,15 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
     if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
     knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
     core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, core);
+    if (p.mst_gpu) {
+      first = Buf<float>(ctx, n);
+      core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, first, 0);
+    }
   }
   std::vector<int32_t> ncl((size_t)T, 0), status((size_t)T, HDB_OK);
   hdb_run_stats rs = {};
-  batch_after_knn(ctx, ids, core, X, n, d, k, p, labels, &rs, seg, ncl.data(), status.data());
+  batch_after_knn(ctx, ids, core, X, n, d, k, p, labels, &rs, seg, ncl.data(), status.data(),
+                  first.get());
 
   // outputs
   if (p.host_io) {
@@ -561,7 +597,7 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
     HDB_CUDA(cudaEventRecord(ev[1], st));
     int64_t dropped = 0;
     Buf<int32_t> ids(ctx, (size_t)n * k);
-    Buf<float> core(ctx, n);
+    Buf<float> core(ctx, n), first;
     {
       Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
       nndescent(ctx, Xuse, n, d, p.knn, G, &dropped, &js);
@@ -570,8 +606,12 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
       core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
+      if (p.mst_gpu) {
+        first = Buf<float>(ctx, n);
+        core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, first, 0);
+      }
     }
-    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs);
+    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs, first.get());
     if (p.host_io)
       HDB_CUDA(cudaMemcpyAsync(labels, Luse, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     HDB_CUDA(cudaEventRecord(ev[6], st));
@@ -708,14 +748,18 @@ HDB_API hdb_status hdb_run_knn(hdb_ctx *h, const hdb_nnd_element *G, const float
     HDB_CUDA(cudaEventRecord(ev[1], st));
     HDB_CUDA(cudaEventRecord(ev[2], st));
     Buf<int32_t> ids(ctx, (size_t)n * k);
-    Buf<float> core(ctx, n);
+    Buf<float> core(ctx, n), first;
     {
       Buf<float> dist;
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, Guse, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
       core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
+      if (p.mst_gpu) {
+        first = Buf<float>(ctx, n);
+        core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, first, 0);
+      }
     }
-    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs);
+    run_after_knn(ctx, ids, core, Xuse, n, d, k, p, Luse, &rs, first.get());
     if (p.host_io)
       HDB_CUDA(cudaMemcpyAsync(labels, Luse, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     HDB_CUDA(cudaEventRecord(ev[6], st));

@@ -327,11 +327,11 @@ __global__ void k_emit_reverse(const int32_t *__restrict__ ids, const uint32_t *
   }
 }
 
-__global__ void k_core_from_dist(const float *__restrict__ dist, int64_t n, int k,
+__global__ void k_core_from_dist(const float *__restrict__ dist, int64_t n, int k, int col,
                                  float *__restrict__ core) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    core[i] = dist[i * k + (k - 1)];
+    core[i] = dist[i * k + col];
 }
 
 // Core distance as the reference's fix_distances would give it for the k-th
@@ -344,7 +344,7 @@ __global__ void k_core_from_dist(const float *__restrict__ dist, int64_t n, int 
 constexpr int kCoreCols = 32, kCoreLd = kCoreCols + 1, kCoreWarps = 4;
 __global__ void __launch_bounds__(32 * kCoreWarps)
     k_core_sqrt(const float *__restrict__ X, const int32_t *__restrict__ ids, int64_t n, int d, int k,
-                float *__restrict__ core) {
+                int col, float *__restrict__ core) {
   __shared__ float stage[kCoreWarps][2][32 * kCoreLd];
   const int lane = lane_id(), w = threadIdx.x >> 5;
   float *own = stage[w][0], *nb = stage[w][1];
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(32 * kCoreWarps)
     const int64_t row = r0 + lane;
     const bool active = row < n;
     const uint32_t act = __ballot_sync(0xffffffffu, active);
-    const int32_t v = active ? ids[row * k + (k - 1)] : 0;
+    const int32_t v = active ? ids[row * k + col] : 0;
     float soma = 0.0f;
     for (int c0 = 0; c0 < d; c0 += kCoreCols) {
       const int wd = min(kCoreCols, d - c0);
@@ -586,13 +586,15 @@ int bits_for(int64_t n) {
 }  // namespace
 
 void core_distances(Context *ctx, const float *dist, const float *X, const int32_t *ids,
-                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core) {
+                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core, int32_t col) {
   int g = grid_for(ctx, n, 256);
+  if (col < 0) col = k - 1;
+  HDB_REQUIRE(col < k, HDB_ERR_ARG, "core distances: column outside the kNN rows");
   if (mode == HDB_DIST_SQRT)
     k_core_sqrt<<<grid_for(ctx, (n + 31) / 32, kCoreWarps, 8), 32 * kCoreWarps, 0, ctx->stream>>>(
-        X, ids, n, d, k, core);
+        X, ids, n, d, k, col, core);
   else
-    k_core_from_dist<<<g, 256, 0, ctx->stream>>>(dist, n, k, core);
+    k_core_from_dist<<<g, 256, 0, ctx->stream>>>(dist, n, k, col, core);
   ctx->launches++;
   HDB_CHECK_LAUNCH();
 }

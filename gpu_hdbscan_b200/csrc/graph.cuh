@@ -9,10 +9,11 @@ struct GraphTimes {
 };
 
 // core[i]: distance to the k-th neighbour (calculateCoreDistance with index
-// k-1, HDBSCAN/graphs/graph.cu:77).  mode HDB_DIST_SQRT recomputes it with
-// fix_distances' sqrt-L2 rounding; HDB_DIST_SQUARED reads dist[i, k-1].
+// k-1, HDBSCAN/graphs/graph.cu:77), or to neighbour `col` when col >= 0.
+// mode HDB_DIST_SQRT recomputes it with fix_distances' sqrt-L2 rounding;
+// HDB_DIST_SQUARED reads dist[i, col].
 void core_distances(Context *ctx, const float *dist, const float *X, const int32_t *ids,
-                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core);
+                    int64_t n, int32_t d, int32_t k, int32_t mode, float *core, int32_t col = -1);
 
 // seg: independent instances (antihubs and clique per instance); ids must
 // stay inside their row's instance.  Empty for one instance.

@@ -12,6 +12,10 @@
 // root), pointer jumping, and compaction of the edges that still cross
 // components.  The chosen keys, radix-sorted, give the reference's sorted
 // MSTedge list directly.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "hdb_internal.cuh"
 #include "mst.cuh"
 
@@ -29,6 +33,45 @@ struct alignas(16) CEdge {
 __device__ __forceinline__ uint32_t weight_key(float w) {
   // -0.0 and +0.0 compare equal in the reference (std::sort / merge on <)
   return float_key(w == 0.0f ? 0.0f : w);
+}
+
+// ---- the reference's mst_gpu = 1 mode (int-quantised weights) ------------
+// buildGPUgraph (core-sg.cu:33-36): (int)(10^m * w); a product outside the
+// int range takes INT_MIN, the value x86's truncating conversion gives it.
+__device__ __forceinline__ int32_t quantise(float w, double p10) {
+  const double v = __dmul_rn(p10, (double)w);
+  return (v < 2147483648.0 && v > -2147483649.0) ? (int32_t)v : INT32_MIN;
+}
+// buildMST_gpu (mst.cu:360): (1.0 * q) / 10^m, stored as float.
+__device__ __forceinline__ float dequantise(int32_t q, double p10) {
+  return __double2float_rn(__ddiv_rn((double)q, p10));
+}
+// gpuMST's key (mst.cu:163): the int weight's bits above the edge index, so
+// an INT_MIN weight sorts after every other one.
+__device__ __forceinline__ uint64_t quant_key(int32_t q, int64_t j) {
+  return ((uint64_t)(uint32_t)q << 32) | (uint64_t)(uint32_t)j;
+}
+
+// Smallest positive first-neighbour distance of every instance's rows after
+// its first (GetMinDistanceFromKNNG, tools/filetool.hpp:330-336); the first
+// row's own rule is applied on the host.  Positive floats order as their bits.
+__global__ void k_first_min(const float *__restrict__ first, int64_t stride, int64_t n, Segments seg,
+                            uint32_t *__restrict__ minbits) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = seg.count > 0 ? seg.of_point(i) : 0;
+    if (i == (seg.count > 0 ? seg.off[t] : 0)) continue;
+    const float d = first[i * stride];
+    if (d > 0.0f) atomicMin(&minbits[t], __float_as_uint(d));
+  }
+}
+
+__global__ void k_first_rows(const float *__restrict__ first, int64_t stride, Segments seg,
+                             float *__restrict__ out) {
+  const int32_t T = seg.count > 0 ? seg.count : 1;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T;
+       t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = first[(seg.count > 0 ? seg.off[t] : 0) * stride];
 }
 
 __global__ void k_count_canon(const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
@@ -49,14 +92,18 @@ __global__ void k_count_canon(const int64_t *__restrict__ nindex, const int32_t 
   }
 }
 
+// quant (optional): per-instance 10^m of the mst_gpu = 1 mode; keys then
+// order by (int weight, edge index) as gpuMST's do.
 __global__ void k_emit_canon(const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
                              const float *__restrict__ ew, const int64_t *__restrict__ off,
-                             int64_t n, CEdge *__restrict__ el) {
+                             int64_t n, const double *__restrict__ quant, Segments seg,
+                             CEdge *__restrict__ el) {
   const int lane = lane_id();
   int64_t row = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
   for (; row < n; row += (int64_t)gridDim.x * kWarps) {
     int64_t b = nindex[row], e = nindex[row + 1];
     int64_t p = off[row];
+    const double p10 = quant ? quant[seg.count > 0 ? seg.of_point(row) : 0] : 0.0;
     for (int64_t j0 = b; j0 < e; j0 += 32) {
       int64_t j = j0 + lane;
       bool take = j < e && nlist[j] > row;
@@ -65,7 +112,8 @@ __global__ void k_emit_canon(const int64_t *__restrict__ nindex, const int32_t *
         CEdge c;
         c.a = (int32_t)row;
         c.b = nlist[j];
-        c.key = ((uint64_t)weight_key(ew[j]) << 32) | (uint64_t)(uint32_t)j;
+        c.key = quant ? quant_key(quantise(ew[j], p10), j)
+                      : ((uint64_t)weight_key(ew[j]) << 32) | (uint64_t)(uint32_t)j;
         el[p + __popc(m & lanemask_lt())] = c;
       }
       p += __popc(m);
@@ -203,9 +251,11 @@ __device__ __forceinline__ int32_t row_of(const int64_t *__restrict__ nindex, in
   return (int32_t)lo;
 }
 
+// quant (optional): write the dequantised weight (buildMST_gpu).
 __global__ void k_gather_mst(const uint64_t *__restrict__ keys, int64_t m,
                              const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
-                             const float *__restrict__ ew, int64_t n, hdb_mst_edge *__restrict__ out,
+                             const float *__restrict__ ew, int64_t n, const double *__restrict__ quant,
+                             Segments seg, hdb_mst_edge *__restrict__ out,
                              uint8_t *__restrict__ in_mst) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -213,9 +263,28 @@ __global__ void k_gather_mst(const uint64_t *__restrict__ keys, int64_t m,
     hdb_mst_edge e;
     e.from_node = row_of(nindex, n, j);
     e.to_node = nlist[j];
-    e.weight = ew[j];
+    if (quant) {
+      const double p10 = quant[seg.count > 0 ? seg.of_point(e.from_node) : 0];
+      e.weight = dequantise(quantise(ew[j], p10), p10);
+    } else {
+      e.weight = ew[j];
+    }
     out[t] = e;
     if (in_mst) in_mst[j] = 1;
+  }
+}
+
+// mst_gpu = 1 output order: buildMST_gpu lists the tree in CSR order and
+// sort_edges sorts it stably by the dequantised weight, i.e. by (weight, edge
+// index).  Re-key the chosen edges that way.
+__global__ void k_quant_rekey(uint64_t *__restrict__ keys, int64_t m,
+                              const int64_t *__restrict__ nindex, const float *__restrict__ ew,
+                              int64_t n, const double *__restrict__ quant, Segments seg) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = (uint32_t)keys[t];
+    const double p10 = quant[seg.count > 0 ? seg.of_point(row_of(nindex, n, j)) : 0];
+    keys[t] = ((uint64_t)weight_key(dequantise(quantise(ew[j], p10), p10)) << 32) | (uint64_t)j;
   }
 }
 
@@ -255,8 +324,41 @@ __global__ void k_permute_edges(const hdb_mst_edge *__restrict__ in, const uint3
 
 }  // namespace
 
+void quant_scales(Context *ctx, const float *first, int64_t stride, int64_t n, const Segments &seg,
+                  double *p10_dev, int32_t *mult_out) {
+  cudaStream_t st = ctx->stream;
+  const int32_t T = seg.count > 0 ? seg.count : 1;
+  Buf<uint32_t> minbits(ctx, T);
+  Buf<float> row0(ctx, T);
+  std::vector<uint32_t> hb((size_t)T, 0x7f800000u);  // +inf: no positive distance
+  HDB_CUDA(cudaMemcpyAsync(minbits, hb.data(), T * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  k_first_min<<<grid_for(ctx, n, 256), 256, 0, st>>>(first, stride, n, seg, minbits); ctx->launches++;
+  k_first_rows<<<grid_for(ctx, T, 256), 256, 0, st>>>(first, stride, seg, row0); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  std::vector<float> h0((size_t)T);
+  HDB_CUDA(cudaMemcpyAsync(hb.data(), minbits, T * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  HDB_CUDA(cudaMemcpyAsync(h0.data(), row0, T * sizeof(float), cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  std::vector<double> p10((size_t)T);
+  for (int32_t t = 0; t < T; t++) {
+    // GetMinDistanceFromKNNG (filetool.hpp:318-336): start at 999, the first
+    // row's distance replaces it when positive, later ones when smaller
+    double m = h0[t] > 0.0f ? (double)h0[t] : 999.0;
+    float later;
+    memcpy(&later, &hb[t], sizeof(float));
+    if ((double)later < m) m = (double)later;
+    // buildGPUgraph (core-sg.cu:13, 35): m = ceil(-log10|min|) + 2, 10^m
+    const int32_t mult = (int32_t)(std::ceil(-std::log10(std::fabs(m))) + 2);
+    p10[t] = std::pow(10.0, mult);
+    if (mult_out) mult_out[t] = mult;
+  }
+  HDB_CUDA(cudaMemcpyAsync(p10_dev, p10.data(), T * sizeof(double), cudaMemcpyHostToDevice, st));
+  ctx->sync();
+}
+
 int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
-                    int32_t *rounds_out, const Segments &seg, int32_t *inst_edges) {
+                    int32_t *rounds_out, const Segments &seg, int32_t *inst_edges,
+                    const double *quant) {
   const int64_t n = g->nodes;
   HDB_REQUIRE(n >= 2, HDB_ERR_ARG, "MST: need at least 2 nodes");
   // one tree per instance: n - (number of instances) edges
@@ -276,7 +378,7 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
   ctx->sync();
   int64_t m = h[0];
   Buf<CEdge> el(ctx, m > 0 ? m : 1), el2(ctx, m > 0 ? m : 1);
-  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, el); ctx->launches++;
+  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, quant, seg, el); ctx->launches++;
   HDB_CHECK_LAUNCH();
 
   Buf<unsigned long long> minkey(ctx, n);
@@ -346,12 +448,17 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
     if (rounds_out) *rounds_out = rounds;
     return 0;
   }
-  radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
   const int gm = grid_for(ctx, chosen, 256);
+  if (quant) {
+    k_quant_rekey<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->eweight, n, quant, seg); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
+  radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
   if (seg.count > 1) {
     // each instance's edges together, in (weight, edge index) order inside it
     Buf<hdb_mst_edge> tmp(ctx, chosen);
-    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, tmp, in_mst); ctx->launches++;
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, quant, seg,
+                                     tmp, in_mst); ctx->launches++;
     Buf<uint32_t> ikeys(ctx, chosen), idx(ctx, chosen);
     k_edge_instance<<<gm, 256, 0, st>>>(tmp, chosen, seg, ikeys, idx); ctx->launches++;
     HDB_CHECK_LAUNCH();
@@ -360,7 +467,8 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
     radix_sort_u32(ctx, ikeys, idx, chosen, 0, bits);
     k_permute_edges<<<gm, 256, 0, st>>>(tmp, idx, chosen, mst); ctx->launches++;
   } else {
-    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, mst, in_mst); ctx->launches++;
+    k_gather_mst<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->nlist, g->eweight, n, quant, seg,
+                                     mst, in_mst); ctx->launches++;
   }
   HDB_CHECK_LAUNCH();
   ctx->sync();

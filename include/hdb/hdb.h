@@ -89,6 +89,8 @@ typedef struct {
                           HDB_DIST_SQUARED: NN-Descent's squared distances kept */
   int32_t stability;   /* HDB_STAB_FP32 (tree.cu:494-511 order) or HDB_STAB_FP64 */
   int32_t host_io;     /* hdb_run only: 1 = X and labels are host pointers */
+  int32_t mst_gpu;     /* the reference's argv[4] (HDBSCAN/new.cu:38): 0 = the float
+                          MST of cpuMST; 1 = its int-quantised GPU MST (hdb_mst_quantised) */
 } hdb_params;
 
 typedef struct {
@@ -105,6 +107,8 @@ typedef struct {
   int64_t join_rows_gathered;   /* sampled rows staged in shared memory, all launches */
   int64_t join_candidates;      /* candidates that passed the k-th distance filter */
   int64_t gpu_launches;         /* kernel launches issued by the call */
+  int32_t mst_multiplier;       /* mst_gpu = 1: the weight scale exponent m (single runs) */
+  int32_t reserved;
 } hdb_run_stats;
 
 typedef struct hdb_ctx hdb_ctx;
@@ -168,6 +172,21 @@ HDB_API hdb_status hdb_core_sg(hdb_ctx *ctx, const int32_t *ids, const float *di
  * graph is not connected. */
 HDB_API hdb_status hdb_mst(hdb_ctx *ctx, const hdb_graph *graph, uint8_t *in_mst,
                            hdb_mst_edge *mst, int32_t *rounds);
+
+/* The mst_gpu = 1 MST of build_CoreSG (core-sg.cu:533-540): buildGPUgraph
+ * (core-sg.cu:8-44) scales every weight to the int (int)(10^m * w), m =
+ * ceil(-log10(min)) + 2 with `min` the smallest positive first-neighbour
+ * distance as FileTool::GetMinDistanceFromKNNG takes it (row 0's distance
+ * when positive, else 999, then any smaller positive one; dist[i * k] is row
+ * i's first distance, device memory); gpuMST (mst.cu:210-288) spans the
+ * graph under the order (int weight, CSR edge index); buildMST_gpu
+ * (mst.cu:338-380) writes the tree with the weights (float)(q / 10^m), sorted
+ * stably by weight.  A scaled weight beyond the int range becomes INT_MIN, as
+ * the reference's conversion does on x86.  *multiplier (optional) receives m.
+ * HDB_ERR_DISCONNECTED if the graph is not connected. */
+HDB_API hdb_status hdb_mst_quantised(hdb_ctx *ctx, const hdb_graph *graph, const float *dist,
+                                     int32_t k, uint8_t *in_mst, hdb_mst_edge *mst,
+                                     int32_t *multiplier, int32_t *rounds);
 
 /* sort_edges, HDBSCAN/merge_sort/merge_sort.cuh:30: stable ascending sort by
  * weight, in place. */

@@ -3,6 +3,8 @@ import ctypes as C
 import os
 import re
 
+import pytest
+
 from conftest import ROOT
 
 
@@ -46,5 +48,33 @@ def test_struct_layouts_match_reference_records():
     assert O.CONDENSED_NODE.itemsize == 16
     assert O.STABILITY.itemsize == 8
     assert C.sizeof(_lib.KnnParams) == 16
-    assert C.sizeof(_lib.Params) == 32
     assert C.sizeof(_lib.Graph) == 56
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every struct the ctypes binding declares has the size and field
+    offsets the C compiler gives include/hdb/hdb.h."""
+    import shutil
+    import subprocess
+    from gpu_hdbscan_b200 import _lib
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    pairs = {"hdb_knn_params": _lib.KnnParams, "hdb_params": _lib.Params, "hdb_graph": _lib.Graph,
+             "hdb_run_stats": _lib.RunStats, "hdb_instance": _lib.Instance}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hdb/hdb.h"', "int main(void) {"]
+    for cname, cls in pairs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "sizes.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "sizes"
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-I", inc, "-o", str(exe), str(src)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    for cname, cls in pairs.items():
+        assert int(got[cname]) == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, (cname, fname)

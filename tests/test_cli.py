@@ -92,11 +92,15 @@ def test_text_vectors_and_fvecs_conversion(tmp_path):
         for row in X:
             f.write(" ".join(repr(float(v)) for v in row) + "\n")
     fv = tmp_path / "out.fvecs"
+    kg = tmp_path / "g.kgraph"
     la, lb = tmp_path / "a.txt", tmp_path / "b.txt"
-    r = run(0, 8, 1, 0, "--vectors-txt", txt, "--write-fvecs", fv, "--labels", la)
+    r = run(0, 8, 1, 0, "--vectors-txt", txt, "--write-fvecs", fv, "--save-kgraph", kg,
+            "--labels", la)
     assert r.returncode == 0, r.stderr
     back = np.fromfile(fv, np.float32).reshape(1200, 4)
     np.testing.assert_array_equal(back[:, 1:], X)
-    r = run(0, 8, 1, 0, "--vectors", fv, "--labels", lb)
+    # the same graph (two NN-Descent runs may differ a little) from the .fvecs
+    # copy: fix_distances reads the vectors again, so any change would show
+    r = run(0, 8, 1, 0, "--vectors", fv, "--kgraph", kg, "--labels", lb)
     assert r.returncode == 0, r.stderr
     np.testing.assert_array_equal(np.loadtxt(la), np.loadtxt(lb))
