@@ -399,8 +399,11 @@ def run_ours(args, w):
 
 def batch_cpu_sample(bw, layout, min_points=50_000):
     """The first instances of the layout up to `min_points` points, built on
-    the host (numpy) for the CPU timing."""
+    the host (numpy) for the CPU timing (for a split workload: one piece's
+    worth of points drawn from the mixture)."""
     from gpu_hdbscan_b200 import synth
+    if isinstance(bw, synth.SplitWorkload):
+        return [synth.sample(bw.w, min_points)]
     Xs, tot = [], 0
     for i, (n, d, b) in enumerate(layout):
         Xs.append(synth.generate(synth.batch_instance(bw, i, n, d, b)))
@@ -469,7 +472,7 @@ def run_ours_batch(args, bw):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
-    rbw = synth.BatchWorkload(**{**bw.__dict__, "seed": bw.seed + 1000 * rank})
+    rbw = type(bw)(**{**bw.__dict__, "seed": bw.seed + 1000 * rank})
     views, layout = synth.generate_batch_torch(rbw, device=dev, count=args.instances or None)
     n_total = sum(n for n, _, _ in layout)
     ctx = g.Context(local)
@@ -604,10 +607,10 @@ def run_ours_batch(args, bw):
 def main():
     args = parse_args()
     from gpu_hdbscan_b200 import synth
-    if args.workload in synth.BATCH_WORKLOADS:
-        bw = synth.BATCH_WORKLOADS[args.workload]
+    if args.workload in synth.BATCH_WORKLOADS or args.workload in synth.SPLIT_WORKLOADS:
+        bw = synth.BATCH_WORKLOADS.get(args.workload) or synth.SPLIT_WORKLOADS[args.workload]
         if args.precision is None:
-            args.precision = "fp32"
+            args.precision = getattr(bw, "precision", "fp32")
         if args.impl == "reference":
             run_reference_batch(args, bw)
         else:

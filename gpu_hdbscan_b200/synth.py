@@ -160,6 +160,48 @@ BATCH_WORKLOADS = {
 }
 
 
+@dataclass(frozen=True)
+class SplitWorkload:
+    """One workload of WORKLOADS cut into `parts` uneven consecutive pieces
+    (its rows are shuffled, so each piece is a random sample of the mixture),
+    each clustered on its own.  Piece sizes are log-uniform in [1, spread],
+    scaled to the workload's n; `seed` seeds both the sizes and the data."""
+    name: str
+    base: str
+    parts: int
+    spread: float
+    seed: int
+    precision: str = "bf16"
+
+    @property
+    def w(self) -> Workload:
+        return WORKLOADS[self.base]
+
+    @property
+    def count(self):
+        return self.parts
+
+    k = property(lambda self: self.w.k)
+    mpts = property(lambda self: self.w.mpts)
+    sample_num = property(lambda self: self.w.sample_num)
+    iterations = property(lambda self: self.w.iterations)
+
+
+SPLIT_WORKLOADS = {
+    # 50M x 96 (200 Zipf-sized blobs, sigma in [0.2, 3.0], 8 % noise) as 64
+    # uneven sub-instances, sizes spread over a factor of 20
+    "blobs_50m_d96_split64": SplitWorkload("blobs_50m_d96_split64", "blobs_50m_d96", 64, 20.0, 5),
+}
+
+
+def split_sizes(sw: SplitWorkload, count: int | None = None):
+    rng = np.random.default_rng(sw.seed)
+    r = np.exp(rng.uniform(0.0, np.log(sw.spread), size=sw.parts))
+    sizes = np.floor(r / r.sum() * sw.w.n).astype(np.int64)
+    sizes[: sw.w.n - sizes.sum()] += 1
+    return [int(x) for x in sizes[: sw.parts if count is None else count]]
+
+
 def batch_layout(bw: BatchWorkload, count: int | None = None):
     """Per instance (n, d, blobs), seeded; the first `count` instances."""
     rng = np.random.default_rng(bw.seed)
@@ -178,12 +220,21 @@ def batch_instance(bw: BatchWorkload, i: int, n: int, d: int, blobs: int) -> Wor
                     bw.seed * 1_000_003 + i)
 
 
-def generate_batch_torch(bw: BatchWorkload, device="cuda", count: int | None = None):
+def generate_batch_torch(bw, device="cuda", count: int | None = None):
     """The instances on `device`: one [sum n, d] array per d with the instances
     of that d back to back (in instance order), and per instance a view into
-    it, in instance order.  -> (views, layout)."""
+    it, in instance order.  -> (views, layout of (n, d, blobs))."""
     import torch
 
+    if isinstance(bw, SplitWorkload):
+        sizes = split_sizes(bw, count)
+        w = Workload(**{**bw.w.__dict__, "n": sum(sizes), "seed": bw.seed})
+        X = generate_torch(w, device=device)
+        views, row = [], 0
+        for m in sizes:
+            views.append(X[row:row + m])
+            row += m
+        return views, [(m, w.d, 0) for m in sizes]
     layout = batch_layout(bw, count)
     by_d = {}
     for i, (n, d, b) in enumerate(layout):
