@@ -864,6 +864,171 @@ __global__ void k_ovf_bounds(const uint32_t *__restrict__ tgt, int64_t cnt, uint
   }
 }
 
+// ---- locality order ---------------------------------------------------------
+// The local join gathers the rows of every row's samples, i.e. of its current
+// neighbours.  With ids in arbitrary order those rows lie anywhere in X, and
+// the ~2,000 consecutive rows the join works on at any moment fetch them all
+// from HBM.  After the initial graph the points are renumbered so that near
+// points get near ids: by instance, then by the Morton code of three
+// projections on fixed +-1 vectors (10 bits each over the projection's range).
+// The rows in flight then gather from a few MB of X, which L2 holds.  The final
+// graph is mapped back to the original ids and every row re-sorted by
+// (distance, id), so the order is the caller's.
+constexpr int kLocProj = 3;
+
+__device__ __forceinline__ float loc_sign(int p, int j) {
+  return (xorshift64star(((uint64_t)(p + 1) << 32) | (uint32_t)j) >> 63) ? -1.0f : 1.0f;
+}
+
+// One warp per row: the three projections; per block the range of each.
+__global__ void k_loc_project(const float *__restrict__ X, int64_t n, int d,
+                              float *__restrict__ proj, uint32_t *__restrict__ range) {
+  __shared__ uint32_t blk[2 * kLocProj];
+  if (threadIdx.x < 2 * kLocProj) blk[threadIdx.x] = (threadIdx.x & 1) ? 0u : 0xffffffffu;
+  __syncthreads();
+  const int lane = lane_id(), wpb = blockDim.x >> 5;
+  uint32_t lo[kLocProj], hi[kLocProj];
+#pragma unroll
+  for (int p = 0; p < kLocProj; p++) { lo[p] = 0xffffffffu; hi[p] = 0u; }
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    float acc[kLocProj] = {0.0f, 0.0f, 0.0f};
+    for (int j = lane; j < d; j += 32) {
+      const float x = X[row * d + j];
+#pragma unroll
+      for (int p = 0; p < kLocProj; p++) acc[p] += loc_sign(p, j) * x;
+    }
+#pragma unroll
+    for (int p = 0; p < kLocProj; p++) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) acc[p] += __shfl_xor_sync(0xffffffffu, acc[p], o);
+      const uint32_t key = float_key(acc[p]);
+      lo[p] = min(lo[p], key);
+      hi[p] = max(hi[p], key);
+      if (lane == p) proj[row * kLocProj + p] = acc[p];
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int p = 0; p < kLocProj; p++) {
+      atomicMin(&blk[2 * p], lo[p]);
+      atomicMax(&blk[2 * p + 1], hi[p]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kLocProj) {
+    atomicMin(&range[2 * threadIdx.x], blk[2 * threadIdx.x]);
+    atomicMax(&range[2 * threadIdx.x + 1], blk[2 * threadIdx.x + 1]);
+  }
+}
+
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 10 bits -> every third bit
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+__global__ void k_loc_keys(const float *__restrict__ proj, int64_t n, Segments seg,
+                           const uint32_t *__restrict__ range, uint64_t *__restrict__ keys,
+                           uint32_t *__restrict__ vals) {
+  float lo[kLocProj], scale[kLocProj];
+#pragma unroll
+  for (int p = 0; p < kLocProj; p++) {
+    lo[p] = key_float(range[2 * p]);
+    const float w = key_float(range[2 * p + 1]) - lo[p];
+    scale[p] = w > 0.0f ? 1024.0f / w : 0.0f;
+  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int p = 0; p < kLocProj; p++) {
+      const float q = (proj[i * kLocProj + p] - lo[p]) * scale[p];
+      const uint32_t c = q <= 0.0f ? 0u : (q >= 1023.0f ? 1023u : (uint32_t)q);
+      m |= spread3(c) << p;
+    }
+    const uint64_t inst = seg.count > 0 ? (uint64_t)seg.of_point(i) : 0;
+    keys[i] = (inst << 32) | m;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+__global__ void k_loc_inverse(const uint32_t *__restrict__ order, int64_t n, int32_t *__restrict__ inv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    inv[order[i]] = (int32_t)i;
+}
+
+__global__ void k_loc_rows(const float *__restrict__ X, const uint32_t *__restrict__ order, int64_t n,
+                           int d, float *__restrict__ Xp) {
+  const int lane = lane_id(), wpb = blockDim.x >> 5;
+  for (int64_t r = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); r < n;
+       r += (int64_t)gridDim.x * wpb) {
+    const int64_t o = order[r];
+    for (int j = lane; j < d; j += 32) Xp[r * d + j] = X[o * d + j];
+  }
+}
+
+// Row r of the output takes row src[r] of the input with every id mapped
+// through idmap; the row is re-sorted by (distance, mapped id) and each entry
+// keeps its old/new flag.  One warp per row.
+__device__ __forceinline__ void remap_row(int k, int32_t in_lab, float in_dist,
+                                          const int32_t *__restrict__ idmap, int32_t &out_lab,
+                                          float &out_dist) {
+  const int lane = lane_id();
+  const bool have = lane < k;
+  const int32_t id = have ? idmap[decode(in_lab)] : 0;
+  const bool old = have && in_lab < 0;
+  const uint64_t key = warp_sort32(have ? pack(in_dist, id) : ~0ull);
+  const int32_t mine = pk_id(key);
+  bool flag = false;
+  for (int t = 0; t < k; t++) {  // ids are distinct within a row
+    const int32_t idt = __shfl_sync(0xffffffffu, id, t);
+    const bool ot = __shfl_sync(0xffffffffu, old, t);
+    if (idt == mine) flag = ot;
+  }
+  out_dist = pk_dist(key);
+  out_lab = flag ? -mine - 1 : mine;
+}
+
+__global__ void k_loc_lists(const int32_t *__restrict__ gid, const float *__restrict__ gdist,
+                            const float *__restrict__ worst, const uint32_t *__restrict__ order,
+                            const int32_t *__restrict__ inv, int64_t n, int k,
+                            int32_t *__restrict__ gid_p, float *__restrict__ gdist_p,
+                            float *__restrict__ worst_p) {
+  const int lane = lane_id(), wpb = blockDim.x >> 5;
+  for (int64_t r = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); r < n;
+       r += (int64_t)gridDim.x * wpb) {
+    const int64_t o = order[r];
+    const int32_t lab = lane < k ? gid[o * k + lane] : 0;
+    const float dist = lane < k ? gdist[o * k + lane] : 0.0f;
+    int32_t ol;
+    float od;
+    remap_row(k, lab, dist, inv, ol, od);
+    if (lane < k) {
+      gid_p[r * k + lane] = ol;
+      gdist_p[r * k + lane] = od;
+    }
+    if (lane == 0) worst_p[r] = worst[o];
+  }
+}
+
+__global__ void k_loc_restore(const hdb_nnd_element *__restrict__ Gp, const uint32_t *__restrict__ order,
+                              int64_t n, int k, hdb_nnd_element *__restrict__ G) {
+  const int lane = lane_id(), wpb = blockDim.x >> 5;
+  for (int64_t r = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); r < n;
+       r += (int64_t)gridDim.x * wpb) {
+    hdb_nnd_element e = lane < k ? Gp[r * k + lane] : hdb_nnd_element{0.0f, 0};
+    int32_t ol;
+    float od;
+    remap_row(k, e.label_, e.distance_, reinterpret_cast<const int32_t *>(order), ol, od);
+    if (lane < k) G[(int64_t)order[r] * k + lane] = hdb_nnd_element{od, ol};
+  }
+}
+
 int bits_for_rows(int64_t n) {
   int b = 1;
   while (b < 40 && (int64_t(1) << b) < n) b++;
@@ -931,6 +1096,37 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
   k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, seg, gid, gdist, worst); ctx->launches++;
   HDB_CHECK_LAUNCH();
+
+  // renumber the points in locality order (k_loc_project); X stays the
+  // caller's, the iterations work on Xw and the renumbered lists
+  Buf<uint32_t> order(ctx, n);
+  Buf<float> Xp(ctx, (size_t)n * d);
+  {
+    Buf<float> proj(ctx, (size_t)n * kLocProj);
+    Buf<uint32_t> range(ctx, 2 * kLocProj);
+    const uint32_t range0[2 * kLocProj] = {0xffffffffu, 0u, 0xffffffffu, 0u, 0xffffffffu, 0u};
+    HDB_CUDA(cudaMemcpyAsync(range, range0, sizeof(range0), cudaMemcpyHostToDevice, st));
+    k_loc_project<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, proj, range); ctx->launches++;
+    Buf<uint64_t> keys(ctx, n);
+    k_loc_keys<<<grid_for(ctx, n, 256), 256, 0, st>>>(proj, n, seg, range, keys, order); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    int ibits = 0;
+    while (seg.count > 0 && (int64_t(1) << ibits) < seg.count) ibits++;
+    radix_sort_u64(ctx, keys, order, n, 0, 30 + (seg.count > 0 ? 2 + ibits : 0));
+    Buf<int32_t> inv(ctx, n);
+    k_loc_inverse<<<grid_for(ctx, n, 256), 256, 0, st>>>(order, n, inv); ctx->launches++;
+    k_loc_rows<<<grid_rows, 32 * wpb, 0, st>>>(X, order, n, d, Xp); ctx->launches++;
+    Buf<int32_t> gid2(ctx, n * k);
+    Buf<float> gdist2(ctx, n * k), worst2(ctx, n);
+    k_loc_lists<<<grid_rows, 32 * wpb, 0, st>>>(gid, gdist, worst, order, inv, n, k, gid2, gdist2,
+                                                worst2); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    std::swap(gid, gid2);
+    std::swap(gdist, gdist2);
+    std::swap(worst, worst2);
+  }
+  const float *Xw = Xp;
+  Buf<hdb_nnd_element> Gp(ctx, (size_t)n * k);
   const int dp = (d & 1) ? d : d + 1;
   const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
   int jw = (int)((56 * 1024) / per_warp);  // about four blocks per SM
@@ -956,9 +1152,9 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     Buf<double> csum(ctx, d);
     Buf<float> cmean(ctx, d);
     HDB_CUDA(cudaMemsetAsync(csum, 0, d * sizeof(double), st));
-    k_col_sums<<<16 * ctx->num_sms, 256, 0, st>>>(X, n, d, csum); ctx->launches++;
+    k_col_sums<<<16 * ctx->num_sms, 256, 0, st>>>(Xw, n, d, csum); ctx->launches++;
     k_col_mean<<<1, 256, 0, st>>>(csum, d, n, cmean); ctx->launches++;
-    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(X, n, d, dpad, cmean, Xb, nrm); ctx->launches++;
+    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(Xw, n, d, dpad, cmean, Xb, nrm); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (use_tc) {
       tc_join_prepare(ctx, Xb, n, dpad, &tj);
@@ -982,7 +1178,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
         k_join_bf16<<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, newS, oldS, nf, of,
                                                          nrev, orev, worst, ib);
       else
-        k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev,
+        k_join<<<grid_join, 32 * jw, smem_join, st>>>(Xw, n, d, S, newS, oldS, nf, of, nrev, orev,
                                                       worst, ib);
       ctx->launches++;
     }
@@ -991,12 +1187,14 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     sort_overflow(ctx, ib, n);
     HDB_CHECK_LAUNCH();
   }
-  k_finalize<<<grid_rows, 32 * wpb, 0, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
+  k_finalize<<<grid_rows, 32 * wpb, 0, st>>>(n, k, gid, gdist, ib, Gp); ctx->launches++;
   HDB_CHECK_LAUNCH();
   if (bf16) {
-    k_rerank<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, G); ctx->launches++;
+    k_rerank<<<grid_rows, 32 * wpb, smem_stage, st>>>(Xw, n, d, k, Gp); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
+  k_loc_restore<<<grid_rows, 32 * wpb, 0, st>>>(Gp, order, n, k, G); ctx->launches++;
+  HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   ctx->sync();
