@@ -21,20 +21,20 @@ void throw_cuda(cudaError_t e, const char *what, const char *file, int line) {
 Scratch::Scratch(Context *ctx, size_t bytes) { reset(ctx, bytes); }
 
 void Scratch::reset(Context *ctx, size_t bytes) {
-  if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+  if (ptr_) ctx_->cache_give(ptr_, cls_);
   ptr_ = nullptr;
   ctx_ = ctx;
   bytes_ = bytes;
-  if (bytes == 0) bytes = 16;
-  HDB_CUDA(cudaMallocAsync(&ptr_, bytes, ctx->stream));
+  ptr_ = ctx->cache_take(bytes == 0 ? 16 : bytes, &cls_);
 }
 
 Scratch &Scratch::operator=(Scratch &&o) noexcept {
   if (this != &o) {
-    if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+    if (ptr_) ctx_->cache_give(ptr_, cls_);
     ctx_ = o.ctx_;
     ptr_ = o.ptr_;
     bytes_ = o.bytes_;
+    cls_ = o.cls_;
     o.ptr_ = nullptr;
     o.bytes_ = 0;
   }
@@ -42,7 +42,49 @@ Scratch &Scratch::operator=(Scratch &&o) noexcept {
 }
 
 Scratch::~Scratch() {
-  if (ptr_) cudaFreeAsync(ptr_, ctx_->stream);
+  if (ptr_) ctx_->cache_give(ptr_, cls_);
+}
+
+static size_t size_class(size_t bytes) {
+  size_t p = 512;
+  while (p < bytes && p < (size_t(1) << 20)) p <<= 1;
+  if (bytes <= p) return p;
+  size_t top = size_t(1) << 20;
+  while (top * 2 <= bytes) top <<= 1;  // largest power of two <= bytes
+  const size_t step = top / 4;
+  return (bytes + step - 1) / step * step;
+}
+
+void *Context::cache_take(size_t bytes, size_t *cls) {
+  const size_t c = size_class(bytes);
+  *cls = c;
+  auto it = cache_free.find(c);
+  if (it != cache_free.end()) {
+    void *p = it->second;
+    cache_free.erase(it);
+    return p;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, c);
+  if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and retry once
+    cudaGetLastError();
+    cache_release();
+    e = cudaMalloc(&p, c);
+  }
+  HDB_CUDA(e);
+  cache_bytes += c;
+  return p;
+}
+
+void Context::cache_give(void *p, size_t cls) { cache_free.emplace(cls, p); }
+
+void Context::cache_release() {
+  cudaStreamSynchronize(stream);  // queued work may still use a free block
+  for (auto &b : cache_free) {
+    cudaFree(b.second);
+    cache_bytes -= b.first;
+  }
+  cache_free.clear();
 }
 
 void Context::sync() { HDB_CUDA(cudaStreamSynchronize(stream)); }
@@ -104,11 +146,6 @@ HDB_API hdb_status hdb_create(hdb_ctx **out, int32_t device) {
       HDB_CUDA(cudaMemset(c.dev_err, 0, 4 * sizeof(uint32_t)));
       HDB_CUDA(cudaMallocHost(&c.pinned, kPinnedBytes));
       for (auto &e : c.ev) HDB_CUDA(cudaEventCreate(&e));
-      // Keep freed scratch cached in the stream-ordered pool between calls.
-      cudaMemPool_t pool;
-      HDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-      uint64_t thr = UINT64_MAX;
-      HDB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     } catch (...) {
       hdb_destroy(h);
       throw;
@@ -131,6 +168,7 @@ HDB_API hdb_status hdb_destroy(hdb_ctx *h) {
     cudaFree(c.sg_nlist);
     cudaFree(c.sg_eweight);
     cudaFree(c.dev_err);
+    c.cache_release();
     if (c.pinned) cudaFreeHost(c.pinned);
     for (auto &e : c.ev)
       if (e) cudaEventDestroy(e);
@@ -142,6 +180,8 @@ HDB_API hdb_status hdb_destroy(hdb_ctx *h) {
 HDB_API hdb_status hdb_set_stream(hdb_ctx *h, void *stream) {
   return guard([&] {
     HDB_REQUIRE(h != nullptr, HDB_ERR_ARG, "hdb_set_stream: NULL context");
+    // cached scratch blocks were last used in the old stream's order
+    if (h->c.stream) HDB_CUDA(cudaStreamSynchronize(h->c.stream));
     h->c.stream = stream ? static_cast<cudaStream_t>(stream) : h->c.own_stream;
   });
 }

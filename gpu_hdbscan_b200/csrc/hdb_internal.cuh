@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 
@@ -69,8 +70,8 @@ enum : uint32_t {
 // ---------------------------------------------------------------------------
 struct Context;
 
-// Stream-ordered scratch buffer (cudaMallocAsync on the context stream, freed
-// with cudaFreeAsync when it goes out of scope).
+// Scratch buffer from the context's block cache (Context::cache_take), given
+// back to it when it goes out of scope.
 class Scratch {
  public:
   Scratch() = default;
@@ -90,6 +91,7 @@ class Scratch {
   Context *ctx_ = nullptr;
   void *ptr_ = nullptr;
   size_t bytes_ = 0;
+  size_t cls_ = 0;  // size class of the block
 };
 
 template <typename T>
@@ -131,6 +133,19 @@ struct Context {
   cudaEvent_t join_ev[2] = {};
   double join_ms = 0.0;
   int64_t join_launches = 0;
+
+  // Scratch block cache: blocks are rounded up to a size class (four per
+  // octave above 1 MB, powers of two below) and kept on a free list when
+  // their Scratch goes away, so repeated calls reuse them instead of asking
+  // the driver for multi-GB blocks every time.  All of a context's work is in
+  // order on its stream, and every entry point ends with a stream sync, so a
+  // block given back is free for the next taker.  Released by hdb_destroy,
+  // or when the driver runs out of memory.
+  std::multimap<size_t, void *> cache_free;
+  size_t cache_bytes = 0;  // all blocks held (free or in use)
+  void *cache_take(size_t bytes, size_t *cls);
+  void cache_give(void *p, size_t cls);
+  void cache_release();
 
   void sync();
   // Reads and clears the device error word.
