@@ -19,7 +19,10 @@
 //               warps keep more gathers in flight;
 //   warp 6      one thread issues the MMAs and commits them to mbarriers;
 //   warps 0..3  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//               lanes 32w..32w+31 = tile rows), row minima, candidate pushes.
+//               lanes 32w..32w+31 = tile rows), row minima, and the
+//               candidates appended to the target-sorted list of the merge
+//               (one reservation per warp and tile; the per-row inboxes of
+//               the SIMT joins would cost a returning atomic per candidate).
 // Stages form a ring of three (full / empty mbarriers); accumulators a ring
 // of two (acc_full / acc_empty).  Every wait is bounded in time: a wait that
 // gives up sets DEVERR_TIMEOUT and makes every role of the CTA stop, after
@@ -479,39 +482,17 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
     atomicOr(err, DEVERR_TIMEOUT);
 }
 
-// A push whose inbox slot was claimed; the store waits for the next tile so
-// that the atomic's round trip overlaps it.
-struct PendingPush {
-  int32_t target;
-  int32_t slot;  // -1: none
-  uint64_t key;
-};
-
-__device__ __forceinline__ void finish_push(PendingPush &p, const Inbox &ib) {
-  if (p.slot < 0) return;
-  if (p.slot < kInboxCap) {
-    ib.slots[(int64_t)p.target * kInboxCap + p.slot] = p.key;
+// A candidate at position pos of the target-sorted list of the next merge;
+// past the list's capacity only the best dropped candidate per target is kept.
+__device__ __forceinline__ void append_candidate(const Inbox &ib, unsigned long long pos,
+                                                 int32_t target, uint64_t key) {
+  if ((int64_t)pos < ib.ovf_cap) {
+    ib.ovf_tgt[pos] = (uint32_t)target;
+    ib.ovf_key[pos] = key;
   } else {
-    unsigned long long pos = atomicAdd(&ib.counters[3], 1ull);
-    if ((int64_t)pos < ib.ovf_cap) {
-      ib.ovf_tgt[pos] = (uint32_t)p.target;
-      ib.ovf_key[pos] = p.key;
-    } else {
-      atomicMin(&ib.best[p.target], (unsigned long long)p.key);
-      atomicAdd(&ib.counters[0], 1ull);
-    }
+    atomicMin(&ib.best[target], (unsigned long long)key);
+    atomicAdd(&ib.counters[0], 1ull);
   }
-  p.slot = -1;
-}
-
-__device__ __forceinline__ int start_push(PendingPush &p, int32_t target, int32_t cand,
-                                          uint32_t dbits, float wst, const Inbox &ib) {
-  const float dist = __uint_as_float(dbits);
-  if (!(dist < wst)) return 0;  // cannot enter the target's list
-  p.target = target;
-  p.key = pack(dist, cand);
-  p.slot = atomicAdd(&ib.cnt[target], 1);
-  return 1;
 }
 
 // Row minimum over 32 columns: key = clamped distance bits with the column in
@@ -542,7 +523,6 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
   const int j = w >> 1;                 // row-join of this warp's 32 rows
   const bool isnew = (w & 1) == 0;      // new rows (slots 0..31) or old rows (32..63)
   const int slot = (isnew ? 0 : 32) + lane;
-  PendingPush p0{0, -1, 0}, p1{0, -1, 0};
   int64_t t = blockIdx.x;
   for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
     const int s = i % kStages;
@@ -587,9 +567,6 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
       if (lane == 0) mbar_arrive(&sh.empty[s]);
       continue;
     }
-    // the previous tile's claimed slots: their atomics have returned by now
-    finish_push(p0, a.ib);
-    finish_push(p1, a.ib);
     uint32_t k1, k2 = 0xffffffffu;
     int32_t id1 = -1, id2 = -1;
     if (isnew) {
@@ -602,14 +579,22 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
     __syncwarp();
     if (lane == 0) mbar_arrive(&sh.empty[s]);
-    if (vrow) {
-      if (id1 >= 0) cands += start_push(p0, myid, id1, k1 & ~63u, wst, a.ib);
-      if (id2 >= 0) cands += start_push(p1, myid, id2, k2 & ~63u, wst, a.ib);
+    // candidates that can enter their target's list, appended to the list
+    // that is sorted by target before the next merge: one reservation per
+    // warp instead of a returning inbox atomic per candidate
+    const float d1 = __uint_as_float(k1 & ~63u), d2 = __uint_as_float(k2 & ~63u);
+    const bool c1 = vrow && id1 >= 0 && d1 < wst, c2 = vrow && id2 >= 0 && d2 < wst;
+    const uint32_t b1 = __ballot_sync(0xffffffffu, c1), b2 = __ballot_sync(0xffffffffu, c2);
+    const uint32_t tot = __popc(b1) + __popc(b2);
+    if (tot) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&a.ib.counters[3], (unsigned long long)tot);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (c1) append_candidate(a.ib, base + __popc(b1 & lanemask_lt()), myid, pack(d1, id1));
+      if (c2)
+        append_candidate(a.ib, base + __popc(b1) + __popc(b2 & lanemask_lt()), myid, pack(d2, id2));
+      cands += (c1 ? 1 : 0) + (c2 ? 1 : 0);
     }
-  }
-  if (!kProbe) {
-    finish_push(p0, a.ib);
-    finish_push(p1, a.ib);
   }
 }
 

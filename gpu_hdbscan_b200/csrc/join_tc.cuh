@@ -33,7 +33,8 @@ struct TcJoin {
 void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad, TcJoin *tj);
 
 // One local-join pass over all rows: the sample lists of k_sample in, the
-// candidates out through the inbox (same contract as the SIMT join).
+// candidates out through the inbox's overflow list only (ib.ovf_cap must hold
+// a pass's candidates; sort_overflow groups them by target for the merge).
 void tc_join_launch(Context *ctx, const TcJoin &tj, int S, const float *nrm, const int32_t *newS,
                     const int32_t *oldS, const int8_t *nf, const int8_t *of, int32_t *nrev,
                     int32_t *orev, const float *worst, const knn::Inbox &ib);

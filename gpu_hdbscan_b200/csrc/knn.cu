@@ -1072,9 +1072,14 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   Buf<int32_t> newS(ctx, n * 2 * S), oldS(ctx, n * 2 * S), nrev(ctx, n), orev(ctx, n),
       inbox_cnt(ctx, n);
   Buf<int8_t> nf(ctx, n), of(ctx, n);
-  Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
+  // The tensor-core join appends every candidate to the target-sorted list
+  // (a returning inbox atomic per candidate costs it more than the sort), so
+  // it needs no inboxes and a list for a whole iteration's candidates.
+  const bool tc_form = p.precision == HDB_PREC_BF16 && tc_dpad(d) <= kTcMaxDpad;
+  Buf<uint64_t> inbox(ctx, tc_form ? 1 : (size_t)n * kInboxCap);
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
-  const int64_t ovf_cap = n * 16 > (1 << 22) ? n * 16 : (1 << 22);
+  const int64_t ovf_rows = tc_form ? 64 : 16;
+  const int64_t ovf_cap = n * ovf_rows > (1 << 22) ? n * ovf_rows : (1 << 22);
   Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ovf_idx(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
   Buf<uint64_t> ovf_key(ctx, ovf_cap);
   HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));

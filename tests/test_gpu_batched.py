@@ -116,11 +116,11 @@ def _two_group_graph():
     in the first group (equal degrees, ties by index), so the second group is
     unreachable: the reference stops on it with "MST montada incorretamente"
     (mst.cu:317-323)."""
-    n, k = 100, 4
+    n, k = 100, 16
     ids = np.zeros((n, k), np.int32)
     for g0 in (0, 50):
         for i in range(50):
-            ids[g0 + i] = [g0 + (i + s) % 50 for s in (1, 2, 3, 4)]
+            ids[g0 + i] = [g0 + (i + s) % 50 for s in range(1, k + 1)]
     X = np.random.default_rng(0).normal(size=(n, 2)).astype(np.float32)
     G = np.zeros((n, k, 2), np.int32)
     G[..., 0] = np.ones((n, k), np.float32).view(np.int32)
@@ -138,10 +138,10 @@ def test_batched_disconnected_instance_fails_alone(ctx, oracle):
             G, X = _two_group_graph()
         else:
             X = blobs(n, 2, seed=40 + i, spread=2.5)
-            G = ctx.NNDescent(X, k=4, sample_num=2).cpu().numpy()
+            G = ctx.NNDescent(X, k=16, sample_num=8).cpu().numpy()
         Xs.append(X)
         Gs.append(G)
-    kw = dict(k=4, mpts=4)
+    kw = dict(k=16, mpts=8)
     with pytest.raises(g.HdbError, match="DISCONNECTED"):
         ctx.hdbscan_batched_from_knn(Gs, Xs, **kw)
     labels, ncl, st = ctx.hdbscan_batched_from_knn(Gs, Xs, strict=False, **kw)
@@ -152,9 +152,9 @@ def test_batched_disconnected_instance_fails_alone(ctx, oracle):
         if st["instance_status"][i]:
             assert (labels[i].numpy() == -1).all() and ncl[i] == 0
             with pytest.raises(RuntimeError):
-                oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 4)
+                oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 8)
             continue
-        _, ref, rnc = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 4)
+        _, ref, rnc = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 8)
         np.testing.assert_array_equal(labels[i].numpy(), ref)
         assert ncl[i] == rnc
 
