@@ -482,19 +482,6 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
     atomicOr(err, DEVERR_TIMEOUT);
 }
 
-// A candidate at position pos of the target-sorted list of the next merge;
-// past the list's capacity only the best dropped candidate per target is kept.
-__device__ __forceinline__ void append_candidate(const Inbox &ib, unsigned long long pos,
-                                                 int32_t target, uint64_t key) {
-  if ((int64_t)pos < ib.ovf_cap) {
-    ib.ovf_tgt[pos] = (uint32_t)target;
-    ib.ovf_key[pos] = key;
-  } else {
-    atomicMin(&ib.best[target], (unsigned long long)key);
-    atomicAdd(&ib.counters[0], 1ull);
-  }
-}
-
 // Row minimum over 32 columns: key = clamped distance bits with the column in
 // the low 6 bits (skip_col: the row's own column, or -1).
 __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const float *cn, float na,
@@ -584,17 +571,7 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     // warp instead of a returning inbox atomic per candidate
     const float d1 = __uint_as_float(k1 & ~63u), d2 = __uint_as_float(k2 & ~63u);
     const bool c1 = vrow && id1 >= 0 && d1 < wst, c2 = vrow && id2 >= 0 && d2 < wst;
-    const uint32_t b1 = __ballot_sync(0xffffffffu, c1), b2 = __ballot_sync(0xffffffffu, c2);
-    const uint32_t tot = __popc(b1) + __popc(b2);
-    if (tot) {
-      unsigned long long base = 0;
-      if (lane == 0) base = atomicAdd(&a.ib.counters[3], (unsigned long long)tot);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (c1) append_candidate(a.ib, base + __popc(b1 & lanemask_lt()), myid, pack(d1, id1));
-      if (c2)
-        append_candidate(a.ib, base + __popc(b1) + __popc(b2 & lanemask_lt()), myid, pack(d2, id2));
-      cands += (c1 ? 1 : 0) + (c2 ? 1 : 0);
-    }
+    cands += append_candidates(a.ib, c1, myid, pack(d1, id1), c2, myid, pack(d2, id2), false, 0, 0);
   }
 }
 

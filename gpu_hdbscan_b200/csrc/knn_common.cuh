@@ -37,6 +37,45 @@ struct Inbox {
   int64_t ovf_cap;
 };
 
+// Appends this lane's candidates (up to three: target row, packed key; the
+// caller has checked each against its target's worst[]) to the list that is
+// sorted by target before the next merge -- one reservation per warp, no
+// returning atomic per candidate.  Past the list's capacity only the best
+// dropped candidate of each target is kept.  Returns the lane's count.
+__device__ __forceinline__ int append_candidates(const Inbox &ib, bool v0, int32_t t0, uint64_t k0,
+                                                 bool v1, int32_t t1, uint64_t k1, bool v2,
+                                                 int32_t t2, uint64_t k2) {
+  const int lane = threadIdx.x & 31;
+  uint32_t lt;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+  const uint32_t b0 = __ballot_sync(0xffffffffu, v0), b1 = __ballot_sync(0xffffffffu, v1),
+                 b2 = __ballot_sync(0xffffffffu, v2);
+  const uint32_t tot = __popc(b0) + __popc(b1) + __popc(b2);
+  if (tot == 0) return 0;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(&ib.counters[3], (unsigned long long)tot);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const unsigned long long p0 = base + __popc(b0 & lt);
+  const unsigned long long p1 = base + __popc(b0) + __popc(b1 & lt);
+  const unsigned long long p2 = base + __popc(b0) + __popc(b1) + __popc(b2 & lt);
+  const int32_t tt[3] = {t0, t1, t2};
+  const uint64_t kk[3] = {k0, k1, k2};
+  const unsigned long long pp[3] = {p0, p1, p2};
+  const bool vv[3] = {v0, v1, v2};
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    if (!vv[q]) continue;
+    if ((int64_t)pp[q] < ib.ovf_cap) {
+      ib.ovf_tgt[pp[q]] = (uint32_t)tt[q];
+      ib.ovf_key[pp[q]] = kk[q];
+    } else {
+      atomicMin(&ib.best[tt[q]], (unsigned long long)kk[q]);
+      atomicAdd(&ib.counters[0], 1ull);
+    }
+  }
+  return (v0 ? 1 : 0) + (v1 ? 1 : 0) + (v2 ? 1 : 0);
+}
+
 __device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
                                               const float *__restrict__ worst, const Inbox &ib) {
   if (!(d < worst[target])) return 0;  // cannot enter the target's list
