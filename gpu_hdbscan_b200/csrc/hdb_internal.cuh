@@ -171,6 +171,10 @@ void radix_sort_u32(Context *ctx, uint32_t *keys, uint32_t *values, int64_t n, i
                     int end_bit);
 void radix_sort_u64(Context *ctx, uint64_t *keys, uint32_t *values, int64_t n, int begin_bit,
                     int end_bit);
+// The same with u64 values and digits of up to 9 bits (fewer passes for key
+// ranges just above a multiple of 8 bits, e.g. 25-bit row ids: 3 passes).
+void radix_sort_u32_u64(Context *ctx, uint32_t *keys, uint64_t *values, int64_t n, int begin_bit,
+                        int end_bit);
 
 void radix_sort_u32_buffers(cudaStream_t st, uint32_t *keys, uint32_t *vals, uint32_t *ktmp,
                             uint32_t *vtmp, uint32_t *counts, uint32_t *offs, uint32_t *scan_sums,

@@ -280,8 +280,7 @@ __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, floa
     if (32 * q < cnt) merge_chunk(k, rkey, lab, c[q], sk, sl);
   if (ov != ~0ull) insert_chunk(k, rkey, lab, lane == 0 ? ov : ~0ull);
   for (uint32_t base = o0; base < o1; base += 32)
-    merge_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[ib.ovf_idx[base + lane]] : ~0ull, sk,
-                sl);
+    merge_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[base + lane] : ~0ull, sk, sl);
   if (have) dist = pk_dist(rkey);
 }
 
@@ -847,12 +846,6 @@ __global__ void k_fix_distances(const float *__restrict__ X, int64_t n, int d,
   }
 }
 
-__global__ void k_iota_u32(uint32_t *__restrict__ v, int64_t n) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    v[i] = (uint32_t)i;
-}
-
 // Segment [ostart, oend) of every target row in the target-sorted overflow list.
 __global__ void k_ovf_bounds(const uint32_t *__restrict__ tgt, int64_t cnt, uint32_t *__restrict__ ostart,
                              uint32_t *__restrict__ oend) {
@@ -1047,9 +1040,9 @@ static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
   int64_t c = (int64_t)h[0];
   if (c == 0) return;
   if (c > ib.ovf_cap) c = ib.ovf_cap;
-  k_iota_u32<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_idx, c); ctx->launches++;
-  HDB_CHECK_LAUNCH();
-  radix_sort_u32(ctx, ib.ovf_tgt, ib.ovf_idx, c, 0, bits_for_rows(n));
+  // the packed candidates move with their targets, so the merge reads each
+  // row's segment contiguously
+  radix_sort_u32_u64(ctx, ib.ovf_tgt, ib.ovf_key, c, 0, bits_for_rows(n));
   k_ovf_bounds<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_tgt, c, ib.ostart, ib.oend); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemsetAsync(ib.counters + 3, 0, sizeof(unsigned long long), st));
@@ -1083,11 +1076,11 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
   const int64_t ovf_rows = tc_form ? 64 : 16;
   const int64_t ovf_cap = n * ovf_rows > (1 << 22) ? n * ovf_rows : (1 << 22);
-  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ovf_idx(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
+  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
   Buf<uint64_t> ovf_key(ctx, ovf_cap);
   HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
-  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ovf_idx, ostart, oend, dropped, ovf_cap};
+  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, ovf_cap};
   HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
   HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));

@@ -30,8 +30,7 @@ struct Inbox {
   uint64_t *slots;               // [n * kInboxCap] packed (distance, id)
   unsigned long long *best;      // [n]
   uint32_t *ovf_tgt;             // [ovf_cap] overflow: target row (sorted in place)
-  uint64_t *ovf_key;             // [ovf_cap] overflow: packed candidate
-  uint32_t *ovf_idx;             // [ovf_cap] overflow: permutation from the sort
+  uint64_t *ovf_key;             // [ovf_cap] overflow: packed candidate (sorted along)
   uint32_t *ostart, *oend;       // [n] segment of each row in the sorted overflow list
   unsigned long long *counters;  // [0] dropped [1] rows gathered [2] candidates [3] overflow
   int64_t ovf_cap;

@@ -120,86 +120,136 @@ void scan_impl(Context *ctx, const In *in, Out *out, int64_t n, Out *total) {
 }
 
 // ---------------------------------------------------------------------------
-// Stable LSD radix sort, 8-bit digits, tiles of 2048 keys.
+// Stable LSD radix sort.  One tile of kSortThreads * kItems keys per block;
+// each pass sorts by (key >> shift) & mask, digits of up to 8 bits (256 bins)
+// or 9 bits (512 bins).  The per-tile digit counts are laid out either
+// digit-major ([digit][tile]: one flat exclusive scan gives every tile its
+// output positions) or tile-major ([tile][digit]: every block reads and
+// writes its own counts contiguously, and a column scan over chunks of
+// tiles gives the positions).  The sorts of this file use tile-major counts
+// and tiles of 4096 keys; the caller-buffer variant keeps the digit-major
+// layout and 2048-key tiles its buffer sizes are stated in.
 // ---------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 8;
-constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;          // tile-major sorts: 4096-key tiles
+constexpr int kSortItemsFlat = 8;       // digit-major (caller-buffer) sort: 2048-key tiles
+constexpr int kColRows = 512;           // tiles per chunk of the column scan
 
-template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_hist(const K *__restrict__ keys,
-                                                            uint32_t *__restrict__ counts,
-                                                            int64_t n, int shift,
-                                                            uint32_t nblocks) {
-  __shared__ uint32_t hist[256];
-  hist[threadIdx.x] = 0;
-  __syncthreads();
-  int64_t base = (int64_t)blockIdx.x * kSortTile;
-#pragma unroll
-  for (int i = 0; i < kSortItems; i++) {
-    int64_t idx = base + (int64_t)i * kSortThreads + threadIdx.x;
-    if (idx < n) atomicAdd(&hist[(uint32_t)(keys[idx] >> shift) & 0xffu], 1u);
-  }
-  __syncthreads();
-  counts[(int64_t)threadIdx.x * nblocks + blockIdx.x] = hist[threadIdx.x];
+// Dynamic shared memory of one scatter block: the tile's keys and values in
+// digit order, the per-warp digit counts, each digit's first tile position
+// and first output position, and the warp totals of the digit scan.
+template <typename K, typename V, bool kVals, int kBins, int kItems>
+struct SortSmem {
+  static constexpr int kTile = kSortThreads * kItems;
+  static constexpr size_t kValsAt = sizeof(K) * kTile;
+  static constexpr size_t kHistAt = kValsAt + (kVals ? sizeof(V) * kTile : 0);
+  static constexpr size_t kStartAt = kHistAt + sizeof(uint32_t) * kSortWarps * kBins;
+  static constexpr size_t kGofsAt = kStartAt + sizeof(uint32_t) * kBins;
+  static constexpr size_t kWsumAt = kGofsAt + sizeof(uint32_t) * kBins;
+  static constexpr size_t kBytes = kWsumAt + sizeof(uint32_t) * kSortWarps;
+};
+
+template <bool kTileMajor>
+__device__ __forceinline__ int64_t count_at(int d, uint32_t tile, uint32_t nblocks, int bins) {
+  return kTileMajor ? (int64_t)tile * bins + d : (int64_t)d * nblocks + tile;
 }
 
-// Scatter of one 2048-key tile for one digit.  Keys are ranked per warp
-// (match_any), the tile is laid out in digit order in shared memory (stable:
-// input order within a digit), and each digit's run is then written by
-// consecutive threads to consecutive addresses.
-template <typename K, bool kVals>
-__global__ void __launch_bounds__(kSortThreads) radix_scatter(
-    const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, K *__restrict__ keys_out,
-    uint32_t *__restrict__ vals_out, const uint32_t *__restrict__ offsets, int64_t n, int shift,
-    uint32_t nblocks) {
-  __shared__ uint32_t whist[kSortWarps][256];
-  __shared__ uint32_t dstart[256];  // first tile position of each digit
-  __shared__ uint32_t gofs[256];    // global position of the tile's first key of each digit
-  __shared__ uint32_t wsum[kSortWarps];
-  __shared__ K tk[kSortTile];
-  __shared__ uint32_t tv[kVals ? kSortTile : 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&whist[0][0])[i] = 0;
+template <typename K, int kBins, int kItems, bool kTileMajor>
+__global__ void __launch_bounds__(kSortThreads) radix_hist(const K *__restrict__ keys,
+                                                            uint32_t *__restrict__ counts,
+                                                            int64_t n, int shift, uint32_t mask,
+                                                            uint32_t nblocks) {
+  constexpr int kTile = kSortThreads * kItems;
+  __shared__ uint32_t hist[kBins];
+  for (int i = threadIdx.x; i < kBins; i += kSortThreads) hist[i] = 0;
   __syncthreads();
-  const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
-  const int64_t base = tile0 + (int64_t)warp * (32 * kSortItems);
-  K k[kSortItems];
-  uint32_t v[kSortItems];
-  uint32_t local[kSortItems];
-  uint32_t dig[kSortItems];
+  const int64_t base = (int64_t)blockIdx.x * kTile;
+  K k[kItems];
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
-    int64_t idx = base + j * 32 + lane;
-    bool ok = idx < n;
-    k[j] = ok ? keys_in[idx] : K(0);
-    if (kVals) v[j] = ok ? vals_in[idx] : 0u;
-    uint32_t d = ok ? ((uint32_t)(k[j] >> shift) & 0xffu) : (256u + lane);
-    dig[j] = d;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    uint32_t rank = __popc(peers & lanemask_lt());
-    int leader = __ffs(peers) - 1;
+  for (int i = 0; i < kItems; i++) {
+    const int64_t idx = base + (int64_t)i * kSortThreads + threadIdx.x;
+    k[i] = idx < n ? keys[idx] : K(0);
+  }
+#pragma unroll
+  for (int i = 0; i < kItems; i++) {
+    const int64_t idx = base + (int64_t)i * kSortThreads + threadIdx.x;
+    if (idx < n) atomicAdd(&hist[(uint32_t)(k[i] >> shift) & mask], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kBins; i += kSortThreads)
+    counts[count_at<kTileMajor>(i, blockIdx.x, nblocks, kBins)] = hist[i];
+}
+
+// Scatter of one tile for one digit.  Keys are ranked per warp (match_any),
+// the tile is laid out in digit order in shared memory (stable: input order
+// within a digit), and each digit's run is then written by consecutive
+// threads to consecutive addresses.  Values of type V (u32 or u64) move with
+// their keys when kVals.
+template <typename K, typename V, bool kVals, int kBins, int kItems, bool kTileMajor>
+__global__ void __launch_bounds__(kSortThreads) radix_scatter(
+    const K *__restrict__ keys_in, const V *__restrict__ vals_in, K *__restrict__ keys_out,
+    V *__restrict__ vals_out, const uint32_t *__restrict__ offsets, int64_t n, int shift,
+    uint32_t mask, uint32_t nblocks) {
+  using L = SortSmem<K, V, kVals, kBins, kItems>;
+  constexpr int kTile = L::kTile;
+  constexpr int kPer = kBins / kSortThreads;  // digits owned by each thread in the scan
+  extern __shared__ __align__(16) unsigned char sort_smem[];
+  K *tk = reinterpret_cast<K *>(sort_smem);
+  V *tv = reinterpret_cast<V *>(sort_smem + L::kValsAt);
+  uint32_t(*whist)[kBins] = reinterpret_cast<uint32_t(*)[kBins]>(sort_smem + L::kHistAt);
+  uint32_t *dstart = reinterpret_cast<uint32_t *>(sort_smem + L::kStartAt);
+  uint32_t *gofs = reinterpret_cast<uint32_t *>(sort_smem + L::kGofsAt);
+  uint32_t *wsum = reinterpret_cast<uint32_t *>(sort_smem + L::kWsumAt);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&whist[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t tile0 = (int64_t)blockIdx.x * kTile;
+  const int64_t base = tile0 + (int64_t)warp * (32 * kItems);
+  K k[kItems];
+  V v[kItems];
+  uint32_t dl[kItems];  // digit (low 16 bits) | rank among the warp's keys of that digit << 16
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const int64_t idx = base + j * 32 + lane;
+    k[j] = idx < n ? keys_in[idx] : K(0);
+    if (kVals) v[j] = idx < n ? vals_in[idx] : V(0);
+  }
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const bool ok = base + j * 32 + lane < n;
+    // past the end: a digit of its own per lane, outside [0, kBins)
+    const uint32_t d = ok ? ((uint32_t)(k[j] >> shift) & mask) : ((uint32_t)kBins + lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & lanemask_lt());
+    const int leader = __ffs(peers) - 1;
     uint32_t b = 0;
     if (ok) b = whist[warp][d];
     __syncwarp();
     if (ok && lane == leader) whist[warp][d] = b + __popc(peers);
     __syncwarp();
-    local[j] = b + rank;
+    dl[j] = d | ((b + rank) << 16);
   }
   __syncthreads();
   {
-    // one digit per thread: warp prefixes, then the digit's count in the tile
-    const uint32_t d = threadIdx.x;
-    uint32_t run = 0;
+    // kPer consecutive digits per thread: warp prefixes, then the digits'
+    // counts in the tile, then an exclusive scan of the thread totals
+    uint32_t run[kPer];
+    uint32_t tsum = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-      const uint32_t c = whist[w][d];
-      whist[w][d] = run;
-      run += c;
+    for (int r = 0; r < kPer; r++) {
+      const int d = threadIdx.x * kPer + r;
+      uint32_t acc = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; w++) {
+        const uint32_t c = whist[w][d];
+        whist[w][d] = acc;
+        acc += c;
+      }
+      run[r] = acc;
+      tsum += acc;
     }
-    // exclusive scan of the 256 digit counts over the block
-    uint32_t x = run;
+    uint32_t x = tsum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -207,28 +257,34 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(
     }
     if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    uint32_t wpre = 0;
-    for (int w = 0; w < warp; w++) wpre += wsum[w];
-    dstart[d] = wpre + x - run;
-    gofs[d] = offsets[(int64_t)d * nblocks + blockIdx.x];
+    uint32_t excl = x - tsum;
+    for (int w = 0; w < warp; w++) excl += wsum[w];
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const int d = threadIdx.x * kPer + r;
+      dstart[d] = excl;
+      excl += run[r];
+      gofs[d] = offsets[count_at<kTileMajor>(d, blockIdx.x, nblocks, kBins)];
+    }
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
-    if (dig[j] < 256u) {
-      const uint32_t pos = dstart[dig[j]] + whist[warp][dig[j]] + local[j];
+  for (int j = 0; j < kItems; j++) {
+    const uint32_t d = dl[j] & 0xffffu;
+    if (d < (uint32_t)kBins) {
+      const uint32_t pos = dstart[d] + whist[warp][d] + (dl[j] >> 16);
       tk[pos] = k[j];
       if (kVals) tv[pos] = v[j];
     }
   }
   __syncthreads();
-  const int64_t valid = n - tile0 < kSortTile ? n - tile0 : kSortTile;
+  const int64_t valid = n - tile0 < kTile ? n - tile0 : kTile;
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
+  for (int j = 0; j < kItems; j++) {
     const int i = j * kSortThreads + threadIdx.x;
     if (i < valid) {
       const K key = tk[i];
-      const uint32_t d = (uint32_t)(key >> shift) & 0xffu;
+      const uint32_t d = (uint32_t)(key >> shift) & mask;
       const uint32_t pos = gofs[d] + (uint32_t)i - dstart[d];
       keys_out[pos] = key;
       if (kVals) vals_out[pos] = tv[i];
@@ -236,39 +292,126 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(
   }
 }
 
-template <typename K>
-void radix_sort_impl(Context *ctx, K *keys, uint32_t *vals, int64_t n, int begin_bit,
-                     int end_bit) {
+// Column scan of tile-major counts [nblocks][kBins], one thread per digit.
+// (1) per chunk of kColRows tiles, each digit's count in the chunk;
+template <int kBins>
+__global__ void __launch_bounds__(kBins) radix_col_sums(const uint32_t *__restrict__ counts,
+                                                        uint32_t *__restrict__ csum,
+                                                        uint32_t nblocks) {
+  const int d = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * kColRows;
+  const int64_t r1 = r0 + kColRows < (int64_t)nblocks ? r0 + kColRows : (int64_t)nblocks;
+  uint32_t s = 0;
+#pragma unroll 8
+  for (int64_t r = r0; r < r1; r++) s += counts[r * kBins + d];
+  csum[(int64_t)blockIdx.x * kBins + d] = s;
+}
+
+// (2) one block: each digit's exclusive prefix over the chunks (in place) and
+// its first output position (base: exclusive scan of the digit totals);
+template <int kBins>
+__global__ void __launch_bounds__(kBins) radix_col_scan(uint32_t *__restrict__ csum,
+                                                        uint32_t *__restrict__ base,
+                                                        uint32_t nchunks) {
+  __shared__ uint32_t warp_sums[32];
+  const int d = threadIdx.x;
+  uint32_t run = 0;
+  for (uint32_t c0 = 0; c0 < nchunks; c0 += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      v[j] = c0 + j < nchunks ? csum[(int64_t)(c0 + j) * kBins + d] : 0u;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      if (c0 + j < nchunks) csum[(int64_t)(c0 + j) * kBins + d] = run;
+      run += v[j];
+    }
+  }
+  uint32_t total;
+  base[d] = block_exclusive_scan<uint32_t>(run, &total, warp_sums);
+}
+
+// (3) every tile's output position of its first key of each digit.
+template <int kBins>
+__global__ void __launch_bounds__(kBins) radix_col_apply(const uint32_t *__restrict__ counts,
+                                                         const uint32_t *__restrict__ csum,
+                                                         const uint32_t *__restrict__ base,
+                                                         uint32_t *__restrict__ offs,
+                                                         uint32_t nblocks) {
+  const int d = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * kColRows;
+  const int64_t r1 = r0 + kColRows < (int64_t)nblocks ? r0 + kColRows : (int64_t)nblocks;
+  uint32_t run = base[d] + csum[(int64_t)blockIdx.x * kBins + d];
+#pragma unroll 8
+  for (int64_t r = r0; r < r1; r++) {
+    const uint32_t c = counts[r * kBins + d];
+    offs[r * kBins + d] = run;
+    run += c;
+  }
+}
+
+template <typename K, typename V, bool kVals, int kBins, int kItems, bool kTileMajor>
+void launch_scatter(cudaStream_t st, const K *kin, const V *vin, K *kout, V *vout,
+                    const uint32_t *offs, int64_t n, int shift, uint32_t mask, uint32_t nb) {
+  using L = SortSmem<K, V, kVals, kBins, kItems>;
+  auto *fn = radix_scatter<K, V, kVals, kBins, kItems, kTileMajor>;
+  if (L::kBytes > 48 * 1024)
+    HDB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kBytes));
+  fn<<<nb, kSortThreads, L::kBytes, st>>>(kin, vin, kout, vout, offs, n, shift, mask, nb);
+  HDB_CHECK_LAUNCH();
+}
+
+// Digit widths: the fewest passes of at most log2(kBins) bits over
+// [begin_bit, end_bit), the bits spread evenly over them (25 bits with 512
+// bins: 9 + 8 + 8).
+template <typename K, typename V, int kBins>
+void radix_sort_impl(Context *ctx, K *keys, V *vals, int64_t n, int begin_bit, int end_bit) {
   if (n <= 1 || end_bit <= begin_bit) return;
   HDB_REQUIRE(n < (int64_t(1) << 32), HDB_ERR_ARG, "radix sort: more than 2^32 elements");
-  uint32_t nb = (uint32_t)ceil_div(n, kSortTile);
+  constexpr int kMaxBits = kBins == 512 ? 9 : 8;
+  static_assert(kBins == 256 || kBins == 512, "radix sort: 256 or 512 bins");
+  constexpr int kTile = kSortThreads * kSortItems;
+  const cudaStream_t st = ctx->stream;
+  const uint32_t nb = (uint32_t)ceil_div(n, kTile);
+  const uint32_t nchunks = (uint32_t)ceil_div(nb, kColRows);
   Buf<K> ktmp(ctx, n);
-  Buf<uint32_t> vtmp;
-  if (vals) vtmp = Buf<uint32_t>(ctx, n);
-  Buf<uint32_t> counts(ctx, (size_t)nb * 256), offs(ctx, (size_t)nb * 256);
+  Buf<V> vtmp;
+  if (vals) vtmp = Buf<V>(ctx, n);
+  Buf<uint32_t> counts(ctx, (size_t)nb * kBins), offs(ctx, (size_t)nb * kBins),
+      csum(ctx, (size_t)nchunks * kBins), base(ctx, kBins);
   K *kin = keys, *kout = ktmp;
-  uint32_t *vin = vals, *vout = vals ? vtmp.get() : nullptr;
+  V *vin = vals, *vout = vals ? vtmp.get() : nullptr;
   int passes = 0;
-  for (int shift = begin_bit; shift < end_bit; shift += 8, passes++) {
-    radix_hist<K><<<nb, kSortThreads, 0, ctx->stream>>>(kin, counts, n, shift, nb); ctx->launches++;
+  int left = end_bit - begin_bit;
+  int npass = (left + kMaxBits - 1) / kMaxBits;
+  for (int shift = begin_bit; left > 0; passes++, npass--) {
+    const int bits = (left + npass - 1) / npass;
+    const uint32_t mask = (1u << bits) - 1u;
+    radix_hist<K, kBins, kSortItems, true><<<nb, kSortThreads, 0, st>>>(kin, counts, n, shift,
+                                                                       mask, nb);
     HDB_CHECK_LAUNCH();
-    scan_exclusive_u32_u32(ctx, counts, offs, (int64_t)nb * 256, nullptr);
+    radix_col_sums<kBins><<<nchunks, kBins, 0, st>>>(counts, csum, nb);
+    HDB_CHECK_LAUNCH();
+    radix_col_scan<kBins><<<1, kBins, 0, st>>>(csum, base, nchunks);
+    HDB_CHECK_LAUNCH();
+    radix_col_apply<kBins><<<nchunks, kBins, 0, st>>>(counts, csum, base, offs, nb);
+    HDB_CHECK_LAUNCH();
     if (vals)
-      radix_scatter<K, true><<<nb, kSortThreads, 0, ctx->stream>>>(kin, vin, kout, vout, offs, n,
-                                                                   shift, nb);
+      launch_scatter<K, V, true, kBins, kSortItems, true>(st, kin, vin, kout, vout, offs, n, shift,
+                                                          mask, nb);
     else
-      radix_scatter<K, false><<<nb, kSortThreads, 0, ctx->stream>>>(kin, nullptr, kout, nullptr,
-                                                                    offs, n, shift, nb);
-    ctx->launches++;
-    HDB_CHECK_LAUNCH();
+      launch_scatter<K, V, false, kBins, kSortItems, true>(st, kin, nullptr, kout, nullptr, offs,
+                                                           n, shift, mask, nb);
+    ctx->launches += 5;
     K *t = kin; kin = kout; kout = t;
-    uint32_t *tv = vin; vin = vout; vout = tv;
+    V *tv = vin; vin = vout; vout = tv;
+    shift += bits;
+    left -= bits;
   }
   if (passes & 1) {
-    HDB_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+    HDB_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(K), cudaMemcpyDeviceToDevice, st));
     if (vals)
-      HDB_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                               ctx->stream));
+      HDB_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(V), cudaMemcpyDeviceToDevice, st));
   }
 }
 
@@ -286,13 +429,26 @@ void scan_exclusive_u32_u32(Context *ctx, const uint32_t *in, uint32_t *out, int
                             uint32_t *total) {
   scan_impl<uint32_t, uint32_t>(ctx, in, out, n, total);
 }
+// 9-bit digits when they save a pass over 8-bit ones (e.g. 25-bit row ids).
+static bool nine_bit_digits_help(int bits) { return (bits + 8) / 9 < (bits + 7) / 8; }
+
 void radix_sort_u32(Context *ctx, uint32_t *keys, uint32_t *values, int64_t n, int begin_bit,
                     int end_bit) {
-  radix_sort_impl<uint32_t>(ctx, keys, values, n, begin_bit, end_bit);
+  if (nine_bit_digits_help(end_bit - begin_bit))
+    radix_sort_impl<uint32_t, uint32_t, 512>(ctx, keys, values, n, begin_bit, end_bit);
+  else
+    radix_sort_impl<uint32_t, uint32_t, 256>(ctx, keys, values, n, begin_bit, end_bit);
 }
 void radix_sort_u64(Context *ctx, uint64_t *keys, uint32_t *values, int64_t n, int begin_bit,
                     int end_bit) {
-  radix_sort_impl<uint64_t>(ctx, keys, values, n, begin_bit, end_bit);
+  if (nine_bit_digits_help(end_bit - begin_bit))
+    radix_sort_impl<uint64_t, uint32_t, 512>(ctx, keys, values, n, begin_bit, end_bit);
+  else
+    radix_sort_impl<uint64_t, uint32_t, 256>(ctx, keys, values, n, begin_bit, end_bit);
+}
+void radix_sort_u32_u64(Context *ctx, uint32_t *keys, uint64_t *values, int64_t n, int begin_bit,
+                        int end_bit) {
+  radix_sort_impl<uint32_t, uint64_t, 512>(ctx, keys, values, n, begin_bit, end_bit);
 }
 
 // Stable LSD radix sort of u32 keys with u32 values in caller-provided
@@ -304,14 +460,15 @@ void radix_sort_u32_buffers(cudaStream_t st, uint32_t *keys, uint32_t *vals, uin
                             uint32_t *vtmp, uint32_t *counts, uint32_t *offs, uint32_t *scan_sums,
                             uint32_t *scan_offs, int64_t n, int begin_bit, int end_bit) {
   if (n <= 1 || end_bit <= begin_bit) return;
-  const uint32_t nb = (uint32_t)ceil_div(n, kSortTile);
+  const uint32_t nb = (uint32_t)ceil_div(n, kSortThreads * kSortItemsFlat);
   const int64_t nc = (int64_t)nb * 256;
   const int64_t ns = ceil_div(nc, kScanTile);
   HDB_REQUIRE(ns <= kScanTile, HDB_ERR_ARG, "radix sort buffers: too many elements");
   uint32_t *kin = keys, *kout = ktmp, *vin = vals, *vout = vtmp;
   int passes = 0;
   for (int shift = begin_bit; shift < end_bit; shift += 8, passes++) {
-    radix_hist<uint32_t><<<nb, kSortThreads, 0, st>>>(kin, counts, n, shift, nb);
+    radix_hist<uint32_t, 256, kSortItemsFlat, false><<<nb, kSortThreads, 0, st>>>(kin, counts, n,
+                                                                                 shift, 0xffu, nb);
     HDB_CHECK_LAUNCH();
     if (ns == 1) {
       scan_tile_apply<uint32_t, uint32_t><<<1, kScanThreads, 0, st>>>(counts, offs, nullptr, nc,
@@ -326,9 +483,8 @@ void radix_sort_u32_buffers(cudaStream_t st, uint32_t *keys, uint32_t *vals, uin
                                                                                  nullptr);
     }
     HDB_CHECK_LAUNCH();
-    radix_scatter<uint32_t, true><<<nb, kSortThreads, 0, st>>>(kin, vin, kout, vout, offs, n,
-                                                               shift, nb);
-    HDB_CHECK_LAUNCH();
+    launch_scatter<uint32_t, uint32_t, true, 256, kSortItemsFlat, false>(st, kin, vin, kout, vout,
+                                                                         offs, n, shift, 0xffu, nb);
     uint32_t *t = kin; kin = kout; kout = t;
     t = vin; vin = vout; vout = t;
   }

@@ -44,6 +44,33 @@ def test_nndescent_recall_matches_reference_algorithm(ctx, oracle, n, d, k):
     assert r_gpu >= r_orc - 0.005, (r_gpu, r_orc)
 
 
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_row_ids_of_18_bits(ctx, oracle, prec):
+    """200,000 points: row ids need 18 bits, so the target sort of the
+    candidate list and the row sorts of the graph stages take two 9-bit
+    digit passes (every one of the 512 bins in use).  The graph is still a
+    valid, exactly ranked kNN graph and the labels from it equal the
+    oracle's on the same graph."""
+    from gpu_hdbscan_b200 import HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP32
+    n, d, k = 200_000, 8, 16
+    X = blobs(n, d, seed=41, blobs=12)
+    pc = HDB_PREC_BF16 if prec == "bf16" else HDB_PREC_FP32
+    G = ctx.NNDescent(X, k=k, sample_num=8, iterations=6, precision=pc)
+    ids, dist = (_t(a) for a in ctx.knn_split(G))
+    assert oracle.validate_knn(ids)
+    key = dist.view(np.uint32).astype(np.uint64) << np.uint64(32) | ids.astype(np.uint64)
+    assert (np.diff(key, axis=1) > 0).all()
+    rng = np.random.default_rng(1)
+    for i in rng.choice(n, 100, replace=False):
+        for j in range(k):
+            ref = oracle.diffsum(X[i], X[ids[i, j]])
+            assert np.float32(ref).view(np.uint32) == dist[i, j].view(np.uint32)
+    labels, stats = ctx.hdbscan_from_knn(G, X, k=k, mpts=k, distance=HDB_DIST_SQUARED)
+    _, ref_labels, ncl = oracle.hdbscan_from_knn(ids, dist, X, k)
+    np.testing.assert_array_equal(_t(labels), ref_labels)
+    assert stats["num_clusters"] == ncl
+
+
 @pytest.mark.parametrize("distance", ["sqrt", "squared"])
 @pytest.mark.parametrize("stab", ["fp32", "fp64"])
 def test_pipeline_labels_identical_on_shared_graph(ctx, oracle, distance, stab):
