@@ -92,6 +92,28 @@ class Context:
         _lib.check(self.L.hdb_nndescent(self.h, _ptr(X), n, d, C.byref(p), _ptr(G)))
         return G
 
+    def KNNMerge(self, X1, G1, X2, G2, sample_num=12, iterations=11):
+        """gpuknn::KNNMerge (knnmerge.cuh:8-12; KNNMergeFromHost :14-18 when the
+        inputs are host arrays): X1 [n1, d], X2 [n2, d] float32 and their kNN
+        graphs G1 [n1, k, 2], G2 [n2, k, 2] (NNDElement rows, ids local to their
+        set) -> G [n1 + n2, k, 2] on the device, the rows of X1 first and the ids
+        of X2 shifted by n1.  Defaults are MERGE_SAMPLE_NUM and MERGE_ITERATION."""
+        torch = self._torch
+        X1 = self._dev(X1, torch.float32)
+        X2 = self._dev(X2, torch.float32)
+        G1 = self._dev(G1, torch.int32)
+        G2 = self._dev(G2, torch.int32)
+        n1, d = X1.shape
+        n2 = X2.shape[0]
+        k = G1.shape[1]
+        if X2.shape[1] != d or G2.shape[1] != k or G1.shape[0] != n1 or G2.shape[0] != n2:
+            raise ValueError("KNNMerge: X1/X2 need the same d and G1/G2 the same k, one row per point")
+        G = torch.empty((n1 + n2, k, 2), dtype=torch.int32, device=self.device)
+        p = _lib.KnnParams(k, sample_num, iterations, HDB_PREC_FP32)
+        _lib.check(self.L.hdb_knn_merge(self.h, _ptr(X1), n1, _ptr(G1), _ptr(X2), n2, _ptr(G2), d,
+                                        C.byref(p), _ptr(G)))
+        return G
+
     def knn_split(self, G):
         """G [n, k, 2] -> (ids int32 [n, k] with the old/new flag decoded, dist float32)."""
         torch = self._torch

@@ -25,7 +25,8 @@ EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_se
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
-           "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised")
+           "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised",
+           "hdb_knn_merge")
 
 
 class HdbError(RuntimeError):
@@ -87,6 +88,8 @@ def load(path: str = LIB_PATH):
         "hdb_destroy": (C.c_int, [_P]),
         "hdb_set_stream": (C.c_int, [_P, _P]),
         "hdb_nndescent": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(KnnParams), _P]),
+        "hdb_knn_merge": (C.c_int, [_P, _P, _I64, _P, _P, _I64, _P, _I32,
+                                    C.POINTER(KnnParams), _P]),
         "hdb_knn_split": (C.c_int, [_P, _P, _I64, _I32, _P, _P]),
         "hdb_fix_distances": (C.c_int, [_P, _P, _I64, _I32, _P, _I32, _P]),
         "hdb_enhanced_knng": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, C.POINTER(Graph)]),

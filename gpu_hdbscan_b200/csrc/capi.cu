@@ -54,6 +54,22 @@ HDB_API hdb_status hdb_nndescent(hdb_ctx *h, const float *X, int64_t n, int32_t 
   });
 }
 
+HDB_API hdb_status hdb_knn_merge(hdb_ctx *h, const float *X1, int64_t n1,
+                                 const hdb_nnd_element *G1, const float *X2, int64_t n2,
+                                 const hdb_nnd_element *G2, int32_t d,
+                                 const hdb_knn_params *params, hdb_nnd_element *G) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(X1, "X1");
+    require_ptr(X2, "X2");
+    require_ptr(G1, "G1");
+    require_ptr(G2, "G2");
+    require_ptr(G, "G");
+    check_knn_params(params);
+    knn_merge(ctx, X1, n1, G1, X2, n2, G2, d, *params, G, nullptr);
+  });
+}
+
 HDB_API hdb_status hdb_knn_split(hdb_ctx *h, const hdb_nnd_element *G, int64_t n, int32_t k,
                                  int32_t *ids, float *dist) {
   return guard([&] {

@@ -156,6 +156,84 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Seg
   }
 }
 
+// Initial graph of the merge of two point sets A = [0, n1) and B = [n1, n)
+// (InitRandomBlockedKNNGraph, knnmerge.cu:80-185, then the distance pass and
+// per-row sort of InitRandomKNNGraph nndescent.cu:1800-1871 that
+// NNDescentForMerge :2013 runs on it), one warp per row: the first k - k/2
+// entries of the row's own subgraph row (ids shifted into the merged
+// numbering, flagged old as after MarkAllToOld), then k/2 ids of the other
+// set drawn as xorshift64star(local row * (k/2) + t) % |other set|, flagged
+// new.  An id drawn twice is advanced to the next free one (the reference
+// keeps repeats), and every distance is the sequential FP32 difference sum of
+// the join (the reference's distance pass sums over a warp tree).  The rows
+// are sorted by (distance, id); an entry's flag follows from its set: ids of
+// the other set are the new ones.  Own-subgraph ids outside their set, self
+// ids and repeats set DEVERR_ID_RANGE / SELF / DUP and are replaced by a
+// valid id of the set so that no gather leaves X.
+__global__ void k_merge_init(const float *__restrict__ X, int64_t n, int d, int k, int64_t n1,
+                             const hdb_nnd_element *__restrict__ G1,
+                             const hdb_nnd_element *__restrict__ G2, int32_t *__restrict__ gid,
+                             float *__restrict__ gdist, float *__restrict__ worst,
+                             uint32_t *__restrict__ err) {
+  extern __shared__ float smem_stage[];
+  const int lane = lane_id();
+  const int wpb = blockDim.x >> 5;
+  float *sm = smem_stage + (threadIdx.x >> 5) * kStageFloats;
+  const int h = k - k / 2, r = k / 2;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
+       row += (int64_t)gridDim.x * wpb) {
+    const bool inb = row >= n1;
+    const int64_t local = inb ? row - n1 : row;
+    const int64_t own_n = inb ? n - n1 : n1, own_off = inb ? n1 : 0;
+    const int64_t oth_n = inb ? n1 : n - n1, oth_off = inb ? 0 : n1;
+    const hdb_nnd_element *own = inb ? G2 : G1;
+    int64_t label = 0;
+    uint32_t bad = 0;
+    if (lane < h) {
+      label = decode(own[local * k + lane].label_);
+      if (label < 0 || label >= own_n) {
+        bad |= DEVERR_ID_RANGE;
+        label = (local + 1 + lane) % own_n;
+      } else if (label == local) {
+        bad |= DEVERR_SELF_ID;
+        label = (local + 1 + lane) % own_n;
+      }
+    } else if (lane < k) {
+      label = (int64_t)(xorshift64star((uint64_t)(local * r + (lane - h))) % (uint64_t)oth_n);
+    }
+    // repeats among the own entries (input error) and among the drawn ones
+    const uint32_t same = __match_any_sync(0xffffffffu, lane < h ? label : -1 - (int64_t)lane);
+    if (lane < h && (__ffs(same) - 1) != lane) bad |= DEVERR_DUP_ID;
+    for (int t = 0; t < r; t++) {
+      while (true) {
+        const int64_t c = __shfl_sync(0xffffffffu, label, h + t);
+        const bool dup = lane >= h && lane < h + t && label == c;
+        if (__ballot_sync(0xffffffffu, dup) == 0) break;
+        if (lane == h + t) label = (label + 1) % oth_n;
+      }
+    }
+    const uint32_t anybad = __reduce_or_sync(0xffffffffu, bad);
+    if (anybad && lane == 0) atomicOr(err, anybad);
+    if (anybad & DEVERR_DUP_ID) {
+      // keep the rows valid: the own half becomes the next h ids of its set
+      if (lane < h) label = (local + 1 + lane) % own_n;
+    }
+    label += lane < h ? own_off : oth_off;
+    const float ds = diffsum_staged(X, d, row, (int32_t)label, lane < k, sm);
+    uint64_t key = ~0ull;
+    if (lane < k) key = pack(ds, (int32_t)label);
+    key = warp_sort32(key);
+    if (lane < k) {
+      const int32_t id = pk_id(key);
+      const bool isnew = (id >= n1) != inb;
+      gid[row * k + lane] = isnew ? id : -id - 1;
+      gdist[row * k + lane] = pk_dist(key);
+    }
+    const float w = __shfl_sync(0xffffffffu, pk_dist(key), k - 1);
+    if (lane == 0) worst[row] = w;
+  }
+}
+
 // Offers a chunk of up to 32 candidates (one per lane, ~0 for none) to the
 // row held one sorted entry per lane (lane < k; key = (distance, id)).  Only
 // candidates below the row's current k-th key can enter, and the k-th key
@@ -286,11 +364,14 @@ __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, floa
 
 // Merge (iterations >= 1), sample (PrepareGraph :44-98 and reverse samples
 // PrepareReverseGraph :293-346) and MarkAllToOld (:1398), one warp per row.
+// split > 0 is the merge of two point sets [0, split) and [split, n)
+// (PrepareGraphForMerge :100-166): old entries are sampled only from the
+// row's own set; new entries and reverse samples are not filtered.
 __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restrict__ gid,
                          float *__restrict__ gdist, float *__restrict__ worst, Inbox ib,
                          int32_t *__restrict__ newS,
                          int32_t *__restrict__ oldS, int8_t *__restrict__ nf, int8_t *__restrict__ of,
-                         int32_t *__restrict__ nrev, int32_t *__restrict__ orev) {
+                         int32_t *__restrict__ nrev, int32_t *__restrict__ orev, int64_t split) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
   __shared__ uint64_t merge_keys[8][32];  // per-warp merge scratch (8 warps per block)
@@ -303,9 +384,9 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
     if (do_merge) merge_row(row, k, lab, dist, ib, sk, sl);
-    const bool isnew = have && lab >= 0;
-    const bool isold = have && lab < 0;
     const int32_t id = decode(lab);
+    const bool isnew = have && lab >= 0;
+    const bool isold = have && lab < 0 && (split <= 0 || ((row < split) == (id < split)));
     uint32_t nm = __ballot_sync(0xffffffffu, isnew), om = __ballot_sync(0xffffffffu, isold);
     int rn = __popc(nm & lanemask_lt()), ro = __popc(om & lanemask_lt());
     const int64_t sb = row * (2 * S);
@@ -373,7 +454,10 @@ struct JoinSmem {
 // reference's sequential FP32 difference sum.  Tile row/column minima go to
 // the per-neighbour best candidates with one 64-bit shared-memory atomicMin
 // each: every new neighbour gets its closest other new one and its closest old
-// one, every old neighbour its closest new one.
+// one, every old neighbour its closest new one.  cross_only (the merge join,
+// TiledNewOldNeighborsCompareKernelForMerge :1328-1383 launched without the
+// new x new kernel, UpdateGraphForMerge :1582-1640) leaves out the new x new
+// tiles: new neighbours get their closest old one only.
 __device__ __forceinline__ const float *xs_row(const float *Xs, int r, int dp) {
   return Xs + r * dp + (r >= 32 ? 1 : 0);  // old block shifted one bank
 }
@@ -382,7 +466,7 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
                        const int32_t *__restrict__ newS, const int32_t *__restrict__ oldS,
                        const int8_t *__restrict__ nf, const int8_t *__restrict__ of,
                        int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
-                       const float *__restrict__ worst, Inbox ib) {
+                       const float *__restrict__ worst, Inbox ib, int cross_only) {
   extern __shared__ float smem_join[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
@@ -428,7 +512,7 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     best2[lane] = ~0ull;
     best3[lane] = ~0ull;
     __syncwarp();
-    if (nn == 0 || nn + no < 2) continue;
+    if (nn == 0 || nn + no < 2 || (cross_only && no == 0)) continue;
     w_rows += nn + no;
     // stage rows
     for (int idx = lane; idx < (nn + no) * d; idx += 32) {
@@ -439,7 +523,7 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     }
     __syncwarp();
     const int rg = (nn + 3) >> 2;             // row groups (new rows)
-    const int cgn = rg, cgo = (no + 3) >> 2;  // column groups: new, old
+    const int cgn = cross_only ? 0 : rg, cgo = (no + 3) >> 2;  // column groups: new, old
     const int cg = cgn + cgo;
     const int tiles = rg * cg;
     for (int t = lane; t < tiles; t += 32) {
@@ -1169,7 +1253,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   }
   for (int it = 0; it < p.iterations; it++) {
     k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
-                                                       newS, oldS, nf, of, nrev, orev); ctx->launches++;
+                                                       newS, oldS, nf, of, nrev, orev, 0); ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it], st));
     if (use_tc) {
@@ -1180,7 +1264,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
                                                          nrev, orev, worst, ib);
       else
         k_join<<<grid_join, 32 * jw, smem_join, st>>>(Xw, n, d, S, newS, oldS, nf, of, nrev, orev,
-                                                      worst, ib);
+                                                      worst, ib, 0);
       ctx->launches++;
     }
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
@@ -1216,6 +1300,88 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     }
     for (auto &e : jev) cudaEventDestroy(e);
   }
+}
+
+void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element *G1,
+               const float *X2, int64_t n2, const hdb_nnd_element *G2, int32_t d,
+               const hdb_knn_params &p, hdb_nnd_element *G, int64_t *dropped_out) {
+  const int k = p.k, S = p.sample_num;
+  HDB_REQUIRE(k >= 1 && k <= kMaxK, HDB_ERR_ARG, "KNNMerge: k must be in [1, 32]");
+  HDB_REQUIRE(S >= 1 && 2 * S <= k, HDB_ERR_ARG,
+              "KNNMerge: MERGE_SAMPLE_NUM must satisfy 1 <= SAMPLE_NUM and 2*SAMPLE_NUM <= k");
+  HDB_REQUIRE(n1 > k && n2 > k, HDB_ERR_ARG, "KNNMerge: each point set needs more than k points");
+  const int64_t n = n1 + n2;
+  HDB_REQUIRE(n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "KNNMerge: need n1 + n2 < 2^31");
+  HDB_REQUIRE(d >= 1 && d <= 4096, HDB_ERR_ARG, "KNNMerge: d must be in [1, 4096]");
+  HDB_REQUIRE(p.iterations >= 0, HDB_ERR_ARG, "KNNMerge: negative iteration count");
+  HDB_REQUIRE(p.precision == HDB_PREC_FP32, HDB_ERR_ARG,
+              "KNNMerge: the merge join is the FP32 difference sum (precision must be FP32)");
+  cudaStream_t st = ctx->stream;
+  (void)ctx->take_dev_err();
+  // MergeVectors (knnmerge.cu:358-399): the two sets back to back
+  Buf<float> X(ctx, (size_t)n * d);
+  HDB_CUDA(cudaMemcpyAsync(X.get(), X1, (size_t)n1 * d * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  HDB_CUDA(cudaMemcpyAsync(X.get() + (size_t)n1 * d, X2, (size_t)n2 * d * sizeof(float),
+                           cudaMemcpyDeviceToDevice, st));
+  Buf<int32_t> gid(ctx, n * k);
+  Buf<float> gdist(ctx, n * k), worst(ctx, n);
+  Buf<int32_t> newS(ctx, n * 2 * S), oldS(ctx, n * 2 * S), nrev(ctx, n), orev(ctx, n),
+      inbox_cnt(ctx, n);
+  Buf<int8_t> nf(ctx, n), of(ctx, n);
+  Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
+  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
+  const int64_t ovf_cap = n * 16 > (1 << 22) ? n * 16 : (1 << 22);
+  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
+  Buf<uint64_t> ovf_key(ctx, ovf_cap);
+  HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
+  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, ovf_cap};
+  HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
+  HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
+  HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+
+  const int wpb = 8;
+  const int grid_rows = grid_for(ctx, n, wpb, 16);
+  const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  k_merge_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, n1, G1, G2, gid, gdist, worst,
+                                                        ctx->dev_err);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  ctx->sync();
+  const uint32_t e = ctx->take_dev_err();
+  HDB_REQUIRE(!(e & DEVERR_ID_RANGE), HDB_ERR_ARG, "KNNMerge: a subgraph id lies outside its set");
+  HDB_REQUIRE(!(e & DEVERR_SELF_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row lists itself");
+  HDB_REQUIRE(!(e & DEVERR_DUP_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row repeats an id");
+
+  const int dp = (d & 1) ? d : d + 1;
+  const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
+  int jw = (int)((56 * 1024) / per_warp);
+  jw = jw < 1 ? 1 : (jw > 8 ? 8 : jw);
+  const size_t smem_join = per_warp * jw;
+  HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "KNNMerge: d too large for the join tile");
+  HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
+  const int grid_join = grid_for(ctx, n, jw, 64);
+  // NNDescentForMerge (nndescent.cu:1999-2087): PrepareForUpdateForMerge +
+  // UpdateGraphForMerge per iteration
+  for (int it = 0; it < p.iterations; it++) {
+    k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib, newS, oldS,
+                                             nf, of, nrev, orev, n1);
+    ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev,
+                                                  worst, ib, 1);
+    ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    sort_overflow(ctx, ib, n);
+  }
+  k_finalize<<<grid_rows, 32 * wpb, 0, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+  ctx->sync();
+  if (dropped_out) *dropped_out = *static_cast<const int64_t *>(ctx->pinned);
 }
 
 void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,

@@ -16,6 +16,11 @@ struct JoinStats {
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr,
                const Segments &seg = Segments{});
+// Merge of the kNN graphs of two point sets into the graph of their union
+// (hdb_knn_merge): FP32 join, old samples from the row's own set only.
+void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element *G1,
+               const float *X2, int64_t n2, const hdb_nnd_element *G2, int32_t d,
+               const hdb_knn_params &p, hdb_nnd_element *G, int64_t *dropped_out);
 // BF16 tensor-core distances for explicit slot lists (hdb_bf16_distance_tiles).
 void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, const int32_t *ids,
                          const int32_t *counts, int64_t tiles, float *out);

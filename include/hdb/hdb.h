@@ -128,6 +128,24 @@ HDB_API hdb_status hdb_set_stream(hdb_ctx *ctx, void *stream);
 HDB_API hdb_status hdb_nndescent(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
                                  const hdb_knn_params *params, hdb_nnd_element *G);
 
+/* gpuknn::KNNMerge, gpuknn/knnmerge.cuh:8-12 (knnmerge.cu:401-437, with
+ * NNDescentForMerge nndescent.cu:1999-2087): the kNN graph of the union of
+ * two point sets from the graphs of each.  X1 [n1, d], X2 [n2, d] float32;
+ * G1 [n1, k], G2 [n2, k] NNDElement rows with ids local to their set (as
+ * hdb_nndescent writes them; flags ignored) -> G [n1 + n2, k]: rows of set 1,
+ * then set 2, ids of set 2 shifted by n1, sorted by ascending squared L2 with
+ * flags as hdb_nndescent.  params: k of G1 and G2, sample_num =
+ * MERGE_SAMPLE_NUM (reference 12), iterations = MERGE_ITERATION (reference
+ * 11), precision HDB_PREC_FP32 (the merge join is the FP32 difference sum).
+ * Each set needs more than k points.  A subgraph id outside its set, a self
+ * id or a repeated id in a row gives HDB_ERR_ARG.  All pointers are device
+ * memory (KNNMergeFromHost, knnmerge.cuh:14-18, is the caller's copies plus
+ * this call). */
+HDB_API hdb_status hdb_knn_merge(hdb_ctx *ctx, const float *X1, int64_t n1,
+                                 const hdb_nnd_element *G1, const float *X2, int64_t n2,
+                                 const hdb_nnd_element *G2, int32_t d,
+                                 const hdb_knn_params *params, hdb_nnd_element *G);
+
 /* The NNDElement -> (int ids, float distances) split of HDBSCAN/_new.cu:204-229. */
 HDB_API hdb_status hdb_knn_split(hdb_ctx *ctx, const hdb_nnd_element *G, int64_t n, int32_t k,
                                  int32_t *ids, float *dist);

@@ -93,30 +93,15 @@ static int cmp_i32(const void *x, const void *y) {
 
 typedef struct { int32_t target, id; float d; } orc_cand;
 
-/*
- * Sequential restatement of gpuknn::NNDescent (nndescent.cu:2088-2199):
- *   InitRandomKNNGraph (:1800-1871; ids from xorshift64star(pos) % n, :1673-1692),
- *   then `iterations` rounds of PrepareForUpdate (:624-671) + UpdateGraph
- *   (:1487-1580).  Candidate semantics follow the join kernels: every new
- *   neighbour x is offered its closest other new neighbour (:1030-1108) and its
- *   closest old neighbour, every old neighbour its closest new one
- *   (:1259-1326); InsertToGlobalGraph (:969-1028) keeps a sorted, duplicate-free
- *   list of k.  Flags: all entries become "old" before the join (MarkAllToOld
- *   :1398), inserted candidates are "new".
- * Deterministic choices where the reference races: forward samples are the
- * first S new / old entries by list position; reverse samples keep the first S
- * sources in row order; ties order by (distance, id).  The initial distance is
- * the same sequential difference sum as the join (the reference's warp-tree sum
- * at :1694-1726 rounds differently), and an initial id already present in the
- * row is advanced like a self id, so rows never hold duplicates.
- * Output ids carry no old/new flag; distances are squared L2.
- */
-int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
-                  int32_t iterations, int32_t *ids_out, float *dist_out) {
-  if (n < 2 || k < 1 || k > 1024 || S < 1 || 2 * S > k || n <= k) return ORC_ERR_ARG;
-  const int32_t NB = (k + 31) / 32;
-  orc_nb *G = (orc_nb *)malloc(sizeof(orc_nb) * n * k);
-  uint8_t *isnew = (uint8_t *)malloc((size_t)n * k);
+/* `iterations` rounds of sampling + local join + merge on G (n rows of k,
+ * sorted by (distance, id)) with its new/old flags.  split > 0 is the merge of
+ * the point sets [0, split) and [split, n) (NNDescentForMerge,
+ * nndescent.cu:1999-2087): old entries are sampled only from the row's own
+ * set (PrepareGraphForMerge :100-166) and the join compares new x old pairs
+ * only (TiledNewOldNeighborsCompareKernelForMerge :1328-1383 without the
+ * new x new kernel, UpdateGraphForMerge :1582-1640). */
+static int nnd_iterate(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
+                       int32_t iterations, int64_t split, orc_nb *G, uint8_t *isnew) {
   int32_t *newl = (int32_t *)malloc(sizeof(int32_t) * n * 2 * S);
   int32_t *oldl = (int32_t *)malloc(sizeof(int32_t) * n * 2 * S);
   int32_t *nfwd = (int32_t *)calloc(n, 4), *ofwd = (int32_t *)calloc(n, 4);
@@ -126,33 +111,12 @@ int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
   int32_t *ncand = (int32_t *)calloc(n, 4);
   int64_t *off = (int64_t *)malloc(sizeof(int64_t) * (n + 1));
   orc_cand *bucket = (orc_cand *)malloc(sizeof(orc_cand) * n * cap);
-  if (!G || !isnew || !newl || !oldl || !nfwd || !ofwd || !nrev || !orev || !cand || !ncand ||
-      !off || !bucket) {
-    free(G); free(isnew); free(newl); free(oldl); free(nfwd); free(ofwd); free(nrev);
+  if (!newl || !oldl || !nfwd || !ofwd || !nrev || !orev || !cand || !ncand || !off || !bucket) {
+    free(newl); free(oldl); free(nfwd); free(ofwd); free(nrev);
     free(orev); free(cand); free(ncand); free(off); free(bucket);
     return ORC_ERR_ALLOC;
   }
-
-  /* InitKNNGraphIndexKernel (:1673-1692) + distances + per-row sort. */
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < n; i++) {
-    orc_nb *row = G + i * k;
-    for (int32_t t = 0; t < k; t++) {
-      int64_t pos = i * k + t;
-      int32_t blk = t / 32;
-      int64_t label = (int64_t)(orc_xorshift64star((uint64_t)pos) % (uint64_t)n);
-      for (;;) {
-        int bad = (label % NB != blk) || label == i;
-        for (int32_t u = 0; u < t && !bad; u++) bad = (row[u].id == label);
-        if (!bad) break;
-        label = (label + 1) % n;
-      }
-      row[t].id = (int32_t)label;
-      row[t].d = orc_diffsum(X + i * (int64_t)d, X + label * d, d);
-    }
-    qsort(row, k, sizeof(orc_nb), cmp_nb);
-    memset(isnew + i * k, 1, k);
-  }
+  const int cross_only = split > 0;
 
   for (int32_t it = 0; it < iterations; it++) {
     /* PrepareGraph (:44-98): first S new / first S old by position. */
@@ -160,10 +124,11 @@ int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
     for (int64_t i = 0; i < n; i++) {
       int32_t cn = 0, co = 0;
       for (int32_t t = 0; t < k; t++) {
+        const int32_t id = G[i * k + t].id;
         if (isnew[i * k + t]) {
-          if (cn < S) newl[i * 2 * S + cn++] = G[i * k + t].id;
-        } else {
-          if (co < S) oldl[i * 2 * S + co++] = G[i * k + t].id;
+          if (cn < S) newl[i * 2 * S + cn++] = id;
+        } else if (split <= 0 || ((i < split) == (id < split))) {
+          if (co < S) oldl[i * 2 * S + co++] = id;
         }
       }
       nfwd[i] = cn;
@@ -215,13 +180,15 @@ int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
         for (int32_t b = 0; b < no; b++)
           dno[a][b] = orc_diffsum(X + (int64_t)nv[a] * d, X + (int64_t)ov[b] * d, d);
       for (int32_t a = 0; a < nn; a++) {
-        orc_nb best = {1e10f, INT_MAX};
-        for (int32_t b = 0; b < nn; b++) {
-          if (b == a) continue;
-          orc_nb c = {orc_diffsum(X + (int64_t)nv[a] * d, X + (int64_t)nv[b] * d, d), nv[b]};
-          if (nb_less(c, best)) best = c;
+        if (!cross_only) {
+          orc_nb best = {1e10f, INT_MAX};
+          for (int32_t b = 0; b < nn; b++) {
+            if (b == a) continue;
+            orc_nb c = {orc_diffsum(X + (int64_t)nv[a] * d, X + (int64_t)nv[b] * d, d), nv[b]};
+            if (nb_less(c, best)) best = c;
+          }
+          if (best.id != INT_MAX) cb[nc++] = (orc_cand){nv[a], best.id, best.d};
         }
-        if (best.id != INT_MAX) cb[nc++] = (orc_cand){nv[a], best.id, best.d};
         orc_nb best2 = {1e10f, INT_MAX};
         for (int32_t b = 0; b < no; b++) {
           orc_nb c = {dno[a][b], ov[b]};
@@ -273,13 +240,141 @@ int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
       }
     }
   }
-  for (int64_t i = 0; i < n * k; i++) {
-    ids_out[i] = G[i].id;
-    dist_out[i] = G[i].d;
-  }
-  free(G); free(isnew); free(newl); free(oldl); free(nfwd); free(ofwd); free(nrev);
+  free(newl); free(oldl); free(nfwd); free(ofwd); free(nrev);
   free(orev); free(cand); free(ncand); free(off); free(bucket);
   return ORC_OK;
+}
+
+/*
+ * Sequential restatement of gpuknn::NNDescent (nndescent.cu:2088-2199):
+ *   InitRandomKNNGraph (:1800-1871; ids from xorshift64star(pos) % n, :1673-1692),
+ *   then `iterations` rounds of PrepareForUpdate (:624-671) + UpdateGraph
+ *   (:1487-1580).  Candidate semantics follow the join kernels: every new
+ *   neighbour x is offered its closest other new neighbour (:1030-1108) and its
+ *   closest old neighbour, every old neighbour its closest new one
+ *   (:1259-1326); InsertToGlobalGraph (:969-1028) keeps a sorted, duplicate-free
+ *   list of k.  Flags: all entries become "old" before the join (MarkAllToOld
+ *   :1398), inserted candidates are "new".
+ * Deterministic choices where the reference races: forward samples are the
+ * first S new / old entries by list position; reverse samples keep the first S
+ * sources in row order; ties order by (distance, id).  The initial distance is
+ * the same sequential difference sum as the join (the reference's warp-tree sum
+ * at :1694-1726 rounds differently), and an initial id already present in the
+ * row is advanced like a self id, so rows never hold duplicates.
+ * Output ids carry no old/new flag; distances are squared L2.
+ */
+int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
+                  int32_t iterations, int32_t *ids_out, float *dist_out) {
+  if (n < 2 || k < 1 || k > 1024 || S < 1 || 2 * S > k || n <= k) return ORC_ERR_ARG;
+  const int32_t NB = (k + 31) / 32;
+  orc_nb *G = (orc_nb *)malloc(sizeof(orc_nb) * n * k);
+  uint8_t *isnew = (uint8_t *)malloc((size_t)n * k);
+  if (!G || !isnew) {
+    free(G); free(isnew);
+    return ORC_ERR_ALLOC;
+  }
+
+  /* InitKNNGraphIndexKernel (:1673-1692) + distances + per-row sort. */
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    orc_nb *row = G + i * k;
+    for (int32_t t = 0; t < k; t++) {
+      int64_t pos = i * k + t;
+      int32_t blk = t / 32;
+      int64_t label = (int64_t)(orc_xorshift64star((uint64_t)pos) % (uint64_t)n);
+      for (;;) {
+        int bad = (label % NB != blk) || label == i;
+        for (int32_t u = 0; u < t && !bad; u++) bad = (row[u].id == label);
+        if (!bad) break;
+        label = (label + 1) % n;
+      }
+      row[t].id = (int32_t)label;
+      row[t].d = orc_diffsum(X + i * (int64_t)d, X + label * d, d);
+    }
+    qsort(row, k, sizeof(orc_nb), cmp_nb);
+    memset(isnew + i * k, 1, k);
+  }
+
+  int rc = nnd_iterate(X, n, d, k, S, iterations, 0, G, isnew);
+  if (rc == ORC_OK)
+    for (int64_t i = 0; i < n * k; i++) {
+      ids_out[i] = G[i].id;
+      dist_out[i] = G[i].d;
+    }
+  free(G); free(isnew);
+  return rc;
+}
+
+/*
+ * Sequential restatement of gpuknn::KNNMerge (knnmerge.cu:401-437): the kNN
+ * graph of the union of the point sets A = X[0, n1) and B = X[n1, n1 + n2)
+ * (X holds them back to back, as MergeVectors :358-399 lays them out) from
+ * the graphs of each (ids1 [n1, k] local to A, ids2 [n2, k] local to B).
+ * Initial rows (InitRandomBlockedKNNGraph :80-185, k <= 32, one block): the
+ * first k - k/2 entries of the row's own subgraph row, shifted into the
+ * merged numbering and old (MarkAllToOld of both subgraphs, :408-410), then
+ * k/2 ids of the other set, xorshift64star(local row * (k/2) + t) % |other|,
+ * new.  An id drawn twice is advanced to the next free one (the reference
+ * keeps repeats).  All k distances are recomputed (InitRandomKNNGraph with
+ * start_from_random_index = false, nndescent.cu:2013) as the join's sequential
+ * difference sum, and each row is sorted by (distance, id).  Then
+ * `iterations` merge rounds (nnd_iterate with split = n1).  The subgraph ids
+ * must be valid: in their set, no self id, no repeat (ORC_ERR_ARG otherwise).
+ */
+int orc_knn_merge(const float *X, int64_t n1, int64_t n2, int32_t d, const int32_t *ids1,
+                  const int32_t *ids2, int32_t k, int32_t S, int32_t iterations,
+                  int32_t *ids_out, float *dist_out) {
+  if (k < 1 || k > 32 || S < 1 || 2 * S > k || n1 <= k || n2 <= k) return ORC_ERR_ARG;
+  const int64_t n = n1 + n2;
+  const int32_t h = k - k / 2, r = k / 2;
+  for (int64_t i = 0; i < n; i++) {
+    const int inb = i >= n1;
+    const int64_t local = inb ? i - n1 : i, own_n = inb ? n2 : n1;
+    const int32_t *own = inb ? ids2 : ids1;
+    for (int32_t t = 0; t < h; t++) {
+      const int32_t v = own[local * k + t];
+      if (v < 0 || v >= own_n || v == local) return ORC_ERR_ARG;
+      for (int32_t u = 0; u < t; u++)
+        if (own[local * k + u] == v) return ORC_ERR_ARG;
+    }
+  }
+  orc_nb *G = (orc_nb *)malloc(sizeof(orc_nb) * n * k);
+  uint8_t *isnew = (uint8_t *)malloc((size_t)n * k);
+  if (!G || !isnew) {
+    free(G); free(isnew);
+    return ORC_ERR_ALLOC;
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    const int inb = i >= n1;
+    const int64_t local = inb ? i - n1 : i;
+    const int64_t own_off = inb ? n1 : 0, oth_n = inb ? n1 : n2, oth_off = inb ? 0 : n1;
+    const int32_t *own = inb ? ids2 : ids1;
+    orc_nb *row = G + i * k;
+    for (int32_t t = 0; t < h; t++) row[t].id = (int32_t)(own[local * k + t] + own_off);
+    for (int32_t t = 0; t < r; t++) {
+      int64_t label = (int64_t)(orc_xorshift64star((uint64_t)(local * r + t)) % (uint64_t)oth_n);
+      for (;;) {
+        int dup = 0;
+        for (int32_t u = 0; u < t && !dup; u++) dup = (row[h + u].id == label + oth_off);
+        if (!dup) break;
+        label = (label + 1) % oth_n;
+      }
+      row[h + t].id = (int32_t)(label + oth_off);
+    }
+    for (int32_t t = 0; t < k; t++)
+      row[t].d = orc_diffsum(X + i * (int64_t)d, X + (int64_t)row[t].id * d, d);
+    qsort(row, k, sizeof(orc_nb), cmp_nb);
+    for (int32_t t = 0; t < k; t++) isnew[i * k + t] = (uint8_t)((row[t].id >= n1) != inb);
+  }
+  int rc = nnd_iterate(X, n, d, k, S, iterations, n1, G, isnew);
+  if (rc == ORC_OK)
+    for (int64_t i = 0; i < n * k; i++) {
+      ids_out[i] = G[i].id;
+      dist_out[i] = G[i].d;
+    }
+  free(G); free(isnew);
+  return rc;
 }
 
 /* Exact kNN in FP64 (the ground truth cmake/eval.py:57 reads from outside the

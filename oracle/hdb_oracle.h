@@ -40,6 +40,9 @@ int orc_num_threads(void);
 uint64_t orc_xorshift64star(uint64_t x);
 int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t sample_num,
                   int32_t iterations, int32_t *ids_out, float *dist_out);
+int orc_knn_merge(const float *X, int64_t n1, int64_t n2, int32_t d, const int32_t *ids1,
+                  const int32_t *ids2, int32_t k, int32_t sample_num, int32_t iterations,
+                  int32_t *ids_out, float *dist_out);
 int orc_bruteforce_knn(const float *X, int64_t n, int32_t d, int32_t k,
                        const int64_t *queries, int64_t nq, int32_t *ids_out, double *dist_out);
 double orc_recall(const int32_t *ids, int32_t k_ids, const int32_t *gt, int32_t k_gt,

@@ -49,6 +49,7 @@ def lib():
             "orc_num_threads": (C.c_int, []),
             "orc_xorshift64star": (C.c_uint64, [C.c_uint64]),
             "orc_nndescent": (C.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _P, _P]),
+            "orc_knn_merge": (C.c_int, [_P, _I64, _I64, _I32, _P, _P, _I32, _I32, _I32, _P, _P]),
             "orc_bruteforce_knn": (C.c_int, [_P, _I64, _I32, _I32, _P, _I64, _P, _P]),
             "orc_recall": (C.c_double, [_P, _I32, _P, _I32, _I64, _I32]),
             "orc_fix_distances": (None, [_P, _I64, _I32, _P, _I32, _P]),
@@ -102,6 +103,27 @@ def nndescent(X, k=32, sample_num=16, iterations=6):
     rc = lib().orc_nndescent(_p(X), n, d, k, sample_num, iterations, _p(ids), _p(dist))
     if rc:
         raise ValueError(f"orc_nndescent failed ({rc})")
+    return ids, dist
+
+
+def knn_merge(X1, ids1, X2, ids2, sample_num=12, iterations=11):
+    """gpuknn::KNNMerge (knnmerge.cu:401-437) restated: the kNN graph of the
+    union of X1 and X2 (rows of X1 first, ids of X2 shifted by len(X1)) from
+    ids1 [n1, k] and ids2 [n2, k], ids local to their set."""
+    X1 = _c(X1, np.float32)
+    X2 = _c(X2, np.float32)
+    ids1 = _c(ids1, np.int32)
+    ids2 = _c(ids2, np.int32)
+    n1, d = X1.shape
+    n2 = X2.shape[0]
+    k = ids1.shape[1]
+    X = np.ascontiguousarray(np.concatenate([X1, X2]))
+    ids = np.empty((n1 + n2, k), np.int32)
+    dist = np.empty((n1 + n2, k), np.float32)
+    rc = lib().orc_knn_merge(_p(X), n1, n2, d, _p(ids1), _p(ids2), k, sample_num, iterations,
+                             _p(ids), _p(dist))
+    if rc:
+        raise ValueError(f"orc_knn_merge failed ({rc})")
     return ids, dist
 
 
