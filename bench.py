@@ -45,6 +45,10 @@ def parse_args():
                     help="form (default: bf16; fp32 for the batched workloads)")
     ap.add_argument("--instances", type=int, default=0,
                     help="batched workloads: only the first N instances (0: all)")
+    ap.add_argument("--shard-instances", action="store_true",
+                    help="batched workloads on N GPUs: one batch, its instances spread over the "
+                         "ranks by greedy size balancing (strong scaling) instead of a seeded "
+                         "copy of the batch per rank (weak scaling)")
     ap.add_argument("--loop-instances", type=int, default=256,
                     help="batched workloads: instances timed in the per-instance loop comparison")
     ap.add_argument("--no-compare", action="store_true",
@@ -162,6 +166,24 @@ def max_over_ranks(ms, device):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def sum_over_ranks(v, device):
+    """The sum of a per-rank count over all ranks (the value itself on one rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def batch_instance_sizes(bw, count):
+    """Points of every instance of a batched workload (its first `count`)."""
+    from gpu_hdbscan_b200 import synth
+    if isinstance(bw, synth.SplitWorkload):
+        return synth.split_sizes(bw, count)
+    return [n for n, _, _ in synth.batch_layout(bw, count)]
 
 
 def whole_job_rate(n, steps, world, ms):
@@ -472,9 +494,25 @@ def run_ours_batch(args, bw):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
-    rbw = type(bw)(**{**bw.__dict__, "seed": bw.seed + 1000 * rank})
-    views, layout = synth.generate_batch_torch(rbw, device=dev, count=args.instances or None)
+    count = args.instances or None
+    if args.shard_instances:
+        # one batch over all ranks: rank r clusters the instances the greedy
+        # size balancing gives it (same seed everywhere, no exchange)
+        from gpu_hdbscan_b200 import sharding
+        all_sizes = batch_instance_sizes(bw, count)
+        if len(all_sizes) < world:
+            raise SystemExit("--shard-instances needs at least one instance per rank")
+        parts = sharding.assign_instances(all_sizes, world)
+        rbw = bw
+        views, layout = synth.generate_batch_torch(rbw, device=dev, count=count,
+                                                   indices=parts[rank])
+        n_job = sum(all_sizes)
+    else:
+        rbw = type(bw)(**{**bw.__dict__, "seed": bw.seed + 1000 * rank})
+        views, layout = synth.generate_batch_torch(rbw, device=dev, count=count)
     n_total = sum(n for n, _, _ in layout)
+    if not args.shard_instances:
+        n_job = n_total * world
     ctx = g.Context(local)
     kw = dict(k=bw.k, mpts=bw.mpts, sample_num=bw.sample_num, iterations=bw.iterations,
               precision=prec)
@@ -506,8 +544,8 @@ def run_ours_batch(args, bw):
     ms_max, outs = timed(lambda: ctx.hdbscan_batched(views, **kw_b), args.steps, args.warmup)
     clk = clocks.stop()
     stats = [o[2] for o in outs]
-    value = whole_job_rate(n_total, args.steps, world, ms_max)
-    failed = sum(1 for s_ in stats[-1]["instance_status"] if s_ != 0)
+    value = n_job * args.steps / (ms_max / 1e3)
+    failed = int(sum_over_ranks(sum(1 for s_ in stats[-1]["instance_status"] if s_ != 0), dev))
 
     # per-instance loop (hdb_run per instance) against the batch on the same
     # instances; the loop skips the instances the batch found disconnected
@@ -544,7 +582,7 @@ def run_ours_batch(args, bw):
             pinned = False
         ctx.hdbscan_batched(hosts, **kw_b)
         te, _ = timed(lambda: ctx.hdbscan_batched(hosts, **kw_b), args.steps, 0)
-        e2e = {"value": whole_job_rate(n_total, args.steps, world, te), "unit": UNIT,
+        e2e = {"value": n_job * args.steps / (te / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(sum(v.numel() for v in views) * 4),
                "d2h_bytes_per_step": int(n_total * 4), "pinned_inputs": pinned}
         del hosts
@@ -583,13 +621,15 @@ def run_ours_batch(args, bw):
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
+                "scaling": "strong" if args.shard_instances else "weak", "vs_baseline": None,
                 "dtype": "f32" if prec == g.HDB_PREC_FP32 else "bf16", "data": "synthetic",
                 "config": {"workload": bw.name, "instances": len(layout), "n_total": n_total,
+                           "n_job": n_job,
                            "points_per_d": {str(d): c for d, c in sorted(per_d.items())},
                            "k": bw.k, "mpts": bw.mpts, "sample_num": bw.sample_num,
                            "iterations": bw.iterations, "form": args.precision,
-                           "parallelism": f"replicas{world}",
+                           "parallelism": (f"instances{world}" if args.shard_instances
+                                           else f"replicas{world}"),
                            "l2": f"inputs larger than L2 ({sum(v.numel() for v in views) * 4 / 1e9:.1f} GB)",
                            "stage_ms": {s_: round(last[f"ms_{s_}"], 3) for s_ in
                                         ("knn", "graph", "mst", "tree", "total")},

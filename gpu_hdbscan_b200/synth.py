@@ -220,10 +220,12 @@ def batch_instance(bw: BatchWorkload, i: int, n: int, d: int, blobs: int) -> Wor
                     bw.seed * 1_000_003 + i)
 
 
-def generate_batch_torch(bw, device="cuda", count: int | None = None):
+def generate_batch_torch(bw, device="cuda", count: int | None = None, indices=None):
     """The instances on `device`: one [sum n, d] array per d with the instances
     of that d back to back (in instance order), and per instance a view into
-    it, in instance order.  -> (views, layout of (n, d, blobs))."""
+    it, in instance order.  -> (views, layout of (n, d, blobs)).  `indices`
+    (ascending) keeps only those instances of the first `count`, generated
+    exactly as in the whole batch; views and layout then follow `indices`."""
     import torch
 
     if isinstance(bw, SplitWorkload):
@@ -234,19 +236,26 @@ def generate_batch_torch(bw, device="cuda", count: int | None = None):
         for m in sizes:
             views.append(X[row:row + m])
             row += m
-        return views, [(m, w.d, 0) for m in sizes]
-    layout = batch_layout(bw, count)
+        layout = [(m, w.d, 0) for m in sizes]
+        if indices is not None:
+            views = [views[i].clone() for i in indices]
+            layout = [layout[i] for i in indices]
+            del X
+        return views, layout
+    full = batch_layout(bw, count)
+    keep = list(range(len(full))) if indices is None else list(indices)
+    layout = [full[i] for i in keep]
     by_d = {}
-    for i, (n, d, b) in enumerate(layout):
-        by_d.setdefault(d, []).append(i)
-    views = [None] * len(layout)
+    for j, i in enumerate(keep):
+        by_d.setdefault(full[i][1], []).append((j, i))
+    views = [None] * len(keep)
     for d, idx in by_d.items():
-        total = sum(layout[i][0] for i in idx)
+        total = sum(full[i][0] for _, i in idx)
         buf = torch.empty((total, d), dtype=torch.float32, device=device)
         row = 0
-        for i in idx:
-            n, _, b = layout[i]
+        for j, i in idx:
+            n, _, b = full[i]
             buf[row:row + n] = generate_torch(batch_instance(bw, i, n, d, b), device=device)
-            views[i] = buf[row:row + n]
+            views[j] = buf[row:row + n]
             row += n
     return views, layout
