@@ -4,7 +4,7 @@
 //
 // The reference's multi-GPU plumbing (countDegrees, countThreshold_,
 // calculateUntieScore, calculateMutualReachabilityDistance) loops over 3 GPUs;
-// on a one-GPU box those loops fail, so this driver calls the same reference
+// on a machine with one GPU those loops fail, so this driver calls the same reference
 // kernels and host functions those wrappers call, on device 0, in the order of
 // buildEnhancedKNNG / buildECLgraph (HDBSCAN/graphs/graph.cu:16-176).
 // Everything after the graph -- cpuMST, buildMST (with sort_edges),

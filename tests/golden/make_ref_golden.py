@@ -4,7 +4,7 @@ unmodified reference sources) on small seeded inputs and stores inputs and
 outputs as compressed .npz files.
 
 Needs a GPU (the reference's tree stages allocate managed memory and launch
-fill kernels).  Usage on a GPU box, from the repository root:
+fill kernels).  Usage on a machine with a GPU, from the repository root:
 
     python tests/golden/make_ref_golden.py OUTDIR
     python tests/golden/make_ref_golden.py --add-mst-gpu OUTDIR

@@ -2,7 +2,7 @@
 
 tests/golden/ref_*.npz were produced by tests/golden/make_ref_golden.py, which
 runs the unmodified reference sources (compiled by oracle/ref/Makefile) on a
-GPU box.  These CPU tests pin every stage of the oracle to them; the GPU tests
+machine with a GPU.  These CPU tests pin every stage of the oracle to them; the GPU tests
 (test_gpu_golden.py) pin the CUDA path to the same files."""
 import glob
 import json
