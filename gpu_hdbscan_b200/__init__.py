@@ -252,23 +252,32 @@ class Context:
         return labels, ncl.value, cond, stab
 
     def hdbscan(self, X, k=32, mpts=32, sample_num=16, iterations=6, precision=HDB_PREC_FP32,
-                distance=HDB_DIST_SQRT, stability=HDB_STAB_FP32, labels_out=None, mst_gpu=0):
+                distance=HDB_DIST_SQRT, stability=HDB_STAB_FP32, labels_out=None, mst_gpu=0,
+                want_graph=False):
         """The whole path (hdb_run).  X on the host (numpy / CPU tensor) runs with
         host_io=1: the H2D copy of X and the D2H copy of the labels are inside
-        the call.  X on the device returns device labels."""
+        the call.  X on the device returns device labels.  want_graph=True
+        (hdb_run_with_graph) also returns the kNN graph the labels were
+        computed from, [n, k, 2] NNDElement rows beside the labels:
+        (labels, stats, G)."""
         torch = self._torch
         host = not (isinstance(X, torch.Tensor) and X.is_cuda)
+        dev = None if host else self.device
         if host:
             X = torch.as_tensor(X, dtype=torch.float32).contiguous()
-            labels = labels_out if labels_out is not None else torch.empty(X.shape[0], dtype=torch.int32)
         else:
             X = X.to(torch.float32).contiguous()
-            labels = labels_out if labels_out is not None else torch.empty(
-                X.shape[0], dtype=torch.int32, device=self.device)
+        labels = labels_out if labels_out is not None else torch.empty(
+            X.shape[0], dtype=torch.int32, device=dev)
         n, d = X.shape
         p = _lib.Params(_lib.KnnParams(k, sample_num, iterations, precision), mpts, distance,
                         stability, 1 if host else 0, mst_gpu)
         st = _lib.RunStats()
+        if want_graph:
+            G = torch.empty((n, k, 2), dtype=torch.int32, device=dev)
+            _lib.check(self.L.hdb_run_with_graph(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels),
+                                                 _ptr(G), C.byref(st)))
+            return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}, G
         _lib.check(self.L.hdb_run(self.h, _ptr(X), n, d, C.byref(p), _ptr(labels), C.byref(st)))
         return labels, {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
 

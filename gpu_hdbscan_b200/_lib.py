@@ -24,7 +24,7 @@ HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
            "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
-           "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
+           "hdb_run_with_graph", "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
            "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised",
            "hdb_knn_merge")
 
@@ -101,6 +101,8 @@ def load(path: str = LIB_PATH):
         "hdb_condense_select": (C.c_int, [_P, _P, _I64, _I32, _I32, _P, C.POINTER(_I32), _P,
                                           C.POINTER(_I64), _P, C.POINTER(_I64)]),
         "hdb_run": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(Params), _P, C.POINTER(RunStats)]),
+        "hdb_run_with_graph": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(Params), _P, _P,
+                                         C.POINTER(RunStats)]),
         "hdb_run_knn": (C.c_int, [_P, _P, _P, _I64, _I32, C.POINTER(Params), _P,
                                   C.POINTER(RunStats)]),
         "hdb_sort_edges_noalloc": (C.c_int, [_P, _I64, _P]),

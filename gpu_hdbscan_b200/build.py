@@ -32,12 +32,30 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(src, obj, verbose):
+    cmd = [NVCC, *ARCH, *FLAGS, "-c", "-o", obj, src]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every csrc/*.cu that changed (in parallel, objects under
+    _build/), then links libhdb_b200.so."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = _sources()
-    deps = srcs + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [
+    headers = glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [
         os.path.join(ROOT, "include", "hdb", "hdb.h")]
-    if force or _stale(LIB, deps):
-        cmd = [NVCC, *ARCH, *FLAGS, "-shared", "-o", LIB, *srcs, "-lcudart"]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s, *headers])]
+    if todo:
+        with ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 4)) as ex:
+            for f in [ex.submit(_compile, s, o, verbose) for s, o in todo]:
+                f.result()
+    if force or _stale(LIB, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

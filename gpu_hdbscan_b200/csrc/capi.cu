@@ -578,12 +578,10 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
   js_acc->candidates += js.candidates;
 }
 
-}  // namespace
-
-extern "C" {
-
-HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
-                           const hdb_params *params, int32_t *labels, hdb_run_stats *stats) {
+// hdb_run / hdb_run_with_graph: the whole path on one instance; G_out
+// (optional) receives the kNN graph the labels were computed from.
+hdb_status run_single(hdb_ctx *h, const float *X, int64_t n, int32_t d, const hdb_params *params,
+                      int32_t *labels, hdb_nnd_element *G_out, hdb_run_stats *stats) {
   return guard([&] {
     Context *ctx = C(h);
     require_ptr(X, "X");
@@ -618,6 +616,9 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
       Buf<hdb_nnd_element> G(ctx, (size_t)n * k);
       nndescent(ctx, Xuse, n, d, p.knn, G, &dropped, &js);
       HDB_CUDA(cudaEventRecord(ev[2], st));
+      if (G_out)
+        HDB_CUDA(cudaMemcpyAsync(G_out, G.get(), (size_t)n * k * sizeof(hdb_nnd_element),
+                                 p.host_io ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
       Buf<float> dist;
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
@@ -643,6 +644,21 @@ HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
       *stats = rs;
     }
   });
+}
+
+}  // namespace
+
+extern "C" {
+
+HDB_API hdb_status hdb_run(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                           const hdb_params *params, int32_t *labels, hdb_run_stats *stats) {
+  return run_single(h, X, n, d, params, labels, nullptr, stats);
+}
+
+HDB_API hdb_status hdb_run_with_graph(hdb_ctx *h, const float *X, int64_t n, int32_t d,
+                                      const hdb_params *params, int32_t *labels,
+                                      hdb_nnd_element *G, hdb_run_stats *stats) {
+  return run_single(h, X, n, d, params, labels, G, stats);
 }
 
 }  // extern "C"

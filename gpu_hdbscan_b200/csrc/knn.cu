@@ -1375,6 +1375,7 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
     ctx->launches++;
     HDB_CHECK_LAUNCH();
     sort_overflow(ctx, ib, n);
+    HDB_CHECK_LAUNCH();
   }
   k_finalize<<<grid_rows, 32 * wpb, 0, st>>>(n, k, gid, gdist, ib, G); ctx->launches++;
   HDB_CHECK_LAUNCH();

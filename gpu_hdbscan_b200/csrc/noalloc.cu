@@ -9,8 +9,13 @@
 // that every GPU which loads libhdb_b200.so keeps until the process exits.
 //
 // Host code cannot use the array's name as a device address (in host code the
-// symbol is a host-side stand-in); the device address is taken once per device
-// with cudaGetSymbolAddress, on the first call made with that device current.
+// symbol is a host-side stand-in); the device address is taken with
+// cudaGetSymbolAddress on each device, with that device current, by the first
+// call that succeeds there.  With lazy module loading (CUDA 12's default) that
+// same lookup is what places the array and the sort kernels on the device, so
+// it can fail with an out-of-memory error on a device that is already full; a
+// failed lookup is not remembered, the next call tries again.  Callers who run
+// on a full device make one warm-up call (m = 0 is enough) before it fills.
 #include <mutex>
 
 #include "hdb_internal.cuh"
@@ -41,23 +46,27 @@ constexpr size_t kNoAllocScratchBytes = kOffScanOffs + align256(kScanSums * 4); 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-void *g_scratch_addr[kMaxDevices] = {};
-cudaError_t g_setup_err[kMaxDevices] = {};
+std::mutex g_setup_mutex;
+void *g_scratch_addr[kMaxDevices] = {};  // non-null once a lookup succeeded
 
-// Device address of the scratch array for the current device (set up once).
+// Device address of the scratch array on the current device.  Only a
+// successful lookup is kept; a failed one (for instance out of memory while
+// the module is placed) is reported and retried on the next call.
 unsigned char *scratch_for_current_device() {
   int dev = -1;
   HDB_CUDA(cudaGetDevice(&dev));
   HDB_REQUIRE(dev >= 0 && dev < kMaxDevices, HDB_ERR_ARG, "device ordinal out of range");
-  std::call_once(g_once[dev], [dev] {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (g_scratch_addr[dev] == nullptr) {
     void *p = nullptr;
-    g_setup_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();  // not sticky: leave no error behind for the caller
+      throw_cuda(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    }
+    HDB_REQUIRE(p != nullptr, HDB_ERR_CUDA, "no device address for the scratch array");
     g_scratch_addr[dev] = p;
-  });
-  if (g_setup_err[dev] != cudaSuccess)
-    throw_cuda(g_setup_err[dev], "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-  HDB_REQUIRE(g_scratch_addr[dev] != nullptr, HDB_ERR_CUDA, "no device address for the scratch array");
+  }
   return static_cast<unsigned char *>(g_scratch_addr[dev]);
 }
 
@@ -91,10 +100,12 @@ extern "C" HDB_API hdb_status hdb_sort_edges_noalloc(hdb_mst_edge *edges, int64_
     HDB_REQUIRE(m <= kNoAllocMaxEdges, HDB_ERR_ARG,
                 "hdb_sort_edges_noalloc: more than 262144 edges (the static scratch limit); "
                 "use hdb_sort_edges");
+    // placed and looked up before anything else, so that a call with m = 0
+    // serves as the warm-up that places the array
+    unsigned char *base = scratch_for_current_device();
     if (m <= 1) return;
     HDB_REQUIRE(edges != nullptr, HDB_ERR_ARG, "hdb_sort_edges_noalloc: NULL edges");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    unsigned char *base = scratch_for_current_device();
     uint32_t *keys = reinterpret_cast<uint32_t *>(base + kOffKeys);
     uint32_t *keys_tmp = reinterpret_cast<uint32_t *>(base + kOffKeysTmp);
     uint32_t *idx = reinterpret_cast<uint32_t *>(base + kOffIdx);

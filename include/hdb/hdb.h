@@ -232,6 +232,17 @@ HDB_API hdb_status hdb_condense_select(hdb_ctx *ctx, const hdb_linkage_node *hie
 HDB_API hdb_status hdb_run(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
                            const hdb_params *params, int32_t *labels, hdb_run_stats *stats);
 
+/* hdb_run that also hands back the kNN graph it built, the in-memory form of
+ * the .kgraph file the reference's hdbscan_ flow writes between its kNN
+ * and HDBSCAN stages (build_kNNG.cu:131-174, read back at
+ * HDBSCAN/_new.cu:199): G [n, params->knn.k] NNDElement rows as
+ * hdb_nndescent writes them (squared distances, flags kept), the graph the
+ * labels were computed from.  G may be NULL (then this is hdb_run); it is
+ * device memory, or host memory with params->host_io = 1. */
+HDB_API hdb_status hdb_run_with_graph(hdb_ctx *ctx, const float *X, int64_t n, int32_t d,
+                                      const hdb_params *params, int32_t *labels,
+                                      hdb_nnd_element *G, hdb_run_stats *stats);
+
 /* The stages after the kNN graph in the HDBSCAN/_new.cu:196-347 order, which
  * reads a finished .kgraph (ReadBinaryVecs, _new.cu:199) instead of building
  * it: G [n, params->knn.k] NNDElement rows (flags allowed), X [n, d] ->
@@ -306,10 +317,16 @@ HDB_API hdb_status hdb_bf16_distance_tiles(hdb_ctx *ctx, const float *X, int64_t
  * m may be at most 262144 edges (HDB_ERR_ARG above that).  `edges` is device
  * memory; work runs on `stream` (NULL = legacy default stream) of the current
  * device and the call returns when it is done.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the one array: calls whose
- * work overlaps on the GPU (for instance from different streams or threads)
- * race and corrupt each other's result. */
+ * looks up the array's device address (cudaGetSymbolAddress); with CUDA's
+ * lazy module loading that lookup is also what places the array on the
+ * device, so it can fail (HDB_ERR_CUDA) on a device that is already full.
+ * A failed lookup is retried by the next call.  Make one warm-up call on each
+ * device before it fills and before any stream capture: m = 0 (edges may then
+ * be NULL) places the array and sorts nothing; a call with m >= 2 also loads
+ * the sort's kernels, which lazy loading otherwise places on the first real
+ * sort.  All calls share the one
+ * array: calls whose work overlaps on the GPU (for instance from different
+ * streams or threads) race and corrupt each other's result. */
 HDB_API hdb_status hdb_sort_edges_noalloc(hdb_mst_edge *edges, int64_t m, void *stream);
 
 #ifdef __cplusplus

@@ -30,8 +30,17 @@
 #include "tools/filetool.hpp"
 
 // ---- stand-ins for the reference's fixed-path file helpers (build_kNNG.cu) ----
+// The reference passes the kNN graph, the mutual flags, the vectors and the
+// core-SG's Euclidean weights between its stages through files under fixed
+// /nndescent/... paths.  Here each reader serves, and each writer keeps, the
+// arrays of the current driver call.
 static const float *g_vectors = nullptr;
 static int g_dim = 0;
+static const int *g_ids = nullptr;      // kNN ids [g_n, k] of the current call
+static const float *g_dist = nullptr;   // their distances
+static long g_n = 0;
+static int *g_flags = nullptr;          // mutual flags kept by write_bool_dict
+static float *g_euclid = nullptr;       // kept by write_euclidean_distance_vecs
 
 // jesus (build_kNNG.cu:58-77) reads /nndescent/.../vectors.fvecs and gathers
 // the antihub rows; here the rows come from the caller's array.
@@ -42,21 +51,55 @@ float *jesus(int *antihubs, int num_antihubs, int *paz) {
   *paz = g_dim;
   return out;
 }
-// write_bool_dict (build_kNNG.cu:79-87) only persists the mutual flags.
-void write_bool_dict(int *, long, long) {}
-
-// The other fixed-path helpers of build_kNNG.cu that core-sg.cu links against
-// serve only build_CoreSG's own file flow, which this driver never enters.
-static void not_in_driver(const char *what) {
-  fprintf(stderr, "%s is not available in the reference driver\n", what);
-  abort();
+// write_bool_dict / read_bool_dict (build_kNNG.cu:79-87): the mutual flags of
+// calculate_nindex, read back by Union_kNNG_MST (core-sg.cu:296).
+void write_bool_dict(int *flags, long n, long kk) {
+  free(g_flags);
+  g_flags = (int *)malloc((size_t)n * kk * sizeof(int));
+  memcpy(g_flags, flags, (size_t)n * kk * sizeof(int));
 }
-float *ReadObjects(long *) { not_in_driver("ReadObjects"); return nullptr; }
-NNDElement *ReadkNNGgraph() { not_in_driver("ReadkNNGgraph"); return nullptr; }
-int *read_bool_dict() { not_in_driver("read_bool_dict"); return nullptr; }
-float *read_euclidean_distance_vecs() { not_in_driver("read_euclidean_distance_vecs"); return nullptr; }
-void write_euclidean_distance_vecs(float *, long) { not_in_driver("write_euclidean_distance_vecs"); }
+int *read_bool_dict() {
+  int *out = (int *)malloc((size_t)g_n * k * sizeof(int));
+  memcpy(out, g_flags, (size_t)g_n * k * sizeof(int));
+  return out;
+}
+// ReadkNNGgraph: the .kgraph of the current call as NNDElement rows (the
+// callers release it with delete, as they do the reader's array).
+NNDElement *ReadkNNGgraph() {
+  NNDElement *G = new NNDElement[(size_t)g_n * k];
+  for (long i = 0; i < g_n * (long)k; i++) G[i] = NNDElement(g_dist[i], g_ids[i]);
+  return G;
+}
+// ReadObjects: the vectors (core_sg_calculate_MRD_mst frees them with free()).
+float *ReadObjects(long *pf) {
+  float *out = (float *)malloc((size_t)g_n * g_dim * sizeof(float));
+  memcpy(out, g_vectors, (size_t)g_n * g_dim * sizeof(float));
+  *pf = g_dim;
+  return out;
+}
+// The core-SG's Euclidean weights, written by Union_kNNG_MST (core-sg.cu:394)
+// and read back by update_core_sg_weights (core-sg.cu:466).
+void write_euclidean_distance_vecs(float *e, long edges) {
+  free(g_euclid);
+  g_euclid = (float *)malloc((size_t)edges * sizeof(float));
+  memcpy(g_euclid, e, (size_t)edges * sizeof(float));
+}
+float *read_euclidean_distance_vecs() {
+  float *out = g_euclid;  // ownership passes to the caller
+  g_euclid = nullptr;
+  return out;
+}
 
+// The helpers of HDBSCAN/core-sg/core-sg.cu that Union_kNNG_MST calls
+// (defined there, not declared in its header).
+void core_sg_calculate_nindex(long int nodes, int *flag_knn, int *kNN, ECLgraph *g,
+                              MSTedge *mst_edges);
+void core_sg_calculate_nlist(long int nodes, int *flag_knn, int *kNN, ECLgraph *g,
+                             MSTedge *mst_edges, long int *auxiliar_edges, long int *offsets,
+                             float *euclidean_distance, float *distance);
+void core_sg_calculate_MRD_mst(ECLgraph *g, long int *auxiliar_edges, MSTedge *mst_edges,
+                               long int nodes, float *euclidean_distance_);
+void update_core_sg_weights(ECLgraph *g, int nodes, long int mpts);
 
 static int check(const char *what) {
   cudaError_t e = cudaDeviceSynchronize();
@@ -274,6 +317,100 @@ int ref_mst_gpu(const long *nindex, const int *nlist, const float *ew, long n,
   gg.nlist = nullptr;
   gg.eweight = nullptr;
   return 0;
+}
+
+// build_CoreSG's graph (core-sg.cu:477-571 with mst_gpu = 0): Union_kNNG_MST
+// (core-sg.cu:292-420) on the kNN graph and its sorted MST, then
+// update_core_sg_weights (core-sg.cu:432-471), which leaves the Euclidean
+// weights in eweight.  Union_kNNG_MST's body runs here step by step because
+// its MRD pass (calculateMutualReachabilityDistance, calculates.cu:199-273)
+// loops over three GPUs; the MRD kernel it launches (calculateMRD) runs once
+// over all edges instead.  Its MRD weights are overwritten by
+// update_core_sg_weights and are not part of the result.  The mutual flags
+// come from calculate_nindex (calculates.cu:286-333), as buildEnhancedKNNG
+// writes them.  Outputs are malloc'd; free with ref_free.
+long ref_core_sg(const int *ids_in, const float *dist_in, const float *X, long n, int d,
+                 int kk, const MSTedge *mst_in, long **nindex_out, int **nlist_out,
+                 float **ew_out) {
+  if (kk != k) {
+    fprintf(stderr, "reference compiled with k = %d\n", k);
+    return -1;
+  }
+  g_vectors = X;
+  g_dim = d;
+  g_ids = ids_in;
+  g_dist = dist_in;
+  g_n = n;
+  long vectorSize = n * (long)k;
+  int *kNN = new int[vectorSize];
+  float *distances = new float[vectorSize];
+  memcpy(kNN, ids_in, vectorSize * sizeof(int));
+  memcpy(distances, dist_in, vectorSize * sizeof(float));
+  // the mutual flags (write_bool_dict keeps them); no antihubs needed for them
+  {
+    ECLgraph t;
+    t.nindex = (long *)calloc(n + 1, sizeof(long));
+    int *flag_tmp = (int *)malloc(vectorSize * sizeof(int));
+    int no_antihub = -1;
+    calculate_nindex((int)n, kNN, flag_tmp, &t, &no_antihub, 0);
+    free(flag_tmp);
+    free(t.nindex);
+  }
+  int *flag_knn = read_bool_dict();
+  MSTedge *mst_edges = (MSTedge *)malloc((n - 1) * sizeof(MSTedge));
+  memcpy(mst_edges, mst_in, (n - 1) * sizeof(MSTedge));
+  // Union_kNNG_MST (core-sg.cu:292-420)
+  ECLgraph g;
+  g.nodes = (int)n;
+  cudaMallocManaged(&g.nindex, (n + 1) * sizeof(long));
+  memset(g.nindex, 0, (n + 1) * sizeof(long));
+  core_sg_calculate_nindex(n, flag_knn, kNN, &g, mst_edges);
+  long *offsets, *auxiliar_edges;
+  cudaMallocManaged(&offsets, n * sizeof(long));
+  cudaMallocManaged(&auxiliar_edges, n * sizeof(long));
+  memset(auxiliar_edges, 0, n * sizeof(long));
+  cudaMallocManaged(&g.nlist, g.nindex[n] * sizeof(int));
+  g.edges = g.nindex[n];
+  float *euclidean_distance = new float[g.edges];
+  core_sg_calculate_nlist(n, flag_knn, kNN, &g, mst_edges, auxiliar_edges, offsets,
+                          euclidean_distance, distances);
+  int *aux_nodes;
+  cudaMallocManaged(&aux_nodes, g.edges * sizeof(int));
+  createNodeList(aux_nodes, &g);
+  if (check("createNodeList")) return -1;
+  float *coreDistances;
+  cudaMallocManaged(&coreDistances, n * sizeof(float));
+  calculateCoreDistance(distances, coreDistances, n, k, mpts - 1);
+  cudaMallocManaged(&g.eweight, g.edges * sizeof(float));
+  calculateMRD<<<(unsigned)(g.edges / blockSize + 1), blockSize>>>(g.eweight, aux_nodes, g.nlist,
+                                                                   coreDistances, g.edges);
+  if (check("calculateMRD")) return -1;
+  core_sg_calculate_MRD_mst(&g, offsets, mst_edges, n, euclidean_distance);
+  write_euclidean_distance_vecs(euclidean_distance, g.edges);
+  delete[] euclidean_distance;
+  cudaFree(aux_nodes);
+  cudaFree(coreDistances);
+  cudaFree(offsets);
+  cudaFree(auxiliar_edges);
+  // update_core_sg_weights (core-sg.cu:432-471), unmodified: eweight becomes
+  // the Euclidean weights kept above
+  update_core_sg_weights(&g, (int)n, mpts);
+  if (check("update_core_sg_weights")) return -1;
+  long E = g.edges;
+  *nindex_out = (long *)malloc((n + 1) * sizeof(long));
+  *nlist_out = (int *)malloc(E * sizeof(int));
+  *ew_out = (float *)malloc(E * sizeof(float));
+  memcpy(*nindex_out, g.nindex, (n + 1) * sizeof(long));
+  memcpy(*nlist_out, g.nlist, E * sizeof(int));
+  memcpy(*ew_out, g.eweight, E * sizeof(float));
+  free(g.eweight);  // the array read_euclidean_distance_vecs handed over
+  cudaFree(g.nindex);
+  cudaFree(g.nlist);
+  free(mst_edges);
+  free(flag_knn);
+  delete[] kNN;
+  delete[] distances;
+  return E;
 }
 
 void ref_free(void *p) { free(p); }

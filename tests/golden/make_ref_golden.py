@@ -8,10 +8,23 @@ fill kernels).  Usage on a machine with a GPU, from the repository root:
 
     python tests/golden/make_ref_golden.py OUTDIR
     python tests/golden/make_ref_golden.py --add-mst-gpu OUTDIR
+    python tests/golden/make_ref_golden.py --add-core-sg OUTDIR
+    python tests/golden/make_ref_golden.py --nndescent-recall [--cg] OUTDIR
 
 The second form adds the reference's mst_gpu = 1 MST (int-quantised weights,
 gpuMST, buildMST_gpu) of every committed fixture's enhanced graph as
 `mstgpu` / `mstgpu_mult`, leaving the fixture's other arrays as they are.
+The third adds the reference's core-SG (Union_kNNG_MST + update_core_sg_weights
+on the fixture's kNN graph and sorted MST) as `coresg_nindex` /
+`coresg_nlist` / `coresg_eweight`, and, for the d = 12 fixture, the
+reference's initial NN-Descent graph (gpuknn::NNDescent with 0 iterations) as
+`ref_init_ids` / `ref_init_dist`.
+The fourth runs the reference's NN-Descent (6 iterations, VEC_DIM = 12) on
+d = 12 point sets up to the 100,000-point blob configuration and writes the
+recall@32 of its graph, of the oracle's restatement and the rows holding a
+repeated id to ref_nndescent_recall[_cg].json; --cg uses the build whose global
+loads bypass L1 (oracle/ref/Makefile, libhdbref_cg.so).  Run it once per
+library, each in its own process (both libraries export the same symbols).
 
 The kNN graphs fed to the reference come from the oracle's NN-Descent (with
 fix_distances applied), so every later stage sees one shared input.  The
@@ -48,8 +61,8 @@ def grid_points(n, seed):
     return rng.integers(0, 12, size=(n, 2)).astype(np.float32)
 
 
-def load_ref():
-    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libhdbref.so"), mode=C.RTLD_GLOBAL)
+def load_ref(name="libhdbref.so"):
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", name), mode=C.RTLD_GLOBAL)
     P = C.c_void_p
     L.ref_enhanced_knng.restype = C.c_long
     L.ref_enhanced_knng.argtypes = [P, P, P, C.c_long, C.c_int, C.c_int, P, P, P, P, P]
@@ -59,6 +72,8 @@ def load_ref():
     L.ref_nndescent.argtypes = [P, C.c_long, C.c_int, C.c_int, P]
     L.ref_mst_gpu.restype = C.c_int
     L.ref_mst_gpu.argtypes = [P, P, P, C.c_long, C.c_char_p, P, P]
+    L.ref_core_sg.restype = C.c_long
+    L.ref_core_sg.argtypes = [P, P, P, C.c_long, C.c_int, C.c_int, P, P, P, P]
     L.ref_free.argtypes = [P]
     return L
 
@@ -161,14 +176,92 @@ def add_mst_gpu(L, outdir):
         print(name, "mst_gpu multiplier", mult, flush=True)
 
 
+def ref_core_sg(L, ids, dist, X, mst):
+    """The reference's core-SG rows and Euclidean weights (ref_driver.cu)."""
+    n, d = X.shape
+    pn, pl, pw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    E = L.ref_core_sg(p(np.ascontiguousarray(ids, np.int32)), p(np.ascontiguousarray(dist, np.float32)),
+                      p(np.ascontiguousarray(X, np.float32)), n, d, 32,
+                      p(np.ascontiguousarray(mst, MST_EDGE)), C.byref(pn), C.byref(pl), C.byref(pw))
+    assert E > 0, "reference core-SG failed"
+    return (take(L, pn, n + 1, C.c_long).astype(np.int64), take(L, pl, E, C.c_int),
+            take(L, pw, E, C.c_float))
+
+
+def ref_graph(L, X, iterations):
+    """gpuknn::NNDescent (VEC_DIM = 12) on X: (decoded ids, distances)."""
+    n, d = X.shape
+    G = np.zeros((n, 32, 2), np.int32)
+    assert L.ref_nndescent(p(np.ascontiguousarray(X, np.float32)), n, d, iterations, p(G)) == 0
+    ids = G[:, :, 1].copy()
+    return np.where(ids < 0, -ids - 1, ids).astype(np.int32), G[:, :, 0].copy().view(np.float32)
+
+
+def rows_with_repeats(ids):
+    s = np.sort(ids, axis=1)
+    return int((s[:, 1:] == s[:, :-1]).any(axis=1).sum())
+
+
+def add_core_sg(L, outdir):
+    import glob
+    for f in sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "ref_*.npz"))):
+        d = dict(np.load(f))
+        name = os.path.basename(f)[4:-4]
+        d["coresg_nindex"], d["coresg_nlist"], d["coresg_eweight"] = ref_core_sg(
+            L, d["ids"], d["dist"], d["X"], d["mst_32"])
+        if d["X"].shape[1] == 12:
+            d["ref_init_ids"], d["ref_init_dist"] = ref_graph(L, d["X"], 0)
+        np.savez_compressed(os.path.join(outdir, os.path.basename(f)), **d)
+        print(name, "core-SG edges", len(d["coresg_nlist"]), flush=True)
+
+
+def nndescent_sets():
+    """d = 12 point sets for the NN-Descent comparison: the 1,500-point
+    fixture, 20,000 points of 20 blobs, and the 100,000-point configuration
+    (10 blobs, centres in [-10, 10]^12, sigma 1, 5 % noise)."""
+    from gpu_hdbscan_b200 import synth
+    fx = np.load(os.path.join(ROOT, "tests", "golden", "ref_blobs_d12.npz"))["X"]
+    return [("ref_blobs_d12", fx, None),
+            ("blobs_20k_d12", blobs(20000, 12, 19, blobs=20), None),
+            ("blobs_100k_d12", synth.generate(synth.WORKLOADS["blobs_100k_d12"]), 3000)]
+
+
+def nndescent_recall(L, outdir, tag):
+    out = {"library": tag, "k": 32, "sample_num": 16, "iterations": 6, "sets": {}}
+    for name, X, nq in nndescent_sets():
+        X = np.ascontiguousarray(X, np.float32)
+        n = len(X)
+        q = np.arange(n) if nq is None else np.random.default_rng(5).choice(n, nq, replace=False)
+        q = np.sort(q)
+        gt, _ = O.bruteforce_knn(X, 32, q)
+        rids, _ = ref_graph(L, X, 6)
+        oids, _ = O.nndescent(X, 32, 16, 6)
+        out["sets"][name] = {
+            "n": n, "queries": "all rows" if nq is None else f"{nq} rows, default_rng(5) choice",
+            "ref_recall32": O.recall(rids[q], gt, 32),
+            "ref_rows_with_repeated_ids": rows_with_repeats(rids),
+            "oracle_recall32": O.recall(oids[q], gt, 32)}
+        print(name, out["sets"][name], flush=True)
+    with open(os.path.join(outdir, f"ref_nndescent_recall{'_cg' if tag.endswith('_cg.so') else ''}.json"),
+              "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     outdir = args[0] if args else os.path.join(ROOT, "tests", "golden")
     os.makedirs(outdir, exist_ok=True)
     O.build()
+    if "--nndescent-recall" in sys.argv:
+        name = "libhdbref_cg.so" if "--cg" in sys.argv else "libhdbref.so"
+        nndescent_recall(load_ref(name), outdir, name)
+        return
     L = load_ref()
     if "--add-mst-gpu" in sys.argv:
         add_mst_gpu(L, outdir)
+        return
+    if "--add-core-sg" in sys.argv:
+        add_core_sg(L, outdir)
         return
     for case in CASES:
         run_case(L, *case, outdir)

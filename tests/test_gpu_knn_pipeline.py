@@ -107,7 +107,30 @@ def test_full_run_labels_are_consistent_with_its_own_graph_quality(ctx, oracle):
     assert adjusted_rand_score(lab[keep], got[keep]) > 0.99
 
 
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_full_run_labels_equal_oracle_on_its_own_graph(ctx, oracle, prec):
+    """hdb_run end to end (hdb_run_with_graph): the labels equal the oracle's
+    HDBSCAN of the very kNN graph the same call built -- with device buffers
+    and with host buffers (host_io, copies inside the call)."""
+    import torch
+    from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32
+    pc = HDB_PREC_BF16 if prec == "bf16" else HDB_PREC_FP32
+    X = blobs(4000, 12, seed=3)
+    Xd = torch.from_numpy(X).cuda()
+    for src in (Xd, X):
+        labels, st, G = ctx.hdbscan(src, k=32, mpts=32, precision=pc, want_graph=True)
+        assert labels.is_cuda == (src is Xd) and G.is_cuda == (src is Xd)
+        g = _t(G)
+        ids = np.where(g[:, :, 1] < 0, -g[:, :, 1] - 1, g[:, :, 1]).astype(np.int32)
+        assert oracle.validate_knn(ids)
+        _, ref, ncl = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 32)
+        np.testing.assert_array_equal(_t(labels), ref)
+        assert st["num_clusters"] == ncl and ncl >= 2
+
+
 def test_pipeline_device_and_host_io_agree(ctx):
+    """hdb_run_knn on one graph gives the same labels with device and with
+    host buffers."""
     import torch
     X = blobs(4000, 12, seed=3)
     Xd = torch.from_numpy(X).cuda()
@@ -116,126 +139,3 @@ def test_pipeline_device_and_host_io_agree(ctx):
     lh, _ = ctx.hdbscan_from_knn(G.cpu(), X)
     assert not lh.is_cuda
     np.testing.assert_array_equal(lh.numpy(), _t(ld))
-    lr, st = ctx.hdbscan(X)  # full path with host buffers
-    assert not lr.is_cuda and lr.shape == (4000,) and st["num_clusters"] >= 1
-
-
-def test_invalid_knn_graphs_are_rejected(ctx):
-    from gpu_hdbscan_b200 import HdbError
-    rng = np.random.default_rng(1)
-    n, k = 200, 8
-    X = rng.normal(size=(n, 3)).astype(np.float32)
-    ids = np.stack([rng.choice(np.delete(np.arange(n), i), k, replace=False) for i in range(n)])
-    dist = np.ones((n, k), np.float32)
-    bad = ids.copy(); bad[3, 2] = bad[3, 1]
-    with pytest.raises(HdbError, match="repeats"):
-        ctx.buildEnhancedKNNG(bad, dist, X)
-    bad = ids.copy(); bad[5, 0] = 5
-    with pytest.raises(HdbError, match="own id"):
-        ctx.buildEnhancedKNNG(bad, dist, X)
-    bad = ids.copy(); bad[7, 3] = n
-    with pytest.raises(HdbError, match="outside"):
-        ctx.buildEnhancedKNNG(bad, dist, X)
-    g = ctx.buildEnhancedKNNG(ids, dist, X)  # the context still works
-    assert g.edges > 0
-
-
-def test_disconnected_graph_is_reported(ctx):
-    """Two groups whose kNN lists stay inside the group; every antihub falls in
-    the first group (ties broken by index), so the second is unreachable --
-    the reference exits with "MST montada incorretamente" (mst.cu:317-323)."""
-    from gpu_hdbscan_b200 import HdbError, _lib
-    n, k = 100, 4
-    ids = np.zeros((n, k), np.int32)
-    for g0 in (0, 50):
-        for i in range(50):
-            ids[g0 + i] = [g0 + (i + s) % 50 for s in (1, 2, 3, 4)]
-    X = np.random.default_rng(0).normal(size=(n, 2)).astype(np.float32)
-    dist = np.ones((n, k), np.float32)
-    g = ctx.buildEnhancedKNNG(ids, dist, X)
-    assert (g.antihubs.cpu().numpy() < 50).all()
-    with pytest.raises(HdbError) as e:
-        ctx.buildMST(g)
-    assert e.value.status == _lib.HDB_ERR_DISCONNECTED
-
-
-def test_small_and_edge_sizes(ctx, oracle):
-    """n just above k, k < 32, and mpts = 2.  Overlapping blobs: with separated
-    ones the exact 8-NN graph of 100 points already falls apart, and whether the
-    antihub clique joins the pieces depends on which points the approximate
-    graph leaves with the lowest in-degree (the reference then fails with
-    "MST montada incorretamente", as this library does with
-    HDB_ERR_DISCONNECTED)."""
-    for n, k, mpts in [(40, 32, 32), (100, 8, 8), (33, 32, 2), (500, 16, 16)]:
-        X = blobs(n, 3, seed=n, spread=2.5)
-        G = ctx.NNDescent(X, k=k, sample_num=k // 2)
-        labels, _ = ctx.hdbscan_from_knn(G, X, k=k, mpts=mpts)
-        ids = _t(ctx.knn_split(G)[0])
-        fd = oracle.fix_distances(X, ids)
-        _, ref, _ = oracle.hdbscan_from_knn(ids, fd, X, mpts)
-        np.testing.assert_array_equal(_t(labels), ref)
-        lab2, _ = ctx.hdbscan(X, k=k, mpts=mpts, sample_num=k // 2)
-        assert lab2.shape == (n,)
-
-
-def test_argument_errors(ctx):
-    from gpu_hdbscan_b200 import HdbError
-    X = blobs(500, 4, seed=1)
-    with pytest.raises(HdbError, match="mpts"):
-        ctx.hdbscan(X, k=16, mpts=1, sample_num=8)
-    with pytest.raises(HdbError, match="SAMPLE_NUM"):
-        ctx.hdbscan(X, k=16, sample_num=9)
-    with pytest.raises(HdbError, match="k"):
-        ctx.hdbscan(X, k=64)
-
-
-@pytest.mark.parametrize("n,d", [(6000, 128), (5000, 12), (4000, 96)])
-def test_bf16_nndescent_graph_is_valid_and_reranked_exactly(ctx, oracle, n, d):
-    """BF16 tensor-core candidate distances, then an FP32 re-rank: the graph
-    handed on is valid, sorted, and carries the exact FP32 difference sums."""
-    from gpu_hdbscan_b200 import HDB_PREC_BF16
-    X = blobs(n, d, seed=31 + d, blobs=10, spread=20.0)
-    G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=HDB_PREC_BF16)
-    ids, dist = (_t(a) for a in ctx.knn_split(G))
-    assert oracle.validate_knn(ids)
-    key = dist.view(np.uint32).astype(np.uint64) << np.uint64(32) | ids.astype(np.uint64)
-    assert (np.diff(key, axis=1) > 0).all()
-    rng = np.random.default_rng(1)
-    for i in rng.choice(n, 100, replace=False):
-        for j in range(0, 32, 3):
-            assert np.float32(oracle.diffsum(X[i], X[ids[i, j]])).view(np.uint32) == \
-                dist[i, j].view(np.uint32)
-
-
-@pytest.mark.parametrize("d", [128, 64])
-def test_bf16_recall_matches_fp32_form(ctx, oracle, d):
-    """Recall@32 of the BF16 form within 0.5 pt of the plain FP32 form (the
-    benchmark's 'equal recall@k' condition) on the 20M x 128 workload's
-    distribution (blob centres in [-20, 20], sigma in [0.5, 1.5]) at 30,000
-    points, in 128 and in 64 dimensions."""
-    from dataclasses import replace
-
-    from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
-    w = synth.scaled("blobs_20m_d128", 30000)
-    X = synth.generate(w if d == 128 else replace(w, d=d, seed=5))
-    # every row is a query: two independent NN-Descent runs differ by a few
-    # tenths of a point on a subsample, which this comparison must not see
-    q = np.arange(len(X))
-    gt, _ = oracle.bruteforce_knn(X, 32, q)
-    rec = {}
-    for name, prec in (("fp32", HDB_PREC_FP32), ("bf16", HDB_PREC_BF16)):
-        G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=prec)
-        rec[name] = oracle.recall(_t(ctx.knn_split(G)[0])[q], gt, 32)
-    assert rec["bf16"] >= rec["fp32"] - 0.005, rec
-
-
-def test_bf16_pipeline_labels_identical_on_shared_graph(ctx, oracle):
-    from gpu_hdbscan_b200 import HDB_PREC_BF16
-    X = blobs(6000, 64, seed=41, blobs=8, spread=20.0)
-    G = ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=HDB_PREC_BF16)
-    labels, stats = ctx.hdbscan_from_knn(G, X, k=32, mpts=32)
-    ids = _t(ctx.knn_split(G)[0])
-    _, ref, ncl = oracle.hdbscan_from_knn(ids, oracle.fix_distances(X, ids), X, 32)
-    np.testing.assert_array_equal(_t(labels), ref)
-    lab2, st2 = ctx.hdbscan(X, precision=HDB_PREC_BF16)
-    assert st2["num_clusters"] >= 2
