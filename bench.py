@@ -240,6 +240,59 @@ def default_cpu_sample(w):
     return 100_000 if w.d <= 16 else 50_000
 
 
+def cpu_reference_legs(X, k, mpts):
+    """The CPU path the reference validates against, timed on the host cores:
+    (i) its ground-truth kNN, which it reads from exact brute-force files
+    (HDBSCAN/cmake/eval.py:57) -- stood in for by scipy's cKDTree (d <= 12) or
+    a blocked FP64 brute force (d > 12), and (ii) the CPU HDBSCAN its labels
+    are checked against (PyPI hdbscan, prims_kdtree / EOM,
+    HDBSCAN/groundtruth/groundtruth.py:115-119; not installable here) --
+    stood in for by sklearn.cluster.HDBSCAN with the same min_cluster_size,
+    min_samples and EOM selection.  Returns both legs in points/s."""
+    import numpy as np
+    n, d = X.shape
+    t0 = time.perf_counter()
+    if d <= 12:
+        from scipy.spatial import cKDTree
+        cKDTree(X).query(X, k=k + 1, workers=-1)
+        knn_method = "scipy cKDTree(workers=-1), k+1 nearest per point"
+    else:
+        X64 = X.astype(np.float64)
+        nrm = (X64 * X64).sum(1)
+        for s0 in range(0, n, 2048):
+            D = nrm[s0:s0 + 2048, None] + nrm[None, :] - 2.0 * (X64[s0:s0 + 2048] @ X64.T)
+            np.argpartition(D, k + 1, axis=1)[:, :k + 1]
+        knn_method = "blocked FP64 brute force (numpy BLAS), k+1 nearest per point"
+    t1 = time.perf_counter()
+    import warnings
+    from sklearn.cluster import HDBSCAN
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        HDBSCAN(min_cluster_size=mpts, min_samples=mpts, cluster_selection_method="eom",
+                n_jobs=-1).fit(X)
+    t2 = time.perf_counter()
+    return {"exact_knn": {"value": n / (t1 - t0), "unit": UNIT, "method": knn_method},
+            "cpu_hdbscan": {"value": n / (t2 - t1), "unit": UNIT,
+                            "method": f"sklearn.cluster.HDBSCAN(min_cluster_size={mpts}, "
+                                      f"min_samples={mpts}, cluster_selection_method='eom', "
+                                      "n_jobs=-1), stand-in for PyPI hdbscan prims_kdtree"},
+            "knn_plus_hdbscan": {"value": n / (t2 - t0), "unit": UNIT},
+            "sample_points": n, "cores": len(os.sched_getaffinity(0))}
+
+
+def add_reference_legs(cb, w):
+    """Adds the reference's CPU ground-truth kNN + CPU HDBSCAN legs to a CPU
+    baseline record, on a sample of the workload's mixture sized to run in
+    seconds (sklearn's HDBSCAN grows faster than linearly)."""
+    from gpu_hdbscan_b200 import synth
+    try:
+        cb["legs"] = cpu_reference_legs(synth.sample(w, 20_000 if w.d <= 16 else 5_000),
+                                        w.k, w.mpts)
+    except Exception as e:  # report, never lose the line
+        cb["legs"] = {"error": f"{type(e).__name__}: {e}"}
+    return cb
+
+
 def run_reference(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -247,7 +300,7 @@ def run_reference(args, w):
     n_s = args.cpu_sample or default_cpu_sample(w)
     for _ in range(args.warmup):
         pass  # the CPU port has no warm-up state; warm-up steps are not repeated work
-    cb = cpu_baseline_run(w, n_s, max(1, args.steps))
+    cb = add_reference_legs(cpu_baseline_run(w, n_s, max(1, args.steps)), w)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -391,7 +444,8 @@ def run_ours(args, w):
         cb = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                cb = cpu_baseline_run(w, args.cpu_sample or default_cpu_sample(w), 1)
+                cb = add_reference_legs(
+                    cpu_baseline_run(w, args.cpu_sample or default_cpu_sample(w), 1), w)
             except Exception as e:  # report, never lose the GPU line
                 cb = {"error": f"{type(e).__name__}: {e}"}
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
@@ -455,6 +509,15 @@ def cpu_batch_run(bw, Xs):
                       f"each, oracle port (NN-Descent + enhanced kNNG + Kruskal + trees)"}
 
 
+def batch_reference_legs(bw, Xs):
+    """The reference's CPU ground-truth kNN + CPU HDBSCAN legs on the first
+    instance of the CPU sample (at most 20,000 of its points)."""
+    try:
+        return cpu_reference_legs(Xs[0][:20_000], bw.k, bw.mpts)
+    except Exception as e:
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def run_reference_batch(args, bw):
     from gpu_hdbscan_b200 import synth
     if int(os.environ.get("RANK", "0")) != 0:
@@ -464,6 +527,7 @@ def run_reference_batch(args, bw):
     vals = [cpu_batch_run(bw, Xs) for _ in range(max(1, args.steps))]
     cb = vals[-1]
     cb["value"] = statistics.median(v["value"] for v in vals)
+    cb["legs"] = batch_reference_legs(bw, Xs)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -615,7 +679,9 @@ def run_ours_batch(args, bw):
         cb = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                cb = cpu_batch_run(rbw, batch_cpu_sample(rbw, layout))
+                Xs_cpu = batch_cpu_sample(rbw, layout)
+                cb = cpu_batch_run(rbw, Xs_cpu)
+                cb["legs"] = batch_reference_legs(rbw, Xs_cpu)
             except Exception as e:
                 cb = {"error": f"{type(e).__name__}: {e}"}
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,

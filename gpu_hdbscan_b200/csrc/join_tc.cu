@@ -13,23 +13,31 @@
 // in the SIMT BF16 join.
 //
 // Warp roles (224 threads, a persistent loop over tiles):
-//   warps 4, 5  producers (alternate tiles): slot lists, TMA gathers of the
-//               rows, cp.async of their norms and worst[] into the stage; a
-//               TMA gather occupies its issuing warp for a while, so two
-//               warps keep more gathers in flight;
-//   warp 6      one thread issues the MMAs and commits them to mbarriers;
+//   warps 4, 5  producers (alternate tiles): slot lists into the tile's
+//               metadata slot (ids, nn / no, cp.async of the rows' norms and
+//               worst[]), then TMA gathers of the rows, one 64-element K block
+//               of the tile per operand stage; a TMA gather occupies its
+//               issuing warp for a while, so two warps keep more gathers in
+//               flight;
+//   warp 6      one thread issues the MMAs, K block by K block, and commits
+//               each operand stage back to its producer as soon as the MMAs
+//               reading it are done, and the finished tile to the epilogue;
 //   warps 0..3  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//               lanes 32w..32w+31 = tile rows), row minima, and the
-//               candidates appended to the target-sorted list of the merge
-//               (one reservation per warp and tile; the per-row inboxes of
-//               the SIMT joins would cost a returning atomic per candidate).
-// Stages form a ring of three (full / empty mbarriers); accumulators a ring
-// of two (acc_full / acc_empty).  Every wait is bounded in time: a wait that
-// gives up sets DEVERR_TIMEOUT and makes every role of the CTA stop, after
-// which the CTA still waits (bounded) for its own copies and MMAs before it
-// frees its tensor memory and exits.  tcgen05.ld / alloc are .sync.aligned:
-// the warp is reconverged with __syncwarp() right before each, because the
-// code ahead of them branches per lane.
+//               lanes 32w..32w+31 = tile rows), row minima against the
+//               metadata slot, and the candidates appended to the
+//               target-sorted list of the merge (one reservation per warp and
+//               tile; the per-row inboxes of the SIMT joins would cost a
+//               returning atomic per candidate).
+// Three rings, each with full / empty mbarriers: operand stages (one K block
+// of a tile each, held only from the gather to the end of its MMAs), metadata
+// slots (held until the epilogue is done with the tile) and two
+// accumulators.  A stage is therefore not held while the epilogue works,
+// which keeps more gathers in flight per SM.  Every wait is bounded in time:
+// a wait that gives up sets DEVERR_TIMEOUT and makes every role of the CTA
+// stop, after which the CTA still waits (bounded) for its own copies and MMAs
+// before it frees its tensor memory and exits.  tcgen05.ld / alloc are
+// .sync.aligned: the warp is reconverged with __syncwarp() right before each,
+// because the code ahead of them branches per lane.
 //
 // Row minima: each distance is clamped at 0 and its float bits (order-preserving
 // for non-negative floats) have their low 6 bits replaced by the column, so one
@@ -50,8 +58,9 @@ using namespace knn;
 
 namespace {
 
-constexpr int kStages = 3;
-constexpr int kKBlockBytes = kTcTileRows * 128;  // one 64-element K block of a stage
+constexpr int kStages = 6;    // operand stages (one 64-element K block of a tile each)
+constexpr int kMetaSlots = 8; // tile metadata slots
+constexpr int kKBlockBytes = kTcTileRows * 128;  // one 64-element K block of a tile
 constexpr int kAccCols = 128;                     // FP32 accumulator columns (N)
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kEpiWarps = 4;
@@ -59,8 +68,7 @@ constexpr int kProducers = 2;  // producer warps, alternating tiles
 constexpr int kProducerWarp0 = kEpiWarps;
 constexpr int kMmaWarp = kProducerWarp0 + kProducers;
 constexpr int kThreads = 32 * (kMmaWarp + 1);
-constexpr uint32_t kFullArrivals = 1 + 32;          // expect_tx + one cp.async arrival per lane
-constexpr uint32_t kEmptyArrivals = 1 + kEpiWarps;  // MMA commit + epilogue warps
+constexpr uint32_t kMetaArrivals = 1 + 32;          // producer + one cp.async arrival per lane
 constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s
 constexpr uint32_t kNoKey = 0x7F800000u;            // keys at or above: no candidate
 // Shared memory is padded to at least this size so that no more than two
@@ -81,9 +89,12 @@ struct StageMeta {
 };
 
 struct Shared {
-  StageMeta meta[kStages];
-  unsigned long long full[kStages], empty[kStages], acc_full[2], acc_empty[2];
-  uint32_t armed[kStages];  // uses of each stage armed so far (for the drain)
+  StageMeta meta[kMetaSlots];
+  unsigned long long full[kStages], empty[kStages];        // operand stages
+  unsigned long long mfull[kMetaSlots], mempty[kMetaSlots];  // metadata slots
+  unsigned long long acc_full[2], acc_empty[2];
+  uint32_t armed[kStages];       // uses of each operand stage armed so far (for the drain)
+  uint32_t marmed[kMetaSlots];   // uses of each metadata slot armed so far
   uint32_t tmem_base;
   int abort;
 };
@@ -378,9 +389,11 @@ __device__ __forceinline__ int stage_probe(const JoinArgs &a, int64_t t, int j, 
 }
 
 // Producer p of the CTA stages the CTA's tiles i = p, p + kProducers, ...
-// (tile index blockIdx.x + i * gridDim.x): TMA gathers are issued lane by
-// lane and occupy the issuing warp, so several producer warps keep more of
-// them in flight.
+// (tile index blockIdx.x + i * gridDim.x): the tile's metadata into slot
+// i % kMetaSlots, then its rows, one K block per operand stage; stage
+// positions are i * kbc + kb around the ring, the order in which the MMA
+// thread consumes them.  TMA gathers are issued lane by lane and occupy the
+// issuing warp, so several producer warps keep more of them in flight.
 template <bool kProbe>
 __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shared &sh,
                          unsigned char *tiles, int64_t n, int64_t ntiles, int kbc, int S,
@@ -394,20 +407,20 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
     cur[1] = load_row(a, 2 * t + 1, n, S);
   }
   for (uint32_t i = p; t < ntiles; t += step, i += kProducers) {
-    const int s = i % kStages;
-    const uint32_t use = i / kStages;
-    if (!__all_sync(0xffffffffu, mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort))) {
+    const int m = i % kMetaSlots;
+    const uint32_t muse = i / kMetaSlots;
+    if (!__all_sync(0xffffffffu, mbar_wait(&sh.mempty[m], (muse & 1) ^ 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }
-    StageMeta &m = sh.meta[s];
+    StageMeta &M = sh.meta[m];
     int nn[2], no[2], groups;
     if (kProbe) {
-      groups = stage_probe(a, t, 0, m, nn[0], no[0]);
-      groups += stage_probe(a, t, 1, m, nn[1], no[1]);
+      groups = stage_probe(a, t, 0, M, nn[0], no[0]);
+      groups += stage_probe(a, t, 1, M, nn[1], no[1]);
     } else {
-      groups = stage_join(a, cur[0], 0, m, nn[0], no[0]);
-      groups += stage_join(a, cur[1], 1, m, nn[1], no[1]);
+      groups = stage_join(a, cur[0], 0, M, nn[0], no[0]);
+      groups += stage_join(a, cur[1], 1, M, nn[1], no[1]);
       // this warp's next tile: its lists are in flight while this one is gathered
       const int64_t tn = t + step;
       if (tn < ntiles) {
@@ -416,26 +429,42 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
       }
     }
     rows_staged += nn[0] + no[0] + nn[1] + no[1];
-    __syncwarp();
-    if (lane == 0) mbar_arrive_tx(&sh.full[s], (uint32_t)groups * kbc * 512u);
-    __syncwarp();
-    {
-      // lane g: four-row group g & 15 of row-join g >> 4 (new groups 0..7,
-      // old groups 8..15)
-      const int j = lane >> 4, q = lane & 15;
-      const bool oldg = q >= 8;
-      const int slot = oldg ? 32 + 4 * (q - 8) : 4 * q;
-      const int cnt = oldg ? no[j] : nn[j];
-      if (4 * (q & 7) < cnt) {
-        const int32_t *gi = m.ids + 64 * j + slot;
-        for (int kb = 0; kb < kbc; kb++) {
-          unsigned char *dst = tiles + ((size_t)s * kbc + kb) * kKBlockBytes + (64 * j + slot) * 128;
-          tma_gather4(dst, xmap, kb * kTcKBlock, gi[0], gi[1], gi[2], gi[3], &sh.full[s]);
-        }
+    __syncwarp();  // the slot's ids / counts are written (and read below by every lane)
+    cp_async_arrive_noinc(&sh.mfull[m]);
+    if (lane == 0) {
+      mbar_arrive(&sh.mfull[m]);
+      atomicAdd(&sh.marmed[m], 1u);
+    }
+    // lane g: four-row group g & 15 of row-join g >> 4 (new groups 0..7,
+    // old groups 8..15)
+    const int j = lane >> 4, q = lane & 15;
+    const bool oldg = q >= 8;
+    const int slot = oldg ? 32 + 4 * (q - 8) : 4 * q;
+    const bool mine = 4 * (q & 7) < (oldg ? no[j] : nn[j]);
+    const int32_t *gi = M.ids + 64 * j + slot;
+    bool ok = true;
+    for (int kb = 0; kb < kbc; kb++) {
+      const uint32_t g = i * (uint32_t)kbc + kb;
+      const int s = g % kStages;
+      const uint32_t use = g / kStages;
+      if (!__all_sync(0xffffffffu, mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort))) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        mbar_arrive_tx(&sh.full[s], (uint32_t)groups * 512u);
+        atomicAdd(&sh.armed[s], 1u);
+      }
+      __syncwarp();
+      if (mine) {
+        unsigned char *dst = tiles + (size_t)s * kKBlockBytes + (64 * j + slot) * 128;
+        tma_gather4(dst, xmap, kb * kTcKBlock, gi[0], gi[1], gi[2], gi[3], &sh.full[s]);
       }
     }
-    cp_async_arrive_noinc(&sh.full[s]);
-    if (lane == 0) atomicAdd(&sh.armed[s], 1u);
+    if (!ok) {
+      give_up(sh, a.err);
+      break;
+    }
     if (!kProbe) {
       cur[0] = nxt[0];
       cur[1] = nxt[1];
@@ -449,8 +478,6 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
   int last_b = -1;
   uint32_t last_parity = 0;
   for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
-    const int s = i % kStages;
-    const uint32_t use = i / kStages;
     const int b = i & 1;
     const uint32_t ub = i >> 1;
     if (!mbar_wait(&sh.acc_empty[b], (ub & 1) ^ 1, &sh.abort)) {
@@ -458,24 +485,31 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
       break;
     }
     tc_fence_after();
-    if (!mbar_wait(&sh.full[s], use & 1, &sh.abort)) {
-      give_up(sh, err);
-      break;
-    }
-    tc_fence_after();
     const uint32_t d = tmem + (uint32_t)(b * kAccCols);
+    int issued = 0;
     for (int kb = 0; kb < kbc; kb++) {
-      const uint32_t base = smem_u32(tiles + ((size_t)s * kbc + kb) * kKBlockBytes);
+      const uint32_t g = i * (uint32_t)kbc + kb;
+      const int s = g % kStages;
+      if (!mbar_wait(&sh.full[s], (g / kStages) & 1, &sh.abort)) break;
+      issued++;
+      tc_fence_after();
+      const uint32_t base = smem_u32(tiles + (size_t)s * kKBlockBytes);
 #pragma unroll
       for (int kk = 0; kk < kTcKBlock / 16; kk++) {
         const uint64_t desc = sw128_desc(base + 32u * kk);
         tc_mma(d, desc, desc, (kb | kk) != 0 ? 1u : 0u);
       }
+      tc_commit(&sh.empty[s]);  // the stage goes back once these MMAs are done
     }
-    tc_commit(&sh.acc_full[b]);
-    tc_commit(&sh.empty[s]);
-    last_b = b;
-    last_parity = ub & 1;
+    if (issued > 0) {  // also after a give-up mid-tile: the drain below then covers it
+      tc_commit(&sh.acc_full[b]);
+      last_b = b;
+      last_parity = ub & 1;
+    }
+    if (issued < kbc) {
+      give_up(sh, err);
+      break;
+    }
   }
   // drain: the last MMA chain has completed before tensor memory is freed
   if (last_b >= 0 && !mbar_wait(&sh.acc_full[last_b], last_parity, nullptr))
@@ -512,15 +546,15 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
   const int slot = (isnew ? 0 : 32) + lane;
   int64_t t = blockIdx.x;
   for (uint32_t i = 0; t < ntiles; t += gridDim.x, i++) {
-    const int s = i % kStages;
-    const uint32_t use = i / kStages;
+    const int m = i % kMetaSlots;
+    const uint32_t muse = i / kMetaSlots;
     const int b = i & 1;
     const uint32_t ub = i >> 1;
-    if (!__all_sync(0xffffffffu, mbar_wait(&sh.full[s], use & 1, &sh.abort))) {
+    if (!__all_sync(0xffffffffu, mbar_wait(&sh.mfull[m], muse & 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }
-    const StageMeta &M = sh.meta[s];
+    const StageMeta &M = sh.meta[m];
     const int nn = M.nn[j], no = M.no[j];
     const bool vrow = isnew ? lane < nn : lane < no;
     const int32_t myid = M.ids[64 * j + slot];
@@ -551,7 +585,7 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
         o[32 + c] = __fmaf_rn(-2.0f, __uint_as_float(v1[c]), __fadd_rn(na, cn[32 + c]));
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&sh.empty[s]);
+      if (lane == 0) mbar_arrive(&sh.mempty[m]);
       continue;
     }
     uint32_t k1, k2 = 0xffffffffu;
@@ -565,7 +599,7 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     }
     if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sh.empty[s]);
+    if (lane == 0) mbar_arrive(&sh.mempty[m]);
     // candidates that can enter their target's list, appended to the list
     // that is sorted by target before the next merge: one reservation per
     // warp instead of a returning inbox atomic per candidate
@@ -582,24 +616,29 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ unsigned char smem_raw[];
   // the swizzled operand tiles start on a 1024-byte boundary of shared memory
   unsigned char *tiles = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  Shared &sh = *reinterpret_cast<Shared *>(tiles + (size_t)kStages * kbc * kKBlockBytes);
+  Shared &sh = *reinterpret_cast<Shared *>(tiles + (size_t)kStages * kKBlockBytes);
   const int warp = threadIdx.x >> 5;
   // stale columns of a stage must hold finite values: start from zeros
   {
     uint4 *z = reinterpret_cast<uint4 *>(tiles);
-    const int nz = kStages * kbc * kKBlockBytes / 16;
+    const int nz = kStages * kKBlockBytes / 16;
     for (int i = threadIdx.x; i < nz; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
   }
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&sh.full[s], kFullArrivals);
-      mbar_init(&sh.empty[s], kEmptyArrivals);
+      mbar_init(&sh.full[s], 1);   // the producer's expect_tx; the gathers complete it
+      mbar_init(&sh.empty[s], 1);  // the MMA thread's commit
+      sh.armed[s] = 0;
+    }
+    for (int m = 0; m < kMetaSlots; m++) {
+      mbar_init(&sh.mfull[m], kMetaArrivals);
+      mbar_init(&sh.mempty[m], kEpiWarps);
+      sh.marmed[m] = 0;
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&sh.acc_full[b], 1);
       mbar_init(&sh.acc_empty[b], kEpiWarps);
     }
-    for (int s = 0; s < kStages; s++) sh.armed[s] = 0;
     sh.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -640,6 +679,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t u = sh.armed[s];
       if (u > 0 && !mbar_wait(&sh.full[s], (u - 1) & 1, nullptr)) atomicOr(a.err, DEVERR_TIMEOUT);
     }
+    for (int m = 0; m < kMetaSlots; m++) {  // the norm / worst[] copies as well
+      const uint32_t u = sh.marmed[m];
+      if (u > 0 && !mbar_wait(&sh.mfull[m], (u - 1) & 1, nullptr)) atomicOr(a.err, DEVERR_TIMEOUT);
+    }
   }
   __syncthreads();
   if (warp == kMmaWarp) {
@@ -665,8 +708,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
   return fn;
 }
 
-size_t smem_bytes(int kbc) {
-  size_t b = 1024 + (size_t)kStages * kbc * kKBlockBytes + sizeof(Shared);
+size_t smem_bytes() {
+  size_t b = 1024 + (size_t)kStages * kKBlockBytes + sizeof(Shared);
   return b < kMinSmem ? kMinSmem : b;
 }
 
@@ -674,7 +717,7 @@ template <bool kProbe>
 void launch(Context *ctx, const TcJoin &tj, int64_t ntiles, int S, const JoinArgs &a) {
   const int kbc = tj.dpad / kTcKBlock;
   HDB_CUDA(cudaFuncSetAttribute(k_join_tc<kProbe>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes(kTcMaxDpad / kTcKBlock)));
+                                (int)smem_bytes()));
   const int64_t g = std::min<int64_t>(ntiles, 2 * (int64_t)ctx->num_sms);
   if (g <= 0) return;
   k_join_tc<kProbe><<<(int)g, kThreads, tj.smem, ctx->stream>>>(tj.xmap, tj.n, ntiles, kbc, S, a);
@@ -704,7 +747,7 @@ void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad,
               "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   tj->n = n;
   tj->dpad = dpad;
-  tj->smem = smem_bytes(dpad / kTcKBlock);
+  tj->smem = smem_bytes();
   (void)ctx;
 }
 

@@ -438,44 +438,107 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
   }
 }
 
+// ---- FP32 local join -----------------------------------------------------
+// Shared memory of one warp: best candidates (u64: best other-new and best old
+// per new row; best new per old row) | slot ids | one chunk of kJc dimensions
+// of every staged row.  Rows are staged a chunk at a time, so a warp needs
+// ~9 KB whatever d is and an SM keeps 16 warps of joins in flight.
+constexpr int kJc = 32;              // dimensions per staged chunk
+constexpr int kJoinTiles = 2;        // 4 x 4 register tiles per lane and pass (64 per pass)
+constexpr int kJoinWarps = 8;
 struct JoinSmem {
-  // layout per warp: best[96] (u64: best other-new, best old per new; best new
-  // per old) | ids[64] | X rows [64 * dp]
-  static constexpr int kBest = 96;  // u64 entries
+  static constexpr int kBest = 96;   // u64 entries
   static constexpr int kIds = 64;
-  __host__ __device__ static int floats(int dp) { return 2 * kBest + kIds + 64 * dp + 2; }
+  static constexpr size_t kBytes = kBest * 8 + kIds * 4 + (size_t)64 * kJc * 4;
 };
 
-// Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).  The
-// sampled rows are staged in shared memory (new rows at slots 0..31, old rows
-// at 32..63).  The distance matrix new x (new U old) is cut into 4 x 4 tiles
-// spread over the lanes; a lane keeps its 16 sums in registers, so each
-// dimension costs 8 shared loads for 16 pair updates, and every pair is the
-// reference's sequential FP32 difference sum.  Tile row/column minima go to
-// the per-neighbour best candidates with one 64-bit shared-memory atomicMin
-// each: every new neighbour gets its closest other new one and its closest old
-// one, every old neighbour its closest new one.  cross_only (the merge join,
-// TiledNewOldNeighborsCompareKernelForMerge :1328-1383 launched without the
-// new x new kernel, UpdateGraphForMerge :1582-1640) leaves out the new x new
-// tiles: new neighbours get their closest old one only.
-__device__ __forceinline__ const float *xs_row(const float *Xs, int r, int dp) {
-  return Xs + r * dp + (r >= 32 ? 1 : 0);  // old block shifted one bank
+// Float offset of 16-byte piece q of staged row r: the pieces of a row are
+// permuted by the row's group of four, so the rows one warp-wide 16-byte load
+// reads (one per tile group) fall into different bank groups.
+__device__ __forceinline__ int stage_off(int r, int q) { return r * kJc + ((q ^ ((r >> 2) & 7)) << 2); }
+
+// Stages dimensions [c0, c0 + 4 * nq) of the nn new rows (slots 0..) and the
+// no old rows (slots 32..): 16-byte cp.async copies when every row piece is
+// 16-byte aligned (d % 4 == 0), else scalar loads, zero padded to a multiple
+// of four (adding fmaf(0, 0, s) = s leaves every sum unchanged).
+__device__ __forceinline__ void stage_chunk(const float *__restrict__ X, int d, int c0, int nq,
+                                            const int32_t *ids, int nn, int no, float *Xs,
+                                            bool vec) {
+  const int lane = lane_id();
+  const int items = (nn + no) * nq;
+  if (vec) {
+    for (int it = lane; it < items; it += 32) {
+      const int r = it / nq, q = it - r * nq;
+      const int slot = r < nn ? r : 32 + (r - nn);
+      const float *src = X + (int64_t)ids[slot] * d + c0 + 4 * q;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(Xs + stage_off(slot, q));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  } else {
+    for (int it = lane; it < items; it += 32) {
+      const int r = it / nq, q = it - r * nq;
+      const int slot = r < nn ? r : 32 + (r - nn);
+      const float *src = X + (int64_t)ids[slot] * d;
+      float4 v;
+      const int c = c0 + 4 * q;
+      v.x = c < d ? __ldg(src + c) : 0.0f;
+      v.y = c + 1 < d ? __ldg(src + c + 1) : 0.0f;
+      v.z = c + 2 < d ? __ldg(src + c + 2) : 0.0f;
+      v.w = c + 3 < d ? __ldg(src + c + 3) : 0.0f;
+      *reinterpret_cast<float4 *>(Xs + stage_off(slot, q)) = v;
+    }
+  }
+  __syncwarp();
 }
 
-__global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64_t n, int d, int S,
-                       const int32_t *__restrict__ newS, const int32_t *__restrict__ oldS,
-                       const int8_t *__restrict__ nf, const int8_t *__restrict__ of,
-                       int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
-                       const float *__restrict__ worst, Inbox ib, int cross_only) {
-  extern __shared__ float smem_join[];
+// Tile t of a row-join with rg row groups (new rows), cgn new and cgo old
+// column groups: the new x new tiles are the upper triangle i <= j (a pair of
+// different groups is computed once and offered to both rows), then the new x
+// old tiles.  Returns the first slot of its rows (r0) and of its columns (c0)
+// and its kind: 1 diagonal, 2 above the diagonal, 3 old columns.
+__device__ __forceinline__ int tile_of(int t, int rg, int cgn, int cgo, int &r0, int &c0) {
+  const int tri = cgn > 0 ? rg * (rg + 1) / 2 : 0;
+  if (t < tri) {
+    int i = 0;
+    while (t >= rg - i) { t -= rg - i; i++; }
+    r0 = 4 * i;
+    c0 = 4 * (i + t);
+    return t == 0 ? 1 : 2;
+  }
+  t -= tri;
+  const int i = t / cgo;
+  r0 = 4 * i;
+  c0 = 32 + 4 * (t - i * cgo);
+  return 3;
+}
+
+// Local join, one warp per row (UpdateGraph, nndescent.cu:1487-1580).  The
+// distance matrix new x (new U old) is cut into 4 x 4 tiles, up to
+// kJoinTiles per lane; a lane keeps its tiles' sums in registers while the
+// rows pass through shared memory a chunk of kJc dimensions at a time, so
+// every pair is the reference's sequential FP32 difference sum over
+// j = 0..d-1.  Tile row/column minima go to the per-row best candidates with
+// one 64-bit shared-memory atomicMin each: every new neighbour gets its closest
+// other new one and its closest old one, every old neighbour its closest new
+// one.  cross_only (the merge join, TiledNewOldNeighborsCompareKernelForMerge
+// :1328-1383 launched without the new x new kernel, UpdateGraphForMerge
+// :1582-1640) leaves out the new x new tiles: new neighbours get their closest
+// old one only.
+__global__ void __launch_bounds__(32 * kJoinWarps, 2)
+    k_join(const float *__restrict__ X, int64_t n, int d, int S, const int32_t *__restrict__ newS,
+           const int32_t *__restrict__ oldS, const int8_t *__restrict__ nf,
+           const int8_t *__restrict__ of, int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
+           const float *__restrict__ worst, Inbox ib, int cross_only) {
+  extern __shared__ __align__(16) unsigned char smem_join[];
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
-  const int dp = (d & 1) ? d : d + 1;
-  float *base = smem_join + (threadIdx.x >> 5) * JoinSmem::floats(dp);
+  unsigned char *base = smem_join + (threadIdx.x >> 5) * JoinSmem::kBytes;
   unsigned long long *best = reinterpret_cast<unsigned long long *>(base);
   unsigned long long *best1 = best, *best2 = best + 32, *best3 = best + 64;
-  int32_t *ids = reinterpret_cast<int32_t *>(base + 2 * JoinSmem::kBest);
-  float *Xs = base + 2 * JoinSmem::kBest + JoinSmem::kIds;
+  int32_t *ids = reinterpret_cast<int32_t *>(base + JoinSmem::kBest * 8);
+  float *Xs = reinterpret_cast<float *>(base + JoinSmem::kBest * 8 + JoinSmem::kIds * 4);
+  const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   unsigned long long w_rows = 0, w_cands = 0;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
@@ -487,14 +550,14 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     // slot t < S: forward sample t; slot S + t: reverse sample t
     bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
     bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
-    int32_t nid = vn ? newS[sb + lane] : -1 - lane;
-    int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    const int32_t nid = vn ? newS[sb + lane] : -1 - lane;
+    const int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
     // de-duplicate (ShrinkGraph RemoveDuplicates, :285-291)
-    uint32_t pn = __match_any_sync(0xffffffffu, nid);
+    const uint32_t pn = __match_any_sync(0xffffffffu, nid);
     vn = vn && (__ffs(pn) - 1 == lane);
-    uint32_t po = __match_any_sync(0xffffffffu, oid);
+    const uint32_t po = __match_any_sync(0xffffffffu, oid);
     vo = vo && (__ffs(po) - 1 == lane);
-    uint32_t bo = __ballot_sync(0xffffffffu, vo);
+    const uint32_t bo = __ballot_sync(0xffffffffu, vo);
     const int no = __popc(bo);
     if (vo) ids[32 + __popc(bo & lanemask_lt())] = oid;
     __syncwarp();
@@ -505,7 +568,7 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
       for (int t = 0; t < no; t++) in_old |= ids[32 + t] == nid;
       vn = vn && !in_old;
     }
-    uint32_t bn = __ballot_sync(0xffffffffu, vn);
+    const uint32_t bn = __ballot_sync(0xffffffffu, vn);
     const int nn = __popc(bn);
     if (vn) ids[__popc(bn & lanemask_lt())] = nid;
     best1[lane] = ~0ull;
@@ -514,73 +577,91 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     __syncwarp();
     if (nn == 0 || nn + no < 2 || (cross_only && no == 0)) continue;
     w_rows += nn + no;
-    // stage rows
-    for (int idx = lane; idx < (nn + no) * d; idx += 32) {
-      int r = idx / d, c = idx - r * d;
-      int slot = r < nn ? r : 32 + (r - nn);
-      float *dst = const_cast<float *>(xs_row(Xs, slot, dp));
-      dst[c] = __ldg(X + (int64_t)ids[slot] * d + c);
-    }
-    __syncwarp();
-    const int rg = (nn + 3) >> 2;             // row groups (new rows)
+    const int rg = (nn + 3) >> 2;                              // row groups (new rows)
     const int cgn = cross_only ? 0 : rg, cgo = (no + 3) >> 2;  // column groups: new, old
-    const int cg = cgn + cgo;
-    const int tiles = rg * cg;
-    for (int t = lane; t < tiles; t += 32) {
-      const int r0 = (t / cg) * 4;
-      const int ci = t - (t / cg) * cg;
-      const bool oldcols = ci >= cgn;
-      const int c0 = oldcols ? 32 + (ci - cgn) * 4 : ci * 4;
-      const float *ra[4], *rc[4];
+    const int tiles = (cgn > 0 ? rg * (rg + 1) / 2 : 0) + rg * cgo;
+    // up to 64 tiles per pass through the rows (rows with more samples
+    // than that -- at most 100 tiles -- take a second pass)
+    for (int t0 = 0; t0 < tiles; t0 += 32 * kJoinTiles) {
+      int r0[kJoinTiles], c0[kJoinTiles], kind[kJoinTiles];
+      float acc[kJoinTiles][4][4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        ra[i] = xs_row(Xs, r0 + i, dp);
-        rc[i] = xs_row(Xs, c0 + i, dp);
-      }
-      float acc[4][4];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
-      for (int k2 = 0; k2 < d; k2++) {
-        float xa[4], xc[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) { xa[i] = ra[i][k2]; xc[i] = rc[i][k2]; }
+      for (int u = 0; u < kJoinTiles; u++) {
+        const int t = t0 + lane + 32 * u;
+        kind[u] = t < tiles ? tile_of(t, rg, cgn, cgo, r0[u], c0[u]) : 0;
+        if (kind[u] == 0) { r0[u] = 0; c0[u] = 0; }
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            float df = __fsub_rn(xa[i], xc[j]);
-            acc[i][j] = __fmaf_rn(df, df, acc[i][j]);
-          }
+          for (int j = 0; j < 4; j++) acc[u][i][j] = 0.0f;
       }
-      const int ncol = oldcols ? no : nn;
-      const int cbase = oldcols ? c0 - 32 : c0;  // column index within its block
-      uint64_t colmin[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+      for (int cd = 0; cd < d; cd += kJc) {
+        const int nq = (min(kJc, d - cd) + 3) >> 2;
+        __syncwarp();  // the previous chunk is no longer read
+        stage_chunk(X, d, cd, nq, ids, nn, no, Xs, vec);
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int a = r0 + i;
-        if (a >= nn) continue;
-        uint64_t rmin = ~0ull;
+        for (int u = 0; u < kJoinTiles; u++) {
+          if (kind[u] == 0) continue;
+          // the four rows of a tile side share one piece permutation
+          const int ka = (r0[u] >> 2) & 7, kc = (c0[u] >> 2) & 7;
+          for (int q = 0; q < nq; q++) {
+            const float *pa = Xs + r0[u] * kJc + ((q ^ ka) << 2);
+            const float *pc = Xs + c0[u] * kJc + ((q ^ kc) << 2);
+            float4 xc[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int c = cbase + j;
-          if (c >= ncol || (!oldcols && c == a)) continue;
-          const uint64_t kr = pack(acc[i][j], ids[c0 + j]);
-          rmin = kr < rmin ? kr : rmin;
-          if (oldcols) {
-            const uint64_t kc = pack(acc[i][j], ids[a]);
-            colmin[j] = kc < colmin[j] ? kc : colmin[j];
+            for (int j = 0; j < 4; j++) xc[j] = *reinterpret_cast<const float4 *>(pc + j * kJc);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const float4 xa = *reinterpret_cast<const float4 *>(pa + i * kJc);
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                float df = __fsub_rn(xa.x, xc[j].x);
+                float s_ = __fmaf_rn(df, df, acc[u][i][j]);
+                df = __fsub_rn(xa.y, xc[j].y);
+                s_ = __fmaf_rn(df, df, s_);
+                df = __fsub_rn(xa.z, xc[j].z);
+                s_ = __fmaf_rn(df, df, s_);
+                df = __fsub_rn(xa.w, xc[j].w);
+                acc[u][i][j] = __fmaf_rn(df, df, s_);
+              }
+            }
           }
         }
-        if (rmin != ~0ull) atomicMin(oldcols ? &best2[a] : &best1[a], (unsigned long long)rmin);
       }
-      if (oldcols) {
+      // tile minima -> per-row best candidates
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (colmin[j] != ~0ull) atomicMin(&best3[cbase + j], (unsigned long long)colmin[j]);
+      for (int u = 0; u < kJoinTiles; u++) {
+        if (kind[u] == 0) continue;
+        const bool oldcols = kind[u] == 3;
+        const int ncol = oldcols ? no : nn;
+        const int cb = oldcols ? c0[u] - 32 : c0[u];  // first column within its block
+        uint64_t colmin[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int a = r0[u] + i;
+          if (a >= nn) continue;
+          uint64_t rmin = ~0ull;
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const int c = cb + j;
+            if (c >= ncol || (kind[u] == 1 && c == a)) continue;
+            const uint64_t kr = pack(acc[u][i][j], ids[c0[u] + j]);
+            rmin = kr < rmin ? kr : rmin;
+            if (kind[u] != 1) {
+              const uint64_t kc = pack(acc[u][i][j], ids[a]);
+              colmin[j] = kc < colmin[j] ? kc : colmin[j];
+            }
+          }
+          if (rmin != ~0ull) atomicMin(oldcols ? &best2[a] : &best1[a], (unsigned long long)rmin);
+        }
+        if (kind[u] != 1) {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (colmin[j] != ~0ull)
+              atomicMin(oldcols ? &best3[cb + j] : &best1[cb + j], (unsigned long long)colmin[j]);
+        }
       }
-    }
+    }  // passes
     __syncwarp();
     int pushed = 0;
     if (lane < nn) {
@@ -604,7 +685,6 @@ __global__ void __launch_bounds__(256) k_join(const float *__restrict__ X, int64
     if (w_cands) atomicAdd(&ib.counters[2], w_cands);
   }
 }
-
 // ---------------------------------------------------------------------------
 // BF16 tensor-core form of the local join.
 //
@@ -1212,14 +1292,10 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   }
   const float *Xw = Xp;
   Buf<hdb_nnd_element> Gp(ctx, (size_t)n * k);
-  const int dp = (d & 1) ? d : d + 1;
-  const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
-  int jw = (int)((56 * 1024) / per_warp);  // about four blocks per SM
-  jw = jw < 1 ? 1 : (jw > 8 ? 8 : jw);
-  const size_t smem_join = per_warp * jw;
-  HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "NN-Descent: d too large for the join tile");
+  const int jw = kJoinWarps;
+  const size_t smem_join = JoinSmem::kBytes * jw;
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
-  const int grid_join = grid_for(ctx, n, jw, 64);
+  const int grid_join = grid_for(ctx, n, jw, 16);
   const bool bf16 = p.precision == HDB_PREC_BF16;
   // BF16 form: the tensor-core tile pipeline (tcgen05) up to 256 padded
   // dimensions, the mma.sync join beyond
@@ -1355,14 +1431,10 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
   HDB_REQUIRE(!(e & DEVERR_SELF_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row lists itself");
   HDB_REQUIRE(!(e & DEVERR_DUP_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row repeats an id");
 
-  const int dp = (d & 1) ? d : d + 1;
-  const size_t per_warp = (size_t)JoinSmem::floats(dp) * sizeof(float);
-  int jw = (int)((56 * 1024) / per_warp);
-  jw = jw < 1 ? 1 : (jw > 8 ? 8 : jw);
-  const size_t smem_join = per_warp * jw;
-  HDB_REQUIRE(smem_join <= 227 * 1024, HDB_ERR_ARG, "KNNMerge: d too large for the join tile");
+  const int jw = kJoinWarps;
+  const size_t smem_join = JoinSmem::kBytes * jw;
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
-  const int grid_join = grid_for(ctx, n, jw, 64);
+  const int grid_join = grid_for(ctx, n, jw, 16);
   // NNDescentForMerge (nndescent.cu:1999-2087): PrepareForUpdateForMerge +
   // UpdateGraphForMerge per iteration
   for (int it = 0; it < p.iterations; it++) {

@@ -93,6 +93,26 @@ static int cmp_i32(const void *x, const void *y) {
 
 typedef struct { int32_t target, id; float d; } orc_cand;
 
+/* Candidate distances of a precision form inside the local join (the
+ * evaluation of the north star's BF16 and FP8 forms; the reference computes
+ * every candidate distance as the FP32 difference sum).  q holds each row's
+ * quantised coordinates (of the column-centred rows), scale a per-row scale
+ * (NULL: 1), nrm the squared norm of the dequantised row; a pair's distance
+ * is nrm_u + nrm_v - 2 s_u s_v (q_u . q_v), clamped at 0, in FP32. */
+typedef struct {
+  const float *q, *scale, *nrm;
+} orc_qrows;
+
+static float pair_dist(const float *X, int32_t d, const orc_qrows *Q, int32_t u, int32_t v) {
+  if (!Q) return orc_diffsum(X + (int64_t)u * d, X + (int64_t)v * d, d);
+  const float *a = Q->q + (int64_t)u * d, *b = Q->q + (int64_t)v * d;
+  float dot = 0.0f;
+  for (int32_t j = 0; j < d; j++) dot = fmaf(a[j], b[j], dot);
+  const float s = Q->scale ? Q->scale[u] * Q->scale[v] : 1.0f;
+  const float r = Q->nrm[u] + Q->nrm[v] - 2.0f * s * dot;
+  return r > 0.0f ? r : 0.0f;
+}
+
 /* `iterations` rounds of sampling + local join + merge on G (n rows of k,
  * sorted by (distance, id)) with its new/old flags.  split > 0 is the merge of
  * the point sets [0, split) and [split, n) (NNDescentForMerge,
@@ -101,7 +121,8 @@ typedef struct { int32_t target, id; float d; } orc_cand;
  * only (TiledNewOldNeighborsCompareKernelForMerge :1328-1383 without the
  * new x new kernel, UpdateGraphForMerge :1582-1640). */
 static int nnd_iterate(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
-                       int32_t iterations, int64_t split, orc_nb *G, uint8_t *isnew) {
+                       int32_t iterations, int64_t split, orc_nb *G, uint8_t *isnew,
+                       const orc_qrows *Q) {
   int32_t *newl = (int32_t *)malloc(sizeof(int32_t) * n * 2 * S);
   int32_t *oldl = (int32_t *)malloc(sizeof(int32_t) * n * 2 * S);
   int32_t *nfwd = (int32_t *)calloc(n, 4), *ofwd = (int32_t *)calloc(n, 4);
@@ -178,13 +199,13 @@ static int nnd_iterate(const float *X, int64_t n, int32_t d, int32_t k, int32_t 
       float dno[64][64];
       for (int32_t a = 0; a < nn; a++)
         for (int32_t b = 0; b < no; b++)
-          dno[a][b] = orc_diffsum(X + (int64_t)nv[a] * d, X + (int64_t)ov[b] * d, d);
+          dno[a][b] = pair_dist(X, d, Q, nv[a], ov[b]);
       for (int32_t a = 0; a < nn; a++) {
         if (!cross_only) {
           orc_nb best = {1e10f, INT_MAX};
           for (int32_t b = 0; b < nn; b++) {
             if (b == a) continue;
-            orc_nb c = {orc_diffsum(X + (int64_t)nv[a] * d, X + (int64_t)nv[b] * d, d), nv[b]};
+            orc_nb c = {pair_dist(X, d, Q, nv[a], nv[b]), nv[b]};
             if (nb_less(c, best)) best = c;
           }
           if (best.id != INT_MAX) cb[nc++] = (orc_cand){nv[a], best.id, best.d};
@@ -263,18 +284,9 @@ static int nnd_iterate(const float *X, int64_t n, int32_t d, int32_t k, int32_t 
  * row is advanced like a self id, so rows never hold duplicates.
  * Output ids carry no old/new flag; distances are squared L2.
  */
-int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
-                  int32_t iterations, int32_t *ids_out, float *dist_out) {
-  if (n < 2 || k < 1 || k > 1024 || S < 1 || 2 * S > k || n <= k) return ORC_ERR_ARG;
+/* InitKNNGraphIndexKernel (:1673-1692) + distances + per-row sort. */
+static void nnd_init(const float *X, int64_t n, int32_t d, int32_t k, orc_nb *G, uint8_t *isnew) {
   const int32_t NB = (k + 31) / 32;
-  orc_nb *G = (orc_nb *)malloc(sizeof(orc_nb) * n * k);
-  uint8_t *isnew = (uint8_t *)malloc((size_t)n * k);
-  if (!G || !isnew) {
-    free(G); free(isnew);
-    return ORC_ERR_ALLOC;
-  }
-
-  /* InitKNNGraphIndexKernel (:1673-1692) + distances + per-row sort. */
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; i++) {
     orc_nb *row = G + i * k;
@@ -294,14 +306,143 @@ int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
     qsort(row, k, sizeof(orc_nb), cmp_nb);
     memset(isnew + i * k, 1, k);
   }
+}
 
-  int rc = nnd_iterate(X, n, d, k, S, iterations, 0, G, isnew);
+int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
+                  int32_t iterations, int32_t *ids_out, float *dist_out) {
+  return orc_nndescent_form(X, n, d, k, S, iterations, ORC_FORM_FP32, ids_out, dist_out);
+}
+
+/* Round to the nearest BF16 value, ties to even. */
+static float round_bf16(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+/* Round to the nearest FP8 e4m3 value (OCP FP8: 4 exponent bits, bias 7, 3
+ * mantissa bits, largest finite 448, subnormal step 2^-9), ties to even,
+ * saturating at +-448. */
+static float round_e4m3(float x) {
+  const float a = fabsf(x);
+  float q;
+  if (a >= 448.0f) {
+    q = 448.0f;
+  } else if (a < 0.015625f) {  /* below 2^-6: subnormal, step 2^-9 */
+    q = rintf(a * 512.0f) / 512.0f;
+  } else {
+    int e;
+    frexpf(a, &e);                       /* a = m 2^e, m in [0.5, 1) */
+    const float step = ldexpf(1.0f, e - 4);  /* 3 mantissa bits below the leading one */
+    q = rintf(a / step) * step;
+    if (q > 448.0f) q = 448.0f;
+  }
+  return copysignf(q, x);
+}
+
+/* Round to the nearest FP16 value (5 exponent bits, bias 15, 10 mantissa
+ * bits; subnormal step 2^-24), ties to even; the callers scale rows so that
+ * nothing overflows. */
+static float round_fp16(float x) {
+  const float a = fabsf(x);
+  float q;
+  if (a < 6.103515625e-05f) {  /* below 2^-14: subnormal, step 2^-24 */
+    q = rintf(a * 16777216.0f) / 16777216.0f;
+  } else {
+    int e;
+    frexpf(a, &e);
+    const float step = ldexpf(1.0f, e - 11);  /* 10 mantissa bits below the leading one */
+    q = rintf(a / step) * step;
+  }
+  return copysignf(q, x);
+}
+
+/*
+ * NN-Descent with the local join's candidate distances taken in a precision
+ * form (ORC_FORM_FP32: the reference's difference sum, as orc_nndescent;
+ * ORC_FORM_BF16: the Gram form of the column-centred rows rounded to BF16;
+ * ORC_FORM_FP8: the Gram form of the column-centred rows in FP8 e4m3 with a
+ * per-row scale max|x| / 448; ORC_FORM_FP16: in FP16 with one power-of-two
+ * scale for all rows), the initial distances exact, and every kept
+ * neighbour re-ranked with the exact FP32 difference sum at the end -- the
+ * structure of the library's BF16 tensor-core form, used to measure what a
+ * form does to the final graph's recall.  Output as orc_nndescent.
+ */
+int orc_nndescent_form(const float *X, int64_t n, int32_t d, int32_t k, int32_t S,
+                       int32_t iterations, int32_t form, int32_t *ids_out, float *dist_out) {
+  if (n < 2 || k < 1 || k > 1024 || S < 1 || 2 * S > k || n <= k) return ORC_ERR_ARG;
+  if (form < ORC_FORM_FP32 || form > ORC_FORM_FP16) return ORC_ERR_ARG;
+  orc_nb *G = (orc_nb *)malloc(sizeof(orc_nb) * n * k);
+  uint8_t *isnew = (uint8_t *)malloc((size_t)n * k);
+  float *q = NULL, *scale = NULL, *nrm = NULL;
+  if (form != ORC_FORM_FP32) {
+    q = (float *)malloc(sizeof(float) * n * d);
+    nrm = (float *)malloc(sizeof(float) * n);
+    if (form == ORC_FORM_FP8 || form == ORC_FORM_FP16) scale = (float *)malloc(sizeof(float) * n);
+  }
+  if (!G || !isnew || (form != ORC_FORM_FP32 && (!q || !nrm)) ||
+      ((form == ORC_FORM_FP8 || form == ORC_FORM_FP16) && !scale)) {
+    free(G); free(isnew); free(q); free(scale); free(nrm);
+    return ORC_ERR_ALLOC;
+  }
+  nnd_init(X, n, d, k, G, isnew);
+  orc_qrows Q = {q, scale, nrm};
+  if (form != ORC_FORM_FP32) {
+    double *mean = (double *)calloc(d, sizeof(double));
+    for (int64_t i = 0; i < n; i++)
+      for (int32_t j = 0; j < d; j++) mean[j] += X[i * d + j];
+    for (int32_t j = 0; j < d; j++) mean[j] /= (double)n;
+    /* FP16: one power-of-two scale for all rows, max |x| / s in [2^14, 2^15) */
+    float gmax = 0.0f, gscale = 1.0f;
+    for (int64_t i = 0; i < n * d; i++) gmax = fmaxf(gmax, fabsf(X[i] - (float)mean[i % d]));
+    if (gmax > 0.0f) {
+      int e = 0;
+      frexpf(gmax, &e);
+      gscale = ldexpf(1.0f, e - 15);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+      float mx = 0.0f, s = 1.0f, acc = 0.0f;
+      for (int32_t j = 0; j < d; j++) mx = fmaxf(mx, fabsf(X[i * d + j] - (float)mean[j]));
+      if (form == ORC_FORM_FP8) {
+        s = mx > 0.0f ? mx / 448.0f : 1.0f;
+        scale[i] = s;
+      } else if (form == ORC_FORM_FP16) {
+        s = gscale;
+        scale[i] = s;
+      }
+      for (int32_t j = 0; j < d; j++) {
+        const float c = X[i * d + j] - (float)mean[j];
+        const float v = form == ORC_FORM_BF16 ? round_bf16(c)
+                        : form == ORC_FORM_FP8 ? round_e4m3(c / s) : round_fp16(c / s);
+        q[i * d + j] = v;
+        acc = fmaf(v * s, v * s, acc);
+      }
+      nrm[i] = acc;
+    }
+    free(mean);
+  }
+  int rc = nnd_iterate(X, n, d, k, S, iterations, 0, G, isnew,
+                       form == ORC_FORM_FP32 ? NULL : &Q);
+  if (rc == ORC_OK && form != ORC_FORM_FP32) {
+    /* re-rank every kept neighbour with the exact difference sum */
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+      orc_nb *row = G + i * k;
+      for (int32_t t = 0; t < k; t++) row[t].d = orc_diffsum(X + i * d, X + (int64_t)row[t].id * d, d);
+      qsort(row, k, sizeof(orc_nb), cmp_nb);
+    }
+  }
   if (rc == ORC_OK)
     for (int64_t i = 0; i < n * k; i++) {
       ids_out[i] = G[i].id;
       dist_out[i] = G[i].d;
     }
-  free(G); free(isnew);
+  free(G); free(isnew); free(q); free(scale); free(nrm);
   return rc;
 }
 
@@ -367,7 +508,7 @@ int orc_knn_merge(const float *X, int64_t n1, int64_t n2, int32_t d, const int32
     qsort(row, k, sizeof(orc_nb), cmp_nb);
     for (int32_t t = 0; t < k; t++) isnew[i * k + t] = (uint8_t)((row[t].id >= n1) != inb);
   }
-  int rc = nnd_iterate(X, n, d, k, S, iterations, n1, G, isnew);
+  int rc = nnd_iterate(X, n, d, k, S, iterations, n1, G, isnew, NULL);
   if (rc == ORC_OK)
     for (int64_t i = 0; i < n * k; i++) {
       ids_out[i] = G[i].id;

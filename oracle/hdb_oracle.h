@@ -40,6 +40,12 @@ int orc_num_threads(void);
 uint64_t orc_xorshift64star(uint64_t x);
 int orc_nndescent(const float *X, int64_t n, int32_t d, int32_t k, int32_t sample_num,
                   int32_t iterations, int32_t *ids_out, float *dist_out);
+/* NN-Descent with the local join's candidate distances in a precision form,
+ * exact initial distances and an exact FP32 re-rank at the end (the
+ * evaluation of the BF16 / FP8 forms). */
+enum { ORC_FORM_FP32 = 0, ORC_FORM_BF16 = 1, ORC_FORM_FP8 = 2, ORC_FORM_FP16 = 3 };
+int orc_nndescent_form(const float *X, int64_t n, int32_t d, int32_t k, int32_t sample_num,
+                       int32_t iterations, int32_t form, int32_t *ids_out, float *dist_out);
 int orc_knn_merge(const float *X, int64_t n1, int64_t n2, int32_t d, const int32_t *ids1,
                   const int32_t *ids2, int32_t k, int32_t sample_num, int32_t iterations,
                   int32_t *ids_out, float *dist_out);

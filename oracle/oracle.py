@@ -49,6 +49,7 @@ def lib():
             "orc_num_threads": (C.c_int, []),
             "orc_xorshift64star": (C.c_uint64, [C.c_uint64]),
             "orc_nndescent": (C.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _P, _P]),
+            "orc_nndescent_form": (C.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _I32, _P, _P]),
             "orc_knn_merge": (C.c_int, [_P, _I64, _I64, _I32, _P, _P, _I32, _I32, _I32, _P, _P]),
             "orc_bruteforce_knn": (C.c_int, [_P, _I64, _I32, _I32, _P, _I64, _P, _P]),
             "orc_recall": (C.c_double, [_P, _I32, _P, _I32, _I64, _I32]),
@@ -103,6 +104,24 @@ def nndescent(X, k=32, sample_num=16, iterations=6):
     rc = lib().orc_nndescent(_p(X), n, d, k, sample_num, iterations, _p(ids), _p(dist))
     if rc:
         raise ValueError(f"orc_nndescent failed ({rc})")
+    return ids, dist
+
+
+FORMS = {"fp32": 0, "bf16": 1, "fp8": 2, "fp16": 3}
+
+
+def nndescent_form(X, form, k=32, sample_num=16, iterations=6):
+    """NN-Descent whose local join takes candidate distances in a precision
+    form ("fp32" exact, "bf16" / "fp8" / "fp16" Gram forms of the centred rows), then an
+    exact FP32 re-rank of the kept neighbours (orc_nndescent_form)."""
+    X = _c(X, np.float32)
+    n, d = X.shape
+    ids = np.empty((n, k), np.int32)
+    dist = np.empty((n, k), np.float32)
+    rc = lib().orc_nndescent_form(_p(X), n, d, k, sample_num, iterations, FORMS[form], _p(ids),
+                                  _p(dist))
+    if rc:
+        raise ValueError(f"orc_nndescent_form failed ({rc})")
     return ids, dist
 
 

@@ -31,10 +31,15 @@ def check_same(ctx, oracle, ids, dist, X, mst):
 
 @pytest.mark.parametrize("path", FILES, ids=lambda p: os.path.basename(p)[4:-4])
 def test_core_sg_on_reference_graphs(ctx, oracle, path):
+    """On the reference's fixtures the GPU core-SG equals the reference's own
+    (Union_kNNG_MST + update_core_sg_weights, stored by make_ref_golden.py)."""
     d = dict(np.load(path))
-    with open(path[:-4] + ".json") as f:
-        meta = json.load(f)
-    check_same(ctx, oracle, d["ids"], d["dist"], d["X"], d[f"mst_{meta['mpts'][0]}"])
+    check_same(ctx, oracle, d["ids"], d["dist"], d["X"], d["mst_32"])
+    sg = ctx.build_CoreSG(d["ids"], d["dist"], d["X"], d["mst_32"])
+    np.testing.assert_array_equal(_t(sg.nindex), d["coresg_nindex"])
+    np.testing.assert_array_equal(_t(sg.nlist), d["coresg_nlist"])
+    np.testing.assert_array_equal(_t(sg.eweight).view(np.uint32),
+                                  d["coresg_eweight"].view(np.uint32))
 
 
 def test_core_sg_on_gpu_graph_squared_distances(ctx, oracle):

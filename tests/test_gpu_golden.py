@@ -72,3 +72,21 @@ def test_cuda_run_from_knn_matches_reference_labels(ctx, golden):
         labels, _ = ctx.hdbscan_from_knn(torch.from_numpy(Gk).cuda(), torch.from_numpy(g["X"]).cuda(),
                                          k=32, mpts=mpts, distance=HDB_DIST_SQUARED)
         np.testing.assert_array_equal(_t(labels), g[f"labels_{mpts}"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_initial_graph_matches_reference(ctx, oracle, golden, prec):
+    """k_init's ids against the reference's initial graph (gpuknn::NNDescent
+    with 0 iterations), and ids and distance bits against the oracle's."""
+    import gpu_hdbscan_b200 as g_
+    from test_oracle_golden import check_initial_graph
+    g, meta = golden
+    if "ref_init_ids" not in g:
+        pytest.skip("the reference NN-Descent is compiled for d = 12 only")
+    pc = g_.HDB_PREC_BF16 if prec == "bf16" else g_.HDB_PREC_FP32
+    G = ctx.NNDescent(g["X"], k=32, sample_num=16, iterations=0, precision=pc)
+    ids, dist = (_t(a) for a in ctx.knn_split(G))
+    check_initial_graph(ids, g["ref_init_ids"])
+    oids, odist = oracle.nndescent(g["X"], 32, 16, 0)
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))

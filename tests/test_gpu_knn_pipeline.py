@@ -139,3 +139,50 @@ def test_pipeline_device_and_host_io_agree(ctx):
     lh, _ = ctx.hdbscan_from_knn(G.cpu(), X)
     assert not lh.is_cuda
     np.testing.assert_array_equal(lh.numpy(), _t(ld))
+
+
+def _golden_recall(name):
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "ref_nndescent_recall_cg.json")
+    with open(path) as f:
+        return json.load(f)["sets"][name]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_recall_on_the_100k_blob_config_is_the_references(ctx, oracle, prec):
+    """The 100,000 x 12 blob configuration itself (10 blobs, centres in
+    [-10, 10]^12, sigma 1, 5 % noise; k = 32, S = 16, 6 iterations): recall@32
+    against the exact FP64 kNN on 3,000 sampled rows is at least the
+    reference's own NN-Descent's on the same data, less 0.5 pt (the reference
+    built with L2-only global loads, recorded by make_ref_golden.py
+    --nndescent-recall --cg), and within 0.5 pt of the oracle's restatement."""
+    from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
+    ref = _golden_recall("blobs_100k_d12")
+    X = synth.generate(synth.WORKLOADS["blobs_100k_d12"])
+    q = np.sort(np.random.default_rng(5).choice(len(X), 3000, replace=False))
+    gt, _ = oracle.bruteforce_knn(X, 32, q)
+    pc = HDB_PREC_BF16 if prec == "bf16" else HDB_PREC_FP32
+    ids, _ = ctx.knn_split(ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=pc))
+    r = oracle.recall(_t(ids)[q], gt, 32)
+    assert r >= ref["ref_recall32"] - 0.005, (r, ref)
+    assert r >= ref["oracle_recall32"] - 0.005, (r, ref)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_recall_on_a_sample_of_the_20m_x_128_distribution(ctx, oracle, prec):
+    """100,000 points drawn from the 20M x 128 mixture (1,000 blobs, sigma in
+    [0.5, 1.5], centres in [-20, 20]^128, 5 % noise): recall@32 on 2,000 rows
+    within 0.5 pt of the oracle's restatement of the reference NN-Descent (the
+    reference itself is compiled for d = 12 only)."""
+    from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
+    X = synth.sample(synth.WORKLOADS["blobs_20m_d128"], 100_000)
+    q = np.sort(np.random.default_rng(6).choice(len(X), 2000, replace=False))
+    gt, _ = oracle.bruteforce_knn(X, 32, q)
+    oids, _ = oracle.nndescent(X, 32, 16, 6)
+    r_orc = oracle.recall(oids[q], gt, 32)
+    pc = HDB_PREC_BF16 if prec == "bf16" else HDB_PREC_FP32
+    ids, _ = ctx.knn_split(ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=pc))
+    r = oracle.recall(_t(ids)[q], gt, 32)
+    assert r >= r_orc - 0.005, (r, r_orc)

@@ -1,8 +1,9 @@
-"""The oracle's Core-SG (core-sg.cu) on the reference's golden fixtures: the
-kNN-plus-reverse part of every row equals the reference's own enhanced-graph
-rows without the antihub clique (buildECLgraph output stored in the
-fixtures), and the MST part holds the incident edges of the reference's
-sorted MST in edge order, with the reference's Euclidean rounding."""
+"""The oracle's Core-SG (core-sg.cu) on the reference's golden fixtures, bit
+for bit against the reference's own core-SG: Union_kNNG_MST
+(core-sg.cu:292-420) + update_core_sg_weights (core-sg.cu:432-471) run on the
+fixture's kNN graph and its sorted MST (tests/golden/make_ref_golden.py
+--add-core-sg): row offsets, rows (own kNN ids, non-mutual reverse sources,
+MST neighbours in sorted-MST edge order) and the Euclidean weights."""
 import glob
 import json
 import os
@@ -22,31 +23,9 @@ def golden(request):
     return dict(np.load(request.param)), meta
 
 
-def test_core_sg_rows_follow_the_reference(oracle, golden):
+def test_core_sg_equals_the_reference(oracle, golden):
     g, meta = golden
-    ids, dist, X = g["ids"], g["dist"], g["X"]
-    n, k = ids.shape
-    mst = g[f"mst_{meta['mpts'][0]}"]
-    nindex, nlist, ew = oracle.core_sg(ids, dist, X, mst)
-    mdeg = np.bincount(np.concatenate([mst["from_node"], mst["to_node"]]), minlength=n)
-    ah = set(g["antihubs"].tolist())
-    ref_ni, ref_nl = g["nindex"], g["nlist"]
-    pos = {}
-    for e, (a, b) in enumerate(zip(mst["from_node"], mst["to_node"])):
-        pos.setdefault(int(b), []).append(int(a))  # to_node's row takes from_node first
-        pos.setdefault(int(a), []).append(int(b))
-    for i in range(n):
-        row = nlist[nindex[i]:nindex[i + 1]]
-        ref = ref_nl[ref_ni[i]:ref_ni[i + 1]]
-        nrev = len(ref) - k - (len(ah) - 1 if i in ah else 0)
-        assert len(row) == k + nrev + mdeg[i]
-        np.testing.assert_array_equal(row[:k + nrev], ref[:k + nrev])
-        np.testing.assert_array_equal(row[k + nrev:], pos.get(i, []))
-        w = ew[nindex[i]:nindex[i + 1]]
-        np.testing.assert_array_equal(w[:k].view(np.uint32), dist[i].view(np.uint32))
-        for t, s in enumerate(row[k:k + nrev]):
-            j = int(np.nonzero(ids[s] == i)[0][0])
-            assert w[k + t].view(np.uint32) == dist[s, j].view(np.uint32)
-        for t, nb in enumerate(row[k + nrev:]):
-            eu = np.float32(oracle.euclid_ref(X[i], X[nb]))
-            assert w[k + nrev + t].view(np.uint32) == eu.view(np.uint32)
+    nindex, nlist, ew = oracle.core_sg(g["ids"], g["dist"], g["X"], g["mst_32"])
+    np.testing.assert_array_equal(nindex, g["coresg_nindex"])
+    np.testing.assert_array_equal(nlist, g["coresg_nlist"])
+    np.testing.assert_array_equal(ew.view(np.uint32), g["coresg_eweight"].view(np.uint32))

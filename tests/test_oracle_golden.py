@@ -77,3 +77,33 @@ def test_fixture_records_the_reference_nndescent_outcome(golden):
         pytest.skip("the reference NN-Descent is compiled for d = 12 only")
     assert "ref_nndescent_recall32" in meta and "oracle_nndescent_recall32" in meta
     assert meta["oracle_nndescent_recall32"] > 0.85
+
+
+def _rows_with_repeats(ids):
+    s = np.sort(ids, axis=1)
+    return (s[:, 1:] == s[:, :-1]).any(axis=1)
+
+
+def check_initial_graph(ids, ref):
+    """Initial kNN graph ids against the reference's (gpuknn::NNDescent with 0
+    iterations: InitKNNGraphIndexKernel, nndescent.cu:1673-1692).  Where the
+    reference's hash draws no id twice in a row, the row holds exactly the
+    reference's ids; where it does (the reference keeps the repeat), the repeat
+    is advanced to the next free id here, so the row holds every id of the
+    reference's row plus the advanced ones.  Returns the rows with repeats."""
+    rep = _rows_with_repeats(ref)
+    np.testing.assert_array_equal(np.sort(ids[~rep], axis=1), np.sort(ref[~rep], axis=1))
+    for i in np.nonzero(rep)[0]:
+        assert set(ref[i].tolist()) <= set(ids[i].tolist()), i
+    return int(rep.sum())
+
+
+def test_initial_graph_matches_reference(oracle, golden):
+    g, meta = golden
+    if "ref_init_ids" not in g:
+        pytest.skip("the reference NN-Descent is compiled for d = 12 only")
+    ids, _ = oracle.nndescent(g["X"], 32, 16, 0)
+    reps = check_initial_graph(ids, g["ref_init_ids"])
+    # the deviation is rare: a repeated draw in about a quarter of the rows at
+    # n = 1,500, k = 32 (birthday bound 1 - exp(-32 * 31 / 2 / 1500) = 0.28)
+    assert reps < 0.4 * len(ids)
