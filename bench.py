@@ -32,6 +32,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "end-to-end HDBSCAN points/s on 1 B200: BF16-TC vs plain FP32, equal recall@k"
 UNIT = "points/s"
+# forms of the NN-Descent candidate distances (hdb_knn_params.precision)
+PRECISIONS = {"bf16": 1, "fp32": 0, "fp16": 2}
+DTYPES = {"bf16": "bf16", "fp32": "f32", "fp16": "f16"}
 
 
 def parse_args():
@@ -41,7 +44,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="blobs_20m_d128")
-    ap.add_argument("--precision", choices=["fp32", "bf16"], default=None,
+    ap.add_argument("--precision", choices=["fp32", "bf16", "fp16"], default=None,
                     help="form (default: bf16; fp32 for the batched workloads)")
     ap.add_argument("--instances", type=int, default=0,
                     help="batched workloads: only the first N instances (0: all)")
@@ -328,7 +331,7 @@ def run_ours(args, w):
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
+    prec = PRECISIONS[args.precision]
     X = synth.generate_torch(replica_workload(w, rank), device=dev)
     ctx = g.Context(local)
     kw = dict(k=w.k, mpts=w.mpts, sample_num=w.sample_num, iterations=w.iterations,
@@ -368,7 +371,7 @@ def run_ours(args, w):
     # of both against the exact FP64 kNN on a sample of rows
     compare = None
     if not args.no_compare:
-        other = g.HDB_PREC_FP32 if prec == g.HDB_PREC_BF16 else g.HDB_PREC_BF16
+        other = g.HDB_PREC_FP32 if prec != g.HDB_PREC_FP32 else g.HDB_PREC_BF16
         kwo = {**kw, "precision": other}
         osteps = max(1, args.steps // 2)
         oms, ostats = timed(kwo, osteps, 1)
@@ -380,7 +383,7 @@ def run_ours(args, w):
     recall = {}
     if args.recall_queries > 0:
         qidx = torch.randperm(w.n, generator=torch.Generator().manual_seed(7))[:args.recall_queries]
-        for name_, pr in (("bf16", g.HDB_PREC_BF16), ("fp32", g.HDB_PREC_FP32)):
+        for name_, pr in PRECISIONS.items():
             if compare is None and pr != prec:
                 continue
             G = ctx.NNDescent(X, k=w.k, sample_num=w.sample_num, iterations=w.iterations,
@@ -421,7 +424,7 @@ def run_ours(args, w):
         # algorithmic bytes of the local join (per launch): staged sample rows,
         # the sample lists and counters, and each pushed candidate (inbox entry,
         # counter atomic, k-th distance read)
-        if prec == g.HDB_PREC_BF16:
+        if prec != g.HDB_PREC_FP32:
             tc = (w.d + 63) // 64 * 64 <= 256  # tensor-core tiles, else the mma.sync join
             jkernel = "k_join_tc" if tc else "k_join_bf16"
             row_bytes = ((w.d + 63) // 64 * 64 if tc else (w.d + 15) // 16 * 16) * 2
@@ -451,7 +454,7 @@ def run_ours(args, w):
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32" if prec == g.HDB_PREC_FP32 else "bf16",
+                "dtype": DTYPES[args.precision],
                 "data": "synthetic",
                 "config": {"workload": w.name, "n": w.n, "d": w.d, "k": w.k, "mpts": w.mpts,
                            "sample_num": w.sample_num, "iterations": w.iterations,
@@ -557,7 +560,7 @@ def run_ours_batch(args, bw):
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    prec = g.HDB_PREC_BF16 if args.precision == "bf16" else g.HDB_PREC_FP32
+    prec = PRECISIONS[args.precision]
     count = args.instances or None
     if args.shard_instances:
         # one batch over all ranks: rank r clusters the instances the greedy
@@ -659,7 +662,7 @@ def run_ours_batch(args, bw):
         per_d = {}
         for n, d, _ in layout:
             per_d[d] = per_d.get(d, 0) + n
-        if prec == g.HDB_PREC_BF16:
+        if prec != g.HDB_PREC_FP32:
             row_bytes = {d: ((d + 63) // 64 * 64) * 2 for d in per_d}
             jkernel = "k_join_tc"
         else:
@@ -688,7 +691,7 @@ def run_ours_batch(args, bw):
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
                 "scaling": "strong" if args.shard_instances else "weak", "vs_baseline": None,
-                "dtype": "f32" if prec == g.HDB_PREC_FP32 else "bf16", "data": "synthetic",
+                "dtype": DTYPES[args.precision], "data": "synthetic",
                 "config": {"workload": bw.name, "instances": len(layout), "n_total": n_total,
                            "n_job": n_job,
                            "points_per_d": {str(d): c for d, c in sorted(per_d.items())},

@@ -24,10 +24,10 @@ import ctypes as C
 from dataclasses import dataclass
 
 from . import _lib
-from ._lib import (HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP32, HDB_STAB_FP32,
-                   HDB_STAB_FP64, HdbError)
+from ._lib import (HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP16, HDB_PREC_FP32,
+                   HDB_STAB_FP32, HDB_STAB_FP64, HdbError)
 
-__all__ = ["Context", "HdbError", "EnhancedGraph", "HDB_PREC_FP32", "HDB_PREC_BF16",
+__all__ = ["Context", "HdbError", "EnhancedGraph", "HDB_PREC_FP32", "HDB_PREC_BF16", "HDB_PREC_FP16",
            "HDB_DIST_SQRT", "HDB_DIST_SQUARED", "HDB_STAB_FP32", "HDB_STAB_FP64"]
 
 

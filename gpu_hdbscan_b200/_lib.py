@@ -16,7 +16,7 @@ HDB_OK, HDB_ERR_ARG, HDB_ERR_ALLOC, HDB_ERR_CUDA, HDB_ERR_IO, HDB_ERR_TIMEOUT, \
 STATUS_NAMES = {0: "HDB_OK", 1: "HDB_ERR_ARG", 2: "HDB_ERR_ALLOC", 3: "HDB_ERR_CUDA",
                 4: "HDB_ERR_IO", 5: "HDB_ERR_TIMEOUT", 6: "HDB_ERR_DISCONNECTED",
                 7: "HDB_ERR_INTERNAL"}
-HDB_PREC_FP32, HDB_PREC_BF16 = 0, 1
+HDB_PREC_FP32, HDB_PREC_BF16, HDB_PREC_FP16 = 0, 1, 2
 HDB_DIST_SQRT, HDB_DIST_SQUARED = 0, 1
 HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 

@@ -30,6 +30,7 @@
 //   --labels PATH       write one label per line (-1 = noise)
 //   --fp64              FP64 stability sums (default: the reference's FP32)
 //   --bf16              build the kNN graph with the BF16 tensor-core form
+//   --fp16              build the kNN graph with the FP16 tensor-core form
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -119,7 +120,7 @@ int main(int argc, char **argv) {
   std::vector<std::string> pos;
   std::string kgraph, vectors, vectors_txt, write_fvecs, labels_path, save_kgraph, save_fixed,
       save_mst;
-  bool squared = false, fp64 = false, bf16 = false;
+  bool squared = false, fp64 = false, bf16 = false, fp16 = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     auto val = [&](std::string &dst) {
@@ -137,6 +138,7 @@ int main(int argc, char **argv) {
     else if (a == "--squared") squared = true;
     else if (a == "--fp64") fp64 = true;
     else if (a == "--bf16") bf16 = true;
+    else if (a == "--fp16") fp16 = true;
     else pos.push_back(a);
   }
   if (pos.size() != 4) {
@@ -177,7 +179,7 @@ int main(int argc, char **argv) {
   if (num_values > 0 && num_values < n) n = num_values;  // knng_num = numValues
   hdb_ctx *ctx = nullptr;
   if (hdb_create(&ctx, 0) != HDB_OK) return fail("hdb_create");
-  hdb_knn_params kp{k, 16, 6, bf16 ? HDB_PREC_BF16 : HDB_PREC_FP32};
+  hdb_knn_params kp{k, 16, 6, fp16 ? HDB_PREC_FP16 : bf16 ? HDB_PREC_BF16 : HDB_PREC_FP32};
 
   auto t_all = std::chrono::steady_clock::now();
   float *Xd = to_device(X.data(), (size_t)n * d);

@@ -75,11 +75,14 @@ constexpr uint32_t kNoKey = 0x7F800000u;            // keys at or above: no cand
 // CTAs (2 x 256 tensor-memory columns = all 512) are resident on one SM.
 constexpr size_t kMinSmem = 80 * 1024;
 
-// M = N = 128, BF16 x BF16 -> FP32, both operands K-major.
-constexpr uint32_t kIdesc = (1u << 4)                       // D format F32
-                            | (1u << 7) | (1u << 10)         // A, B format BF16
-                            | ((uint32_t)(128 >> 3) << 17)   // N / 8
-                            | ((uint32_t)(128 >> 4) << 24);  // M / 16
+// M = N = 128, 16-bit x 16-bit -> FP32, both operands K-major; A and B
+// always have the same format (BF16 or FP16: both come from one tile).
+constexpr uint32_t idesc_for(bool fp16) {
+  return (1u << 4)                                   // D format F32
+         | (fp16 ? 0u : (1u << 7) | (1u << 10))      // A, B format: F16 (0) or BF16 (1)
+         | ((uint32_t)(128 >> 3) << 17)              // N / 8
+         | ((uint32_t)(128 >> 4) << 24);             // M / 16
+}
 
 struct StageMeta {
   int32_t ids[kTcTileRows];
@@ -110,6 +113,8 @@ struct JoinArgs {
   const int32_t *probe_ids, *probe_counts;
   float *probe_out;
   uint32_t *err;
+  uint32_t idesc;  // instruction descriptor of the operand format
+  float dscale;    // distance = |a|^2 + |c|^2 + dscale * accumulator
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -203,13 +208,13 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
+                                       uint32_t idesc, uint32_t accumulate) {
   const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z)
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z)
       : "memory");
 }
 __device__ __forceinline__ void tc_commit(unsigned long long *bar) {
@@ -473,7 +478,7 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
 }
 
 __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int64_t ntiles,
-                           int kbc, uint32_t *err) {
+                           int kbc, uint32_t idesc, uint32_t *err) {
   int64_t t = blockIdx.x;
   int last_b = -1;
   uint32_t last_parity = 0;
@@ -497,7 +502,7 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
 #pragma unroll
       for (int kk = 0; kk < kTcKBlock / 16; kk++) {
         const uint64_t desc = sw128_desc(base + 32u * kk);
-        tc_mma(d, desc, desc, (kb | kk) != 0 ? 1u : 0u);
+        tc_mma(d, desc, desc, idesc, (kb | kk) != 0 ? 1u : 0u);
       }
       tc_commit(&sh.empty[s]);  // the stage goes back once these MMAs are done
     }
@@ -519,7 +524,7 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
 // Row minimum over 32 columns: key = clamped distance bits with the column in
 // the low 6 bits (skip_col: the row's own column, or -1).
 __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const float *cn, float na,
-                                              int skip_col) {
+                                              float dscale, int skip_col) {
   uint32_t best[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};  // four chains
 #pragma unroll
   for (int c4 = 0; c4 < 8; c4++) {
@@ -528,7 +533,7 @@ __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const flo
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const int c = 4 * c4 + e;
-      const float dd = fmaxf(__fmaf_rn(-2.0f, __uint_as_float(v[c]), __fadd_rn(na, ncs[e])), 0.0f);
+      const float dd = fmaxf(__fmaf_rn(dscale, __uint_as_float(v[c]), __fadd_rn(na, ncs[e])), 0.0f);
       uint32_t key = (__float_as_uint(dd) & ~63u) | (uint32_t)c;
       key = c == skip_col ? 0xffffffffu : key;
       best[e] = min(best[e], key);
@@ -581,8 +586,8 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
       float *o = a.probe_out + ((size_t)t * kTcTileRows + 64 * j + slot) * 64;
 #pragma unroll
       for (int c = 0; c < 32; c++) {
-        o[c] = __fmaf_rn(-2.0f, __uint_as_float(v0[c]), __fadd_rn(na, cn[c]));
-        o[32 + c] = __fmaf_rn(-2.0f, __uint_as_float(v1[c]), __fadd_rn(na, cn[32 + c]));
+        o[c] = __fmaf_rn(a.dscale, __uint_as_float(v0[c]), __fadd_rn(na, cn[c]));
+        o[32 + c] = __fmaf_rn(a.dscale, __uint_as_float(v1[c]), __fadd_rn(na, cn[32 + c]));
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.mempty[m]);
@@ -591,11 +596,11 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     uint32_t k1, k2 = 0xffffffffu;
     int32_t id1 = -1, id2 = -1;
     if (isnew) {
-      k1 = row_min32(v0, cn, na, lane);       // closest other new row
-      k2 = row_min32(v1, cn + 32, na, -1);    // closest old row
+      k1 = row_min32(v0, cn, na, a.dscale, lane);     // closest other new row
+      k2 = row_min32(v1, cn + 32, na, a.dscale, -1);  // closest old row
       if (k2 < kNoKey) id2 = M.ids[64 * j + 32 + (k2 & 63u)];
     } else {
-      k1 = row_min32(v0, cn, na, -1);         // closest new row
+      k1 = row_min32(v0, cn, na, a.dscale, -1);       // closest new row
     }
     if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
     __syncwarp();
@@ -660,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     producer<kProbe>(warp - kProducerWarp0, &xmap, a, sh, tiles, n, ntiles, kbc, S, stat);
     if (!kProbe && lane_id() == 0 && stat) atomicAdd(&a.ib.counters[1], stat);
   } else if (warp == kMmaWarp) {
-    if (lane_id() == 0) mma_issuer(sh, tiles, tmem, ntiles, kbc, a.err);
+    if (lane_id() == 0) mma_issuer(sh, tiles, tmem, ntiles, kbc, a.idesc, a.err);
     __syncwarp();
   } else {
     epilogue<kProbe>(a, sh, tmem, ntiles, stat);
@@ -727,7 +732,8 @@ void launch(Context *ctx, const TcJoin &tj, int64_t ntiles, int S, const JoinArg
 
 }  // namespace
 
-void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad, TcJoin *tj) {
+void tc_join_prepare(Context *ctx, const uint16_t *Xb, int64_t n, int dpad, bool fp16, float dscale,
+                     TcJoin *tj) {
   HDB_REQUIRE(dpad % kTcKBlock == 0 && dpad >= kTcKBlock && dpad <= kTcMaxDpad, HDB_ERR_ARG,
               "tensor-core join: padded dimension must be a multiple of 64 in [64, 256]");
   HDB_REQUIRE(n >= 1 && n < (int64_t(1) << 31), HDB_ERR_ARG, "tensor-core join: bad row count");
@@ -736,10 +742,11 @@ void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad,
   auto fn = encode_tiled();
   HDB_REQUIRE(fn != nullptr, HDB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
   cuuint64_t gdim[2] = {(cuuint64_t)dpad, (cuuint64_t)n};
-  cuuint64_t gstride[1] = {(cuuint64_t)dpad * sizeof(__nv_bfloat16)};
+  cuuint64_t gstride[1] = {(cuuint64_t)dpad * sizeof(uint16_t)};
   cuuint32_t box[2] = {(cuuint32_t)kTcKBlock, 1};  // one row high (gather4)
   cuuint32_t estride[2] = {1, 1};
-  CUresult r = fn(&tj->xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(Xb),
+  CUresult r = fn(&tj->xmap, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16,
+                  2, const_cast<uint16_t *>(Xb),
                   gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -748,6 +755,8 @@ void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad,
   tj->n = n;
   tj->dpad = dpad;
   tj->smem = smem_bytes();
+  tj->idesc = idesc_for(fp16);
+  tj->dscale = dscale;
   (void)ctx;
 }
 
@@ -760,16 +769,19 @@ void tc_join_launch(Context *ctx, const TcJoin &tj, int S, const float *nrm, con
       const_cast<int8_t *>(nf), const_cast<int8_t *>(of), nrev, orev);
   ctx->launches++;
   HDB_CHECK_LAUNCH();
-  JoinArgs a{nrm, newS, oldS, nf, of, nrev, orev, worst, ib, nullptr, nullptr, nullptr, ctx->dev_err};
+  JoinArgs a{nrm,     newS,    oldS,    nf,           of,       nrev,     orev,
+             worst,   ib,      nullptr, nullptr,      nullptr,  ctx->dev_err, tj.idesc,
+             tj.dscale};
   launch<false>(ctx, tj, (tj.n + 1) / 2, S, a);
 }
 
-void tc_gram_probe(Context *ctx, const __nv_bfloat16 *Xb, const float *nrm, int64_t n, int dpad,
+void tc_gram_probe(Context *ctx, const uint16_t *Xb, const float *nrm, int64_t n, int dpad,
                    const int32_t *ids, const int32_t *counts, int64_t tiles, float *out) {
   TcJoin tj;
-  tc_join_prepare(ctx, Xb, n, dpad, &tj);
-  JoinArgs a{nrm,     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-             Inbox{}, ids,     counts,  out,     ctx->dev_err};
+  tc_join_prepare(ctx, Xb, n, dpad, false, -2.0f, &tj);
+  JoinArgs a{nrm,     nullptr, nullptr, nullptr, nullptr, nullptr,      nullptr,
+             nullptr, Inbox{}, ids,     counts,  out,     ctx->dev_err, tj.idesc,
+             tj.dscale};
   launch<true>(ctx, tj, tiles, 1, a);
 }
 

@@ -27,10 +27,15 @@ struct TcJoin {
   int dpad = 0;
   size_t smem = 0;
   int grid = 0;
+  uint32_t idesc = 0;    // tcgen05 instruction descriptor (operand format)
+  float dscale = -2.0f;  // distance = |a|^2 + |c|^2 + dscale * (a.c of the stored rows)
 };
 
-// Builds the TMA descriptor over Xb [n, dpad] (dpad = tc_dpad(d) <= kTcMaxDpad).
-void tc_join_prepare(Context *ctx, const __nv_bfloat16 *Xb, int64_t n, int dpad, TcJoin *tj);
+// Builds the TMA descriptor over the 16-bit rows Xh [n, dpad] (dpad =
+// tc_dpad(d) <= kTcMaxDpad): BF16, or FP16 (fp16 = true) of rows stored
+// divided by a power-of-two scale s, with dscale = -2 s^2 (-2 for BF16).
+void tc_join_prepare(Context *ctx, const uint16_t *Xh, int64_t n, int dpad, bool fp16,
+                     float dscale, TcJoin *tj);
 
 // One local-join pass over all rows: the sample lists of k_sample in, the
 // candidates out through the inbox's overflow list only (ib.ovf_cap must hold
@@ -43,7 +48,7 @@ void tc_join_launch(Context *ctx, const TcJoin &tj, int S, const float *nrm, con
 // path): ids [tiles * 128], counts [tiles * 4] = (new0, old0, new1, old1),
 // out [tiles * 128 * 64] = the BF16 distance of every staged row against the
 // 64 slots of its own row-join (+inf for empty columns).
-void tc_gram_probe(Context *ctx, const __nv_bfloat16 *Xb, const float *nrm, int64_t n, int dpad,
+void tc_gram_probe(Context *ctx, const uint16_t *Xb, const float *nrm, int64_t n, int dpad,
                    const int32_t *ids, const int32_t *counts, int64_t tiles, float *out);
 
 }  // namespace hdb

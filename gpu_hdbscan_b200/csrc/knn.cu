@@ -15,7 +15,10 @@
 //    (nndescent.cu:1086-1093, fmaf per element), so every pair has one exact
 //    value wherever it is computed.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
+#include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "hdb_internal.cuh"
@@ -718,13 +721,40 @@ __global__ void k_col_mean(const double *__restrict__ sums, int d, int64_t n, fl
   for (int j = threadIdx.x; j < d; j += blockDim.x) mean[j] = (float)(sums[j] / (double)n);
 }
 
-// BF16 copy of (X - mean) (mean may be null: no centring), zero padded to
-// dpad columns, and the FP32 squared norm of every rounded row.  Distances
-// do not change under a common shift, and centring keeps the coordinates
-// small, which is where BF16 rounding is finest.
-__global__ void k_bf16_prepare(const float *__restrict__ X, int64_t n, int d, int dpad,
-                               const float *__restrict__ mean, __nv_bfloat16 *__restrict__ Xb,
-                               float *__restrict__ nrm) {
+// Largest |x - mean| over X (float bits: non-negative floats order as
+// unsigned integers), for the FP16 form's power-of-two scale.
+__global__ void k_abs_max(const float *__restrict__ X, int64_t n, int d,
+                          const float *__restrict__ mean, uint32_t *__restrict__ out) {
+  uint32_t m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * d;
+       i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(fabsf(__fsub_rn(X[i], mean[i % d]))));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane_id() == 0 && m) atomicMax(out, m);
+}
+
+// 16-bit operand formats of the tensor-core forms.
+struct Bf16Op {
+  using T = __nv_bfloat16;
+  static __device__ __forceinline__ T from(float x) { return __float2bfloat16_rn(x); }
+  static __device__ __forceinline__ float to(T x) { return __bfloat162float(x); }
+};
+struct Fp16Op {
+  using T = __half;
+  static __device__ __forceinline__ T from(float x) { return __float2half_rn(x); }
+  static __device__ __forceinline__ float to(T x) { return __half2float(x); }
+};
+
+// 16-bit copy of (X - mean) / scale (mean may be null: no centring; scale a
+// power of two, 1 for BF16), zero padded to dpad columns, and the FP32
+// squared norm of every rounded row taken back to the original scale.
+// Distances do not change under a common shift, and centring keeps the
+// coordinates small, which is where the rounding is finest.
+template <typename Op>
+__global__ void k_half_prepare(const float *__restrict__ X, int64_t n, int d, int dpad,
+                               const float *__restrict__ mean, float inv_scale, float scale,
+                               typename Op::T *__restrict__ Xh, float *__restrict__ nrm) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
@@ -732,9 +762,9 @@ __global__ void k_bf16_prepare(const float *__restrict__ X, int64_t n, int d, in
     float part = 0.0f;
     for (int j = lane; j < dpad; j += 32) {
       const float x = j < d ? __fsub_rn(X[row * d + j], mean ? mean[j] : 0.0f) : 0.0f;
-      __nv_bfloat16 b = __float2bfloat16_rn(x);
-      Xb[row * dpad + j] = b;
-      float v = __bfloat162float(b);
+      const typename Op::T h = Op::from(__fmul_rn(x, inv_scale));
+      Xh[row * dpad + j] = h;
+      const float v = __fmul_rn(Op::to(h), scale);
       part = __fmaf_rn(v, v, part);
     }
 #pragma unroll
@@ -757,17 +787,28 @@ __device__ __forceinline__ void ldsm_x4(uint32_t &r0, uint32_t &r1, uint32_t &r2
                : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
                : "r"(s));
 }
-__device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+template <bool kFp16>
+__device__ __forceinline__ void mma_16(float *c, const uint32_t *a, uint32_t b0, uint32_t b1) {
+  if (kFp16)
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+  else
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restrict__ Xb,
+// kFp16: FP16 operands (scaled rows; dscale = -2 scale^2), else BF16
+// (dscale = -2).  Xb holds the 16-bit rows.
+template <bool kFp16>
+__global__ void __launch_bounds__(128) k_join_bf16(const uint16_t *__restrict__ Xb,
                                                    const float *__restrict__ nrm, int64_t n,
-                                                   int dpad, int S,
+                                                   int dpad, int S, float dscale,
                                                    const int32_t *__restrict__ newS,
                                                    const int32_t *__restrict__ oldS,
                                                    const int8_t *__restrict__ nf,
@@ -783,7 +824,7 @@ __global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restri
   unsigned long long *best1 = best, *best2 = best + 32, *best3 = best + 64;
   int32_t *ids = reinterpret_cast<int32_t *>(base + 96 * 8);
   float *nr = reinterpret_cast<float *>(base + 96 * 8 + 256);
-  __nv_bfloat16 *Bs = reinterpret_cast<__nv_bfloat16 *>(base + 96 * 8 + 512);
+  uint16_t *Bs = reinterpret_cast<uint16_t *>(base + 96 * 8 + 512);
   const int ld = dpad + 8;  // row stride in elements (16-byte aligned, ldmatrix conflict free)
   const int chunks = dpad >> 3;  // 16-byte chunks per row
   unsigned long long w_rows = 0, w_cands = 0;
@@ -858,8 +899,8 @@ __global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restri
 #pragma unroll
         for (int mt = 0; mt < 2; mt++) {
           if (mt >= mts) continue;
-          mma_bf16(acc[mt][2 * pr], a[mt], b0, b1);
-          mma_bf16(acc[mt][2 * pr + 1], a[mt], b2, b3);
+          mma_16<kFp16>(acc[mt][2 * pr], a[mt], b0, b1);
+          mma_16<kFp16>(acc[mt][2 * pr + 1], a[mt], b2, b3);
         }
       }
     }
@@ -883,7 +924,7 @@ __global__ void __launch_bounds__(128) k_join_bf16(const __nv_bfloat16 *__restri
             const bool oldc = c >= 32;
             const bool ok = arow && (oldc ? (c - 32 < no) : (c < nn && c != a));
             if (!ok) continue;
-            float dd = __fmaf_rn(-2.0f, acc[mt][nt][2 * h + e], __fadd_rn(na, nr[c]));
+            float dd = __fmaf_rn(dscale, acc[mt][nt][2 * h + e], __fadd_rn(na, nr[c]));
             dd = dd > 0.0f ? dd : 0.0f;
             const uint64_t kr = pack(dd, ids[c]);
             if (oldc) {
@@ -1221,8 +1262,9 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   HDB_REQUIRE(n > k && n < (int64_t(1) << 31) - 1, HDB_ERR_ARG, "NN-Descent: need k < n < 2^31");
   HDB_REQUIRE(d >= 1 && d <= 4096, HDB_ERR_ARG, "NN-Descent: d must be in [1, 4096]");
   HDB_REQUIRE(p.iterations >= 0, HDB_ERR_ARG, "NN-Descent: negative iteration count");
-  HDB_REQUIRE(p.precision == HDB_PREC_FP32 || p.precision == HDB_PREC_BF16, HDB_ERR_ARG,
-              "NN-Descent: unknown precision");
+  HDB_REQUIRE(p.precision == HDB_PREC_FP32 || p.precision == HDB_PREC_BF16 ||
+                  p.precision == HDB_PREC_FP16,
+              HDB_ERR_ARG, "NN-Descent: unknown precision");
   cudaStream_t st = ctx->stream;
   Buf<int32_t> gid(ctx, n * k);
   Buf<float> gdist(ctx, n * k), worst(ctx, n);
@@ -1235,7 +1277,8 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   // for a whole iteration's candidates.  The SIMT joins, whose own work is
   // cheaper, keep the inboxes: for them the sort would cost more than the
   // atomics (10M x 12: 737 vs 810 ms a step).
-  const bool tc_form = p.precision == HDB_PREC_BF16 && tc_dpad(d) <= kTcMaxDpad;
+  const bool tc_form = (p.precision == HDB_PREC_BF16 || p.precision == HDB_PREC_FP16) &&
+                       tc_dpad(d) <= kTcMaxDpad;
   Buf<uint64_t> inbox(ctx, tc_form ? 1 : (size_t)n * kInboxCap);
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
   const int64_t ovf_rows = tc_form ? 64 : 16;
@@ -1296,34 +1339,59 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const size_t smem_join = JoinSmem::kBytes * jw;
   HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
   const int grid_join = grid_for(ctx, n, jw, 16);
-  const bool bf16 = p.precision == HDB_PREC_BF16;
-  // BF16 form: the tensor-core tile pipeline (tcgen05) up to 256 padded
-  // dimensions, the mma.sync join beyond
+  // 16-bit forms: BF16, or FP16 of the rows scaled by one power of two; the
+  // tensor-core tile pipeline (tcgen05) up to 256 padded dimensions, the
+  // mma.sync join beyond
+  const bool fp16 = p.precision == HDB_PREC_FP16;
+  const bool bf16 = p.precision == HDB_PREC_BF16 || fp16;
   const bool use_tc = bf16 && tc_dpad(d) <= kTcMaxDpad;
   const int dpad = use_tc ? tc_dpad(d) : (d + 15) & ~15;
-  Buf<__nv_bfloat16> Xb;
+  Buf<uint16_t> Xb;
   Buf<float> nrm;
   int jw16 = 4;
   size_t smem_bf = 0;
   int grid_bf = 0;
+  float dscale = -2.0f;
   TcJoin tj;
   if (bf16) {
-    Xb = Buf<__nv_bfloat16>(ctx, (size_t)n * dpad);
+    Xb = Buf<uint16_t>(ctx, (size_t)n * dpad);
     nrm = Buf<float>(ctx, n);
     Buf<double> csum(ctx, d);
     Buf<float> cmean(ctx, d);
     HDB_CUDA(cudaMemsetAsync(csum, 0, d * sizeof(double), st));
     k_col_sums<<<16 * ctx->num_sms, 256, 0, st>>>(Xw, n, d, csum); ctx->launches++;
     k_col_mean<<<1, 256, 0, st>>>(csum, d, n, cmean); ctx->launches++;
-    k_bf16_prepare<<<grid_rows, 32 * wpb, 0, st>>>(Xw, n, d, dpad, cmean, Xb, nrm); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    if (fp16) {
+      // one power-of-two scale s with max |x - mean| / s in [2^14, 2^15): far
+      // from the FP16 overflow and subnormal ranges, exact to apply
+      Buf<uint32_t> amax(ctx, 1);
+      HDB_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t), st));
+      k_abs_max<<<grid_for(ctx, n * d, 256), 256, 0, st>>>(Xw, n, d, cmean, amax); ctx->launches++;
+      HDB_CHECK_LAUNCH();
+      HDB_CUDA(cudaMemcpyAsync(ctx->pinned, amax, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      ctx->sync();
+      float gmax;
+      memcpy(&gmax, ctx->pinned, sizeof(float));
+      int e = 0;
+      if (gmax > 0.0f && std::isfinite(gmax)) std::frexp(gmax, &e);
+      const float sc = std::ldexp(1.0f, e - 15);
+      dscale = -2.0f * sc * sc;
+      k_half_prepare<Fp16Op><<<grid_rows, 32 * wpb, 0, st>>>(
+          Xw, n, d, dpad, cmean, 1.0f / sc, sc, reinterpret_cast<__half *>(Xb.get()), nrm);
+    } else {
+      k_half_prepare<Bf16Op><<<grid_rows, 32 * wpb, 0, st>>>(
+          Xw, n, d, dpad, cmean, 1.0f, 1.0f, reinterpret_cast<__nv_bfloat16 *>(Xb.get()), nrm);
+    }
+    ctx->launches++;
     HDB_CHECK_LAUNCH();
     if (use_tc) {
-      tc_join_prepare(ctx, Xb, n, dpad, &tj);
+      tc_join_prepare(ctx, Xb, n, dpad, fp16, dscale, &tj);
     } else {
       smem_bf = JoinSmemBf16::bytes(dpad) * jw16;
-      HDB_REQUIRE(smem_bf <= 227 * 1024, HDB_ERR_ARG, "NN-Descent BF16: d too large for the join tile");
-      HDB_CUDA(cudaFuncSetAttribute(k_join_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_bf));
+      HDB_REQUIRE(smem_bf <= 227 * 1024, HDB_ERR_ARG, "NN-Descent 16-bit form: d too large for the join tile");
+      HDB_CUDA(cudaFuncSetAttribute(fp16 ? k_join_bf16<true> : k_join_bf16<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bf));
       grid_bf = grid_for(ctx, n, jw16, 64);
     }
   }
@@ -1335,9 +1403,12 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     if (use_tc) {
       tc_join_launch(ctx, tj, S, nrm, newS, oldS, nf, of, nrev, orev, worst, ib);
     } else {
-      if (bf16)
-        k_join_bf16<<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, newS, oldS, nf, of,
-                                                         nrev, orev, worst, ib);
+      if (fp16)
+        k_join_bf16<true><<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, dscale, newS,
+                                                               oldS, nf, of, nrev, orev, worst, ib);
+      else if (bf16)
+        k_join_bf16<false><<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, dscale, newS,
+                                                                oldS, nf, of, nrev, orev, worst, ib);
       else
         k_join<<<grid_join, 32 * jw, smem_join, st>>>(Xw, n, d, S, newS, oldS, nf, of, nrev, orev,
                                                       worst, ib, 0);
@@ -1464,10 +1535,10 @@ void bf16_distance_tiles(Context *ctx, const float *X, int64_t n, int32_t d, con
   HDB_REQUIRE(tiles >= 0, HDB_ERR_ARG, "BF16 distance tiles: negative tile count");
   if (tiles == 0) return;
   const int dpad = tc_dpad(d);
-  Buf<__nv_bfloat16> Xb(ctx, (size_t)n * dpad);
+  Buf<uint16_t> Xb(ctx, (size_t)n * dpad);
   Buf<float> nrm(ctx, n);
-  k_bf16_prepare<<<grid_for(ctx, n, 8, 16), 256, 0, ctx->stream>>>(X, n, d, dpad, nullptr, Xb,
-                                                                    nrm);
+  k_half_prepare<Bf16Op><<<grid_for(ctx, n, 8, 16), 256, 0, ctx->stream>>>(
+      X, n, d, dpad, nullptr, 1.0f, 1.0f, reinterpret_cast<__nv_bfloat16 *>(Xb.get()), nrm);
   ctx->launches++;
   HDB_CHECK_LAUNCH();
   tc_gram_probe(ctx, Xb, nrm, n, dpad, ids, counts, tiles, out);

@@ -69,7 +69,7 @@ typedef struct {
   int32_t *antihubs; /* [num_antihubs], ascending */
 } hdb_graph;
 
-enum { HDB_PREC_FP32 = 0, HDB_PREC_BF16 = 1 };
+enum { HDB_PREC_FP32 = 0, HDB_PREC_BF16 = 1, HDB_PREC_FP16 = 2 };
 enum { HDB_DIST_SQRT = 0, HDB_DIST_SQUARED = 1 };
 enum { HDB_STAB_FP32 = 0, HDB_STAB_FP64 = 1 };
 
@@ -79,7 +79,10 @@ typedef struct {
   int32_t sample_num;  /* SAMPLE_NUM, 1..k/2 (reference: 16; 2*SAMPLE_NUM <= k) */
   int32_t iterations;  /* NND_ITERATION (reference: 6) */
   int32_t precision;   /* HDB_PREC_FP32: reference difference-sum distances;
-                          HDB_PREC_BF16: tensor-core candidate distances, FP32 re-rank */
+                          HDB_PREC_BF16: tensor-core candidate distances from BF16
+                          rows, FP32 re-rank;
+                          HDB_PREC_FP16: the same from FP16 rows scaled by one
+                          power of two (3 more mantissa bits, same bytes) */
 } hdb_knn_params;
 
 typedef struct {

@@ -154,10 +154,12 @@ def _golden_recall(name):
 def test_recall_on_the_100k_blob_config_is_the_references(ctx, oracle, prec):
     """The 100,000 x 12 blob configuration itself (10 blobs, centres in
     [-10, 10]^12, sigma 1, 5 % noise; k = 32, S = 16, 6 iterations): recall@32
-    against the exact FP64 kNN on 3,000 sampled rows is at least the
-    reference's own NN-Descent's on the same data, less 0.5 pt (the reference
-    built with L2-only global loads, recorded by make_ref_golden.py
-    --nndescent-recall --cg), and within 0.5 pt of the oracle's restatement."""
+    against the exact FP64 kNN on 3,000 sampled rows is within 0.5 pt of the
+    oracle's restatement (0.889, recorded beside the reference's run by
+    make_ref_golden.py --nndescent-recall) or better.  The reference's own
+    NN-Descent, compiled for sm_100a and run on the same data, recorded 0.0015:
+    its graph stays near the random initial one, so the bound it gives is
+    trivially met and the restatement is the working anchor."""
     from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
     ref = _golden_recall("blobs_100k_d12")
     X = synth.generate(synth.WORKLOADS["blobs_100k_d12"])

@@ -70,8 +70,8 @@ def test_mst_and_trees_match_reference(oracle, golden):
 
 def test_fixture_records_the_reference_nndescent_outcome(golden):
     """The reference's own NN-Descent (VEC_DIM = 12 build) was run on the d = 12
-    case; its outcome is recorded (it did not converge on sm_100a), and the
-    kNN graph fed to the later stages is the oracle's."""
+    case; its outcome is recorded (on sm_100a its graph stays near the random
+    initial one), and the kNN graph fed to the later stages is the oracle's."""
     g, meta = golden
     if meta["d"] != 12:
         pytest.skip("the reference NN-Descent is compiled for d = 12 only")
