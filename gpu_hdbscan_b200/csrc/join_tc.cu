@@ -152,12 +152,16 @@ __device__ __forceinline__ uint64_t globaltimer() {
 
 // Waits for the phase of `bar` with the given parity.  Gives up after kWaitNs,
 // or (when `abort` is non-null) as soon as another role of the CTA gave up.
+// A waiting warp backs off with __nanosleep after its first polls, so that
+// it does not take issue slots from the warps of its SM sub-partition that
+// have work (the epilogue's minima, the producers' gathers).
 __device__ __noinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity,
                                        volatile int *abort) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; it++) {
     if (mbar_try(bar, parity)) return true;
+    if (it > 8) __nanosleep(it > 64 ? 256 : 32);
     if ((it & 15) == 0) {
       if (abort && *abort) return false;
       if (globaltimer() - t0 > kWaitNs) return false;
@@ -238,6 +242,22 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 }
 // Waits for this thread's tensor-memory loads; the registers are tied to the
 // wait so that no use of them is scheduled before it.
+__device__ __forceinline__ void tmem_wait_ld2(uint32_t (&v)[32], uint32_t (&w)[32]) {
+  asm volatile(
+      "tcgen05.wait::ld.sync.aligned;"
+      : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]),
+        "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]),
+        "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]),
+        "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]),
+        "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31]),
+        "+r"(w[0]), "+r"(w[1]), "+r"(w[2]), "+r"(w[3]), "+r"(w[4]), "+r"(w[5]), "+r"(w[6]),
+        "+r"(w[7]), "+r"(w[8]), "+r"(w[9]), "+r"(w[10]), "+r"(w[11]), "+r"(w[12]), "+r"(w[13]),
+        "+r"(w[14]), "+r"(w[15]), "+r"(w[16]), "+r"(w[17]), "+r"(w[18]), "+r"(w[19]),
+        "+r"(w[20]), "+r"(w[21]), "+r"(w[22]), "+r"(w[23]), "+r"(w[24]), "+r"(w[25]),
+        "+r"(w[26]), "+r"(w[27]), "+r"(w[28]), "+r"(w[29]), "+r"(w[30]), "+r"(w[31])
+      :
+      : "memory");
+}
 __device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.wait::ld.sync.aligned;"
@@ -543,8 +563,9 @@ __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const flo
 }
 
 template <bool kProbe>
-__device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t ntiles,
+__device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n, int64_t ntiles,
                          unsigned long long &cands) {
+  ListCursor cur;
   const int w = threadIdx.x >> 5, lane = lane_id();
   const int j = w >> 1;                 // row-join of this warp's 32 rows
   const bool isnew = (w & 1) == 0;      // new rows (slots 0..31) or old rows (32..63)
@@ -573,10 +594,11 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     uint32_t v0[32], v1[32];
     const uint32_t taddr = tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(b * kAccCols + 64 * j);
     tmem_ld32(taddr, v0);
-    tmem_wait_ld(v0);
-    if (kProbe || isnew) {
+    if (kProbe || isnew) {  // both loads in flight, one wait
       tmem_ld32(taddr + 32, v1);
-      tmem_wait_ld(v1);
+      tmem_wait_ld2(v0, v1);
+    } else {
+      tmem_wait_ld(v0);
     }
     tc_fence_before();
     __syncwarp();
@@ -610,8 +632,10 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     // warp instead of a returning inbox atomic per candidate
     const float d1 = __uint_as_float(k1 & ~63u), d2 = __uint_as_float(k2 & ~63u);
     const bool c1 = vrow && id1 >= 0 && d1 < wst, c2 = vrow && id2 >= 0 && d2 < wst;
-    cands += append_candidates(a.ib, c1, myid, pack(d1, id1), c2, myid, pack(d2, id2), false, 0, 0);
+    cands += append_candidates(a.ib, cur, (uint32_t)n, c1, myid, pack(d1, id1), c2, myid,
+                               pack(d2, id2));
   }
+  if (!kProbe) list_fill(a.ib, cur.pos, cur.end, (uint32_t)n);  // the rest of the last chunk
 }
 
 template <bool kProbe>
@@ -668,7 +692,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane_id() == 0) mma_issuer(sh, tiles, tmem, ntiles, kbc, a.idesc, a.err);
     __syncwarp();
   } else {
-    epilogue<kProbe>(a, sh, tmem, ntiles, stat);
+    epilogue<kProbe>(a, sh, tmem, n, ntiles, stat);
     if (!kProbe) {
 #pragma unroll
       for (int o = 16; o; o >>= 1) stat += __shfl_xor_sync(0xffffffffu, stat, o);

@@ -469,7 +469,16 @@ __device__ __forceinline__ void stage_chunk(const float *__restrict__ X, int d, 
                                             bool vec) {
   const int lane = lane_id();
   const int items = (nn + no) * nq;
-  if (vec) {
+  if (vec && nq == kJc / 4) {  // full chunk: eight pieces per row, no division
+    for (int it = lane; it < items; it += 32) {
+      const int r = it >> 3, q = it & 7;
+      const int slot = r < nn ? r : 32 + (r - nn);
+      const float *src = X + (int64_t)ids[slot] * d + c0 + 4 * q;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(Xs + stage_off(slot, q));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  } else if (vec) {
     for (int it = lane; it < items; it += 32) {
       const int r = it / nq, q = it - r * nq;
       const int slot = r < nn ? r : 32 + (r - nn);
@@ -1051,12 +1060,15 @@ __global__ void k_fix_distances(const float *__restrict__ X, int64_t n, int d,
   }
 }
 
-// Segment [ostart, oend) of every target row in the target-sorted overflow list.
-__global__ void k_ovf_bounds(const uint32_t *__restrict__ tgt, int64_t cnt, uint32_t *__restrict__ ostart,
-                             uint32_t *__restrict__ oend) {
+// Segment [ostart, oend) of every target row in the target-sorted overflow
+// list; sentinel entries (target n, the unused tail of a chunk) sort last and
+// are skipped.
+__global__ void k_ovf_bounds(const uint32_t *__restrict__ tgt, int64_t cnt, int64_t n,
+                             uint32_t *__restrict__ ostart, uint32_t *__restrict__ oend) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t t = tgt[i];
+    if (t >= n) continue;
     if (i == 0 || tgt[i - 1] != t) ostart[t] = (uint32_t)i;
     if (i == cnt - 1 || tgt[i + 1] != t) oend[t] = (uint32_t)(i + 1);
   }
@@ -1247,8 +1259,9 @@ static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
   if (c > ib.ovf_cap) c = ib.ovf_cap;
   // the packed candidates move with their targets, so the merge reads each
   // row's segment contiguously
-  radix_sort_u32_u64(ctx, ib.ovf_tgt, ib.ovf_key, c, 0, bits_for_rows(n));
-  k_ovf_bounds<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_tgt, c, ib.ostart, ib.oend); ctx->launches++;
+  // n + 1 values: the rows and the sentinel n of unused chunk slots
+  radix_sort_u32_u64(ctx, ib.ovf_tgt, ib.ovf_key, c, 0, bits_for_rows(n + 1));
+  k_ovf_bounds<<<grid_for(ctx, c, 256), 256, 0, st>>>(ib.ovf_tgt, c, n, ib.ostart, ib.oend); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_CUDA(cudaMemsetAsync(ib.counters + 3, 0, sizeof(unsigned long long), st));
 }
@@ -1281,8 +1294,11 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
                        tc_dpad(d) <= kTcMaxDpad;
   Buf<uint64_t> inbox(ctx, tc_form ? 1 : (size_t)n * kInboxCap);
   Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
+  // room for a pass's candidates; the tensor-core join's warps also leave the
+  // unused tail of their last list chunk (at most one chunk per epilogue warp)
   const int64_t ovf_rows = tc_form ? 64 : 16;
-  const int64_t ovf_cap = n * ovf_rows > (1 << 22) ? n * ovf_rows : (1 << 22);
+  const int64_t ovf_cap = (n * ovf_rows > (1 << 22) ? n * ovf_rows : (1 << 22)) +
+                          (tc_form ? (int64_t)8 * ctx->num_sms * kListChunk : 0);
   Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
   Buf<uint64_t> ovf_key(ctx, ovf_cap);
   HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));

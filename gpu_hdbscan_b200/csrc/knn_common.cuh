@@ -36,33 +36,58 @@ struct Inbox {
   int64_t ovf_cap;
 };
 
-// Appends this lane's candidates (up to three: target row, packed key; the
+// Space of the candidate list a warp writes into: [pos, end), taken from the
+// list in chunks of kListChunk slots with one atomic on the list's counter,
+// so that the warps of a join do not all queue on that one counter.
+constexpr uint32_t kListChunk = 1024;
+struct ListCursor {
+  unsigned long long pos = 0, end = 0;
+};
+
+// Writes the sentinel entry (target row `n`, sorted after every row and
+// skipped by the segment bounds; key ~0) at list positions [from, to).
+__device__ __forceinline__ void list_fill(const Inbox &ib, unsigned long long from,
+                                          unsigned long long to, uint32_t n) {
+  for (unsigned long long p = from + (threadIdx.x & 31); p < to; p += 32)
+    if ((int64_t)p < ib.ovf_cap) {
+      ib.ovf_tgt[p] = n;
+      ib.ovf_key[p] = ~0ull;
+    }
+}
+
+// Appends this lane's candidates (up to two: target row, packed key; the
 // caller has checked each against its target's worst[]) to the list that is
-// sorted by target before the next merge -- one reservation per warp, no
-// returning atomic per candidate.  Past the list's capacity only the best
-// dropped candidate of each target is kept.  Returns the lane's count.
-__device__ __forceinline__ int append_candidates(const Inbox &ib, bool v0, int32_t t0, uint64_t k0,
-                                                 bool v1, int32_t t1, uint64_t k1, bool v2,
-                                                 int32_t t2, uint64_t k2) {
+// sorted by target before the next merge.  The warp writes them at its
+// cursor; when they do not fit in the cursor's chunk, the rest of that chunk
+// becomes sentinel entries and one lane takes a new chunk.  Past the list's
+// capacity only the best dropped candidate of each target is kept.  Returns
+// the lane's count.  Called by all 32 lanes of a warp; n is the row count.
+__device__ __forceinline__ int append_candidates(const Inbox &ib, ListCursor &cur, uint32_t n,
+                                                 bool v0, int32_t t0, uint64_t k0, bool v1,
+                                                 int32_t t1, uint64_t k1) {
   const int lane = threadIdx.x & 31;
   uint32_t lt;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-  const uint32_t b0 = __ballot_sync(0xffffffffu, v0), b1 = __ballot_sync(0xffffffffu, v1),
-                 b2 = __ballot_sync(0xffffffffu, v2);
-  const uint32_t tot = __popc(b0) + __popc(b1) + __popc(b2);
+  const uint32_t b0 = __ballot_sync(0xffffffffu, v0), b1 = __ballot_sync(0xffffffffu, v1);
+  const uint32_t tot = __popc(b0) + __popc(b1);
   if (tot == 0) return 0;
-  unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(&ib.counters[3], (unsigned long long)tot);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  const unsigned long long p0 = base + __popc(b0 & lt);
-  const unsigned long long p1 = base + __popc(b0) + __popc(b1 & lt);
-  const unsigned long long p2 = base + __popc(b0) + __popc(b1) + __popc(b2 & lt);
-  const int32_t tt[3] = {t0, t1, t2};
-  const uint64_t kk[3] = {k0, k1, k2};
-  const unsigned long long pp[3] = {p0, p1, p2};
-  const bool vv[3] = {v0, v1, v2};
+  if (cur.pos + tot > cur.end) {
+    list_fill(ib, cur.pos, cur.end, n);
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&ib.counters[3], (unsigned long long)kListChunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    cur.pos = base;
+    cur.end = base + kListChunk;
+  }
+  const unsigned long long p0 = cur.pos + __popc(b0 & lt);
+  const unsigned long long p1 = cur.pos + __popc(b0) + __popc(b1 & lt);
+  cur.pos += tot;
+  const int32_t tt[2] = {t0, t1};
+  const uint64_t kk[2] = {k0, k1};
+  const unsigned long long pp[2] = {p0, p1};
+  const bool vv[2] = {v0, v1};
 #pragma unroll
-  for (int q = 0; q < 3; q++) {
+  for (int q = 0; q < 2; q++) {
     if (!vv[q]) continue;
     if ((int64_t)pp[q] < ib.ovf_cap) {
       ib.ovf_tgt[pp[q]] = (uint32_t)tt[q];
@@ -72,7 +97,7 @@ __device__ __forceinline__ int append_candidates(const Inbox &ib, bool v0, int32
       atomicAdd(&ib.counters[0], 1ull);
     }
   }
-  return (v0 ? 1 : 0) + (v1 ? 1 : 0) + (v2 ? 1 : 0);
+  return (v0 ? 1 : 0) + (v1 ? 1 : 0);
 }
 
 __device__ __forceinline__ int push_candidate(int32_t target, int32_t id, float d,
