@@ -171,6 +171,19 @@ def max_over_ranks(ms, device):
     return float(t.item())
 
 
+def all_ranks(v, device):
+    """Every rank's value of a per-rank number, in rank order (the value itself
+    on one rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        out = [torch.zeros_like(t) for _ in range(dist.get_world_size())]
+        dist.all_gather(out, t)
+        return [float(x.item()) for x in out]
+    return [float(t.item())]
+
+
 def sum_over_ranks(v, device):
     """The sum of a per-rank count over all ranks (the value itself on one rank)."""
     import torch
@@ -590,6 +603,8 @@ def run_ours_batch(args, bw):
         if world > 1:
             dist.barrier()
 
+    rank_ms = []
+
     def timed(fn, steps, warmup):
         for _ in range(warmup):
             fn()
@@ -604,12 +619,14 @@ def run_ours_batch(args, bw):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
+        rank_ms[:] = all_ranks(e0.elapsed_time(e1) / steps, dev)
         return max_over_ranks(e0.elapsed_time(e1), dev), out
 
     clocks = ClockSampler(local)
     clocks.start()
     ms_max, outs = timed(lambda: ctx.hdbscan_batched(views, **kw_b), args.steps, args.warmup)
     clk = clocks.stop()
+    per_rank_ms = [round(x, 3) for x in rank_ms]
     stats = [o[2] for o in outs]
     value = n_job * args.steps / (ms_max / 1e3)
     failed = int(sum_over_ranks(sum(1 for s_ in stats[-1]["instance_status"] if s_ != 0), dev))
@@ -704,7 +721,13 @@ def run_ours_batch(args, bw):
                                         ("knn", "graph", "mst", "tree", "total")},
                            "num_clusters": last["num_clusters"], "edges": last["edges"],
                            "knn_dropped": last["knn_dropped"],
-                           "disconnected_instances": failed, "per_instance_loop": loop},
+                           "disconnected_instances": failed, "per_instance_loop": loop,
+                           "per_rank_ms_per_step": per_rank_ms,
+                           "rank_points": (sharding.rank_loads(all_sizes, parts)
+                                           if args.shard_instances else None),
+                           "label_gather": ("not timed: the host gather of labels "
+                                            "(sharding.gather_labels) runs outside the step"
+                                            if args.shard_instances else None)},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
                 "gpu_launches": int(sum(s_["gpu_launches"] for s_ in stats))}
         print(json.dumps(line), flush=True)

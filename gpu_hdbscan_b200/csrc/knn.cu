@@ -71,9 +71,66 @@ constexpr int kStageCols = 32;
 constexpr int kStageLd = kStageCols + 1;                  // conflict-free column walk
 constexpr int kStageFloats = kStageCols + 32 * kStageLd;  // own segment + 32 rows
 
+// 16-byte form for d % 4 == 0 (rows 16-byte aligned): per chunk, lane i loads
+// piece q = i & 7 of rows i >> 3, + 4, ... (eight 16-byte loads in flight per
+// lane) into rows of 32 floats whose pieces are permuted by the row
+// (piece q of row r at q ^ (r & 7)), so the lanes' walks of their own rows
+// read distinct bank groups.  Same sums as below, element by element.
+__device__ __forceinline__ float diffsum_staged_v4(const float *__restrict__ X, int d, int64_t row,
+                                                   int32_t id, bool active, float *__restrict__ sm) {
+  const int lane = lane_id();
+  float *own = sm;
+  float *nb = sm + kStageCols;
+  const uint32_t act = __ballot_sync(0xffffffffu, active);
+  const int q = lane & 7, rb = lane >> 3;
+  int32_t rid[8];
+#pragma unroll
+  for (int t = 0; t < 8; t++) rid[t] = __shfl_sync(0xffffffffu, id, rb + 4 * t);
+  float s = 0.0f;
+  for (int c0 = 0; c0 < d; c0 += kStageCols) {
+    const int nq = min(kStageCols, d - c0) >> 2;  // 16-byte pieces in this chunk
+    __syncwarp();
+    if (lane < 4 * nq) own[lane] = X[row * d + c0 + lane];
+    if (q < nq) {
+      float4 t4[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        const int r = rb + 4 * t;
+        t4[t] = ((act >> r) & 1u)
+                    ? __ldg(reinterpret_cast<const float4 *>(X + (int64_t)rid[t] * d + c0) + q)
+                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      }
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        const int r = rb + 4 * t;
+        *reinterpret_cast<float4 *>(nb + r * kStageCols + 4 * (q ^ (r & 7))) = t4[t];
+      }
+    }
+    __syncwarp();
+    if (active) {
+      const float *mine = nb + lane * kStageCols;
+      for (int p = 0; p < nq; p++) {
+        const float4 b = *reinterpret_cast<const float4 *>(mine + 4 * (p ^ (lane & 7)));
+        const float4 a = *reinterpret_cast<const float4 *>(own + 4 * p);
+        float df = __fsub_rn(a.x, b.x);
+        s = __fmaf_rn(df, df, s);
+        df = __fsub_rn(a.y, b.y);
+        s = __fmaf_rn(df, df, s);
+        df = __fsub_rn(a.z, b.z);
+        s = __fmaf_rn(df, df, s);
+        df = __fsub_rn(a.w, b.w);
+        s = __fmaf_rn(df, df, s);
+      }
+    }
+  }
+  return s;
+}
+
 __device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int d, int64_t row,
                                                 int32_t id, bool active, float *__restrict__ sm) {
   const int lane = lane_id();
+  if ((d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0)
+    return diffsum_staged_v4(X, d, row, id, active, sm);
   float *own = sm;
   float *nb = sm + kStageCols;
   const uint32_t act = __ballot_sync(0xffffffffu, active);
@@ -117,8 +174,13 @@ __device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int
 
 // With instances (seg.count > 0) every row draws from its own instance with
 // the instance-local position and size, so an instance starts from the graph
-// a run on that instance alone starts from.
+// a run on that instance alone starts from.  With a renumbering (order: new
+// row -> caller's row, inv: caller's row -> new row; X in the new numbering)
+// the ids are drawn for the caller's row from the caller's numbering and then
+// mapped, so the lists are exactly the caller-numbered initial graph
+// renumbered (instances keep their ranges under the renumbering).
 __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Segments seg,
+                       const uint32_t *__restrict__ order, const int32_t *__restrict__ inv,
                        int32_t *__restrict__ gid, float *__restrict__ gdist,
                        float *__restrict__ worst) {
   extern __shared__ float smem_stage[];
@@ -133,7 +195,7 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Seg
       base = seg.off[t];
       cnt = seg.off[t + 1] - base;
     }
-    const int64_t lrow = row - base;
+    const int64_t lrow = (order ? (int64_t)order[row] : row) - base;
     // InitKNNGraphIndexKernel (nndescent.cu:1673-1692): xorshift64star(pos) % n,
     // advanced past the row itself -- and here also past ids already taken.
     int64_t label = (int64_t)(xorshift64star((uint64_t)(lrow * k + lane)) % (uint64_t)cnt);
@@ -146,6 +208,7 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Seg
       }
     }
     label += base;
+    if (order && lane < k) label = inv[label];
     const float ds = diffsum_staged(X, d, row, (int32_t)label, lane < k, sm);
     uint64_t key = ~0ull;
     if (lane < k) key = pack(ds, (int32_t)label);
@@ -301,9 +364,20 @@ __device__ __forceinline__ void merge_chunk(int k, uint64_t &rkey, int32_t &lab,
   if (__ballot_sync(0xffffffffu, ok) == 0) return;
   const int32_t cid = pk_id(cand);
   const int32_t rid = pk_id(rkey);
-  for (int t = 0; t < k; t++) {
-    const int32_t r = __shfl_sync(0xffffffffu, rid, t);  // every lane takes part
-    ok = ok && cid != r;
+  const uint32_t okm = __ballot_sync(0xffffffffu, ok);
+  if (__popc(okm) <= 8) {
+    // few candidates below the k-th key (the common case once rows settle):
+    // one vote of the row per candidate
+    for (uint32_t m = okm; m; m &= m - 1) {
+      const int t = __ffs(m) - 1;
+      const int32_t c = __shfl_sync(0xffffffffu, cid, t);
+      if (__any_sync(0xffffffffu, have && rid == c) && lane == t) ok = false;
+    }
+  } else {
+    for (int t = 0; t < k; t++) {
+      const int32_t r = __shfl_sync(0xffffffffu, rid, t);  // every lane takes part
+      ok = ok && cid != r;
+    }
   }
   const uint32_t same = __match_any_sync(0xffffffffu, ok ? cid : -1 - lane);
   ok = ok && (__ffs(same) - 1 == lane);
@@ -1182,9 +1256,8 @@ __global__ void k_loc_rows(const float *__restrict__ X, const uint32_t *__restri
   }
 }
 
-// Row r of the output takes row src[r] of the input with every id mapped
-// through idmap; the row is re-sorted by (distance, mapped id) and each entry
-// keeps its old/new flag.  One warp per row.
+// A row with every id mapped through idmap, re-sorted by (distance, mapped
+// id); each entry keeps its old/new flag.  One warp per row.
 __device__ __forceinline__ void remap_row(int k, int32_t in_lab, float in_dist,
                                           const int32_t *__restrict__ idmap, int32_t &out_lab,
                                           float &out_dist) {
@@ -1202,28 +1275,6 @@ __device__ __forceinline__ void remap_row(int k, int32_t in_lab, float in_dist,
   }
   out_dist = pk_dist(key);
   out_lab = flag ? -mine - 1 : mine;
-}
-
-__global__ void k_loc_lists(const int32_t *__restrict__ gid, const float *__restrict__ gdist,
-                            const float *__restrict__ worst, const uint32_t *__restrict__ order,
-                            const int32_t *__restrict__ inv, int64_t n, int k,
-                            int32_t *__restrict__ gid_p, float *__restrict__ gdist_p,
-                            float *__restrict__ worst_p) {
-  const int lane = lane_id(), wpb = blockDim.x >> 5;
-  for (int64_t r = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); r < n;
-       r += (int64_t)gridDim.x * wpb) {
-    const int64_t o = order[r];
-    const int32_t lab = lane < k ? gid[o * k + lane] : 0;
-    const float dist = lane < k ? gdist[o * k + lane] : 0.0f;
-    int32_t ol;
-    float od;
-    remap_row(k, lab, dist, inv, ol, od);
-    if (lane < k) {
-      gid_p[r * k + lane] = ol;
-      gdist_p[r * k + lane] = od;
-    }
-    if (lane == 0) worst_p[r] = worst[o];
-  }
 }
 
 __global__ void k_loc_restore(const hdb_nnd_element *__restrict__ Gp, const uint32_t *__restrict__ order,
@@ -1318,11 +1369,9 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
-  k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, seg, gid, gdist, worst); ctx->launches++;
-  HDB_CHECK_LAUNCH();
-
   // renumber the points in locality order (k_loc_project); X stays the
-  // caller's, the iterations work on Xw and the renumbered lists
+  // caller's, the iterations work on Xw and the renumbered lists, and the
+  // initial graph is drawn straight into the new numbering
   Buf<uint32_t> order(ctx, n);
   Buf<float> Xp(ctx, (size_t)n * d);
   {
@@ -1340,14 +1389,10 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
     Buf<int32_t> inv(ctx, n);
     k_loc_inverse<<<grid_for(ctx, n, 256), 256, 0, st>>>(order, n, inv); ctx->launches++;
     k_loc_rows<<<grid_rows, 32 * wpb, 0, st>>>(X, order, n, d, Xp); ctx->launches++;
-    Buf<int32_t> gid2(ctx, n * k);
-    Buf<float> gdist2(ctx, n * k), worst2(ctx, n);
-    k_loc_lists<<<grid_rows, 32 * wpb, 0, st>>>(gid, gdist, worst, order, inv, n, k, gid2, gdist2,
-                                                worst2); ctx->launches++;
     HDB_CHECK_LAUNCH();
-    std::swap(gid, gid2);
-    std::swap(gdist, gdist2);
-    std::swap(worst, worst2);
+    k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(Xp, n, d, k, seg, order, inv, gid, gdist, worst);
+    ctx->launches++;
+    HDB_CHECK_LAUNCH();
   }
   const float *Xw = Xp;
   Buf<hdb_nnd_element> Gp(ctx, (size_t)n * k);
