@@ -12,14 +12,14 @@
 // distance = ||a||^2 + ||c||^2 - 2 a.c with the norms of the rounded rows, as
 // in the SIMT BF16 join.
 //
-// Warp roles (224 threads, a persistent loop over tiles):
-//   warps 4, 5  producers (alternate tiles): slot lists into the tile's
+// Warp roles (256 threads, a persistent loop over tiles):
+//   warps 4-6   producers (take tiles in turn): slot lists into the tile's
 //               metadata slot (ids, nn / no, cp.async of the rows' norms and
 //               worst[]), then TMA gathers of the rows, one 64-element K block
 //               of the tile per operand stage; a TMA gather occupies its
 //               issuing warp for a while, so two warps keep more gathers in
 //               flight;
-//   warp 6      one thread issues the MMAs, K block by K block, and commits
+//   warp 7      one thread issues the MMAs, K block by K block, and commits
 //               each operand stage back to its producer as soon as the MMAs
 //               reading it are done, and the finished tile to the epilogue;
 //   warps 0..3  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
@@ -64,7 +64,7 @@ constexpr int kKBlockBytes = kTcTileRows * 128;  // one 64-element K block of a 
 constexpr int kAccCols = 128;                     // FP32 accumulator columns (N)
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kEpiWarps = 4;
-constexpr int kProducers = 2;  // producer warps, alternating tiles
+constexpr int kProducers = 3;  // producer warps, alternating tiles
 constexpr int kProducerWarp0 = kEpiWarps;
 constexpr int kMmaWarp = kProducerWarp0 + kProducers;
 constexpr int kThreads = 32 * (kMmaWarp + 1);
@@ -287,13 +287,17 @@ __global__ void k_join_lists(int64_t n, int S, int32_t *__restrict__ newS, int32
   int32_t *olds = olds_smem[threadIdx.x >> 5];
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
+    // the row's counts and both lists are loaded together (the lists do not
+    // wait for the counts: one memory round trip per row)
+    const int64_t sb = row * (2 * S);
+    const int32_t nraw = lane < 2 * S ? newS[sb + lane] : 0;
+    const int32_t oraw = lane < 2 * S ? oldS[sb + lane] : 0;
     const int cnf = nf[row], cof = of[row];
     const int cnr = min(nrev[row], S), cor = min(orev[row], S);
-    const int64_t sb = row * (2 * S);
     bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
     bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
-    const int32_t nid = vn ? newS[sb + lane] : -1 - lane;
-    const int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    const int32_t nid = vn ? nraw : -1 - lane;
+    const int32_t oid = vo ? oraw : -100 - lane;
     const uint32_t pn = __match_any_sync(0xffffffffu, nid);
     vn = vn && (__ffs(pn) - 1 == lane);
     const uint32_t po = __match_any_sync(0xffffffffu, oid);

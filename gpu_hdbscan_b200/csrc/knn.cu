@@ -628,16 +628,19 @@ __global__ void __launch_bounds__(32 * kJoinWarps, 2)
   unsigned long long w_rows = 0, w_cands = 0;
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
+    // counts and both sample lists in one memory round trip
+    const int64_t sb = row * (2 * S);
+    const int32_t nraw = lane < 2 * S ? newS[sb + lane] : 0;
+    const int32_t oraw = lane < 2 * S ? oldS[sb + lane] : 0;
     const int cnf = nf[row], cof = of[row];
     const int cnr = min(nrev[row], S), cor = min(orev[row], S);
     __syncwarp();
     if (lane == 0) { nrev[row] = 0; orev[row] = 0; }
-    const int64_t sb = row * (2 * S);
     // slot t < S: forward sample t; slot S + t: reverse sample t
     bool vn = (lane < S) ? (lane < cnf) : (lane < 2 * S && lane - S < cnr);
     bool vo = (lane < S) ? (lane < cof) : (lane < 2 * S && lane - S < cor);
-    const int32_t nid = vn ? newS[sb + lane] : -1 - lane;
-    const int32_t oid = vo ? oldS[sb + lane] : -100 - lane;
+    const int32_t nid = vn ? nraw : -1 - lane;
+    const int32_t oid = vo ? oraw : -100 - lane;
     // de-duplicate (ShrinkGraph RemoveDuplicates, :285-291)
     const uint32_t pn = __match_any_sync(0xffffffffu, nid);
     vn = vn && (__ffs(pn) - 1 == lane);
