@@ -547,6 +547,7 @@ __device__ void mma_issuer(Shared &sh, unsigned char *tiles, uint32_t tmem, int6
 
 // Row minimum over 32 columns: key = clamped distance bits with the column in
 // the low 6 bits (skip_col: the row's own column, or -1).
+template <bool kSkip>
 __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const float *cn, float na,
                                               float dscale, int skip_col) {
   uint32_t best[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};  // four chains
@@ -559,7 +560,7 @@ __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const flo
       const int c = 4 * c4 + e;
       const float dd = fmaxf(__fmaf_rn(dscale, __uint_as_float(v[c]), __fadd_rn(na, ncs[e])), 0.0f);
       uint32_t key = (__float_as_uint(dd) & ~63u) | (uint32_t)c;
-      key = c == skip_col ? 0xffffffffu : key;
+      if (kSkip) key = c == skip_col ? 0xffffffffu : key;
       best[e] = min(best[e], key);
     }
   }
@@ -622,11 +623,11 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     uint32_t k1, k2 = 0xffffffffu;
     int32_t id1 = -1, id2 = -1;
     if (isnew) {
-      k1 = row_min32(v0, cn, na, a.dscale, lane);     // closest other new row
-      k2 = row_min32(v1, cn + 32, na, a.dscale, -1);  // closest old row
+      k1 = row_min32<true>(v0, cn, na, a.dscale, lane);       // closest other new row
+      k2 = row_min32<false>(v1, cn + 32, na, a.dscale, -1);   // closest old row
       if (k2 < kNoKey) id2 = M.ids[64 * j + 32 + (k2 & 63u)];
     } else {
-      k1 = row_min32(v0, cn, na, a.dscale, -1);       // closest new row
+      k1 = row_min32<false>(v0, cn, na, a.dscale, -1);        // closest new row
     }
     if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
     __syncwarp();

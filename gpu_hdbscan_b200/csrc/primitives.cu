@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist(const K *__restrict__
 // threads to consecutive addresses.  Values of type V (u32 or u64) move with
 // their keys when kVals.
 template <typename K, typename V, bool kVals, int kBins, int kItems, bool kTileMajor>
-__global__ void __launch_bounds__(kSortThreads) radix_scatter(
+__global__ void __launch_bounds__(kSortThreads, 3) radix_scatter(
     const K *__restrict__ keys_in, const V *__restrict__ vals_in, K *__restrict__ keys_out,
     V *__restrict__ vals_out, const uint32_t *__restrict__ offsets, int64_t n, int shift,
     uint32_t mask, uint32_t nblocks) {

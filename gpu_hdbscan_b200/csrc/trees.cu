@@ -35,28 +35,34 @@ namespace {
 // ---------------------------------------------------------------------------
 // Union-find over labels [0, 2n-1); hooks always point to a smaller label, so
 // every path ends at a root.  The step bounds only guard against corrupted
-// state and report through the device error word.
+// state and report through the device error word.  A label's state at one
+// level -- parent, the largest rank tagged to it (as a root), whether it was
+// counted, the points its root accumulated -- is one 16-byte record, so the
+// reset of a label is one store and a root's fields share a sector.
 constexpr int64_t kUfBound = int64_t(1) << 31;
 
-__device__ __forceinline__ int32_t uf_find(volatile int32_t *p, int32_t x) {
+struct __align__(16) UfNode {
+  int32_t p, maxr, seen, acc;
+};
+
+__device__ __forceinline__ int32_t uf_find(UfNode *u, int32_t x) {
   for (int64_t s = 0; s < kUfBound; s++) {
-    int32_t px = p[x];
+    const int32_t px = *reinterpret_cast<volatile int32_t *>(&u[x].p);
     if (px == x) return x;
-    int32_t ppx = p[px];
-    if (ppx != px) p[x] = ppx;
+    const int32_t ppx = *reinterpret_cast<volatile int32_t *>(&u[px].p);
+    if (ppx != px) *reinterpret_cast<volatile int32_t *>(&u[x].p) = ppx;
     x = px;
   }
   return x;
 }
 
-__device__ __forceinline__ void uf_union(int32_t *p, int32_t a, int32_t b, uint32_t *err) {
-  volatile int32_t *vp = p;
+__device__ __forceinline__ void uf_union(UfNode *u, int32_t a, int32_t b, uint32_t *err) {
   for (int64_t s = 0; s < kUfBound; s++) {
-    a = uf_find(vp, a);
-    b = uf_find(vp, b);
+    a = uf_find(u, a);
+    b = uf_find(u, b);
     if (a == b) return;
     if (a > b) { int32_t t = a; a = b; b = t; }
-    if (atomicCAS(&p[b], b, a) == b) return;
+    if (atomicCAS(&u[b].p, b, a) == b) return;
   }
   atomicOr(err, DEVERR_TIMEOUT);
 }
@@ -77,24 +83,20 @@ __global__ void k_link_init(const hdb_mst_edge *__restrict__ mst, int64_t m,
   }
 }
 
-__global__ void k_uf_init(int64_t total, int64_t n, int32_t *__restrict__ ufp,
-                          int32_t *__restrict__ maxr, int32_t *__restrict__ seen,
-                          int32_t *__restrict__ acc, int32_t *__restrict__ size) {
+__global__ void k_uf_init(int64_t total, int64_t n, UfNode *__restrict__ u,
+                          int32_t *__restrict__ size) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    ufp[i] = (int32_t)i;
-    maxr[i] = -1;
-    seen[i] = 0;
-    acc[i] = 0;
+    u[i] = UfNode{(int32_t)i, -1, 0, 0};
     size[i] = i < n ? 1 : 0;
   }
 }
 
 __global__ void k_level_union(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
-                              int64_t m, int64_t S, int32_t *ufp, uint32_t *err) {
+                              int64_t m, int64_t S, UfNode *u, uint32_t *err) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x)
-    if (active_lower(r, S, m)) uf_union(ufp, la[r], lb[r], err);
+    if (active_lower(r, S, m)) uf_union(u, la[r], lb[r], err);
 }
 
 // MST input check: endpoints in [0, n).
@@ -109,57 +111,50 @@ __global__ void k_validate_mst(const hdb_mst_edge *__restrict__ mst, int64_t m, 
 }
 
 __global__ void k_level_tag(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
-                            int64_t m, int64_t S, int64_t n, int32_t *ufp, int32_t *maxr,
-                            int32_t *seen, int32_t *acc, const int32_t *__restrict__ size) {
-  volatile int32_t *vp = ufp;
+                            int64_t m, int64_t S, int64_t n, UfNode *u,
+                            const int32_t *__restrict__ size) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     if (!active_lower(r, S, m)) continue;
     int32_t a = la[r], b = lb[r];
-    int32_t root = uf_find(vp, a);
-    atomicMax(&maxr[root], (int32_t)r);
-    if (atomicExch(&seen[a], 1) == 0) atomicAdd(&acc[root], a < n ? 1 : size[a]);
-    if (atomicExch(&seen[b], 1) == 0) atomicAdd(&acc[root], b < n ? 1 : size[b]);
+    int32_t root = uf_find(u, a);
+    atomicMax(&u[root].maxr, (int32_t)r);
+    if (atomicExch(&u[a].seen, 1) == 0) atomicAdd(&u[root].acc, a < n ? 1 : size[a]);
+    if (atomicExch(&u[b].seen, 1) == 0) atomicAdd(&u[root].acc, b < n ? 1 : size[b]);
   }
 }
 
 __global__ void k_level_produce(const int32_t *__restrict__ la, int64_t m, int64_t S, int64_t n,
-                                int32_t *ufp, const int32_t *__restrict__ maxr,
-                                const int32_t *__restrict__ acc, int32_t *__restrict__ size) {
-  volatile int32_t *vp = ufp;
+                                UfNode *u, int32_t *__restrict__ size) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     if (!active_lower(r, S, m)) continue;
-    int32_t root = uf_find(vp, la[r]);
-    if (maxr[root] == (int32_t)r) size[n + r] = acc[root];
+    const int32_t root = uf_find(u, la[r]);
+    if (u[root].maxr == (int32_t)r) size[n + r] = u[root].acc;
   }
 }
 
 __global__ void k_level_relabel(int32_t *__restrict__ la, int32_t *__restrict__ lb, int64_t m,
-                                int64_t S, int64_t n, int32_t *ufp,
-                                const int32_t *__restrict__ maxr) {
-  volatile int32_t *vp = ufp;
+                                int64_t S, int64_t n, UfNode *u) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     if ((r & (S - 1)) < (S >> 1)) continue;
     int32_t a = la[r], b = lb[r];
-    int32_t ra = uf_find(vp, a), rb = uf_find(vp, b);
-    int32_t ma = maxr[ra], mb = maxr[rb];
+    int32_t ra = uf_find(u, a), rb = uf_find(u, b);
+    int32_t ma = u[ra].maxr, mb = u[rb].maxr;
     if (ma >= 0) la[r] = (int32_t)(n + ma);
     if (mb >= 0) lb[r] = (int32_t)(n + mb);
   }
 }
 
 __global__ void k_level_reset(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
-                              int64_t m, int64_t S, int32_t *__restrict__ ufp,
-                              int32_t *__restrict__ maxr, int32_t *__restrict__ seen,
-                              int32_t *__restrict__ acc) {
+                              int64_t m, int64_t S, UfNode *__restrict__ u) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
        r += (int64_t)gridDim.x * blockDim.x) {
     if (!active_lower(r, S, m)) continue;
-    int32_t a = la[r], b = lb[r];
-    ufp[a] = a; maxr[a] = -1; seen[a] = 0; acc[a] = 0;
-    ufp[b] = b; maxr[b] = -1; seen[b] = 0; acc[b] = 0;
+    const int32_t a = la[r], b = lb[r];
+    u[a] = UfNode{a, -1, 0, 0};
+    u[b] = UfNode{b, -1, 0, 0};
   }
 }
 
@@ -805,24 +800,24 @@ void linkage_tree(Context *ctx, const hdb_mst_edge *mst, int64_t n, hdb_linkage_
   HDB_REQUIRE(n >= 2 && n < (int64_t(1) << 30), HDB_ERR_ARG, "linkage tree: bad n");
   cudaStream_t st = ctx->stream;
   const int64_t m = n - (seg.count > 0 ? seg.count : 1), total = n + m;
-  Buf<int32_t> la(ctx, m), lb(ctx, m), ufp(ctx, total), maxr(ctx, total), seen(ctx, total),
-      acc(ctx, total), size(ctx, total);
+  Buf<int32_t> la(ctx, m), lb(ctx, m), size(ctx, total);
+  Buf<UfNode> u(ctx, total);
   const int gm = grid_for(ctx, m, 256), gt = grid_for(ctx, total, 256);
   k_validate_mst<<<gm, 256, 0, st>>>(mst, m, n, ctx->dev_err); ctx->launches++;
   HDB_CHECK_LAUNCH();
   HDB_REQUIRE(!(ctx->take_dev_err() & DEVERR_ID_RANGE), HDB_ERR_ARG,
               "linkage tree: MST edge endpoint outside [0, n)");
   k_link_init<<<gm, 256, 0, st>>>(mst, m, la, lb); ctx->launches++;
-  k_uf_init<<<gt, 256, 0, st>>>(total, n, ufp, maxr, seen, acc, size); ctx->launches++;
+  k_uf_init<<<gt, 256, 0, st>>>(total, n, u, size); ctx->launches++;
   HDB_CHECK_LAUNCH();
   int64_t S = 1;
   while (S < m) S <<= 1;
   for (; S >= 2; S >>= 1) {
-    k_level_union<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, ctx->dev_err); ctx->launches++;
-    k_level_tag<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr, seen, acc, size); ctx->launches++;
-    k_level_produce<<<gm, 256, 0, st>>>(la, m, S, n, ufp, maxr, acc, size); ctx->launches++;
-    k_level_relabel<<<gm, 256, 0, st>>>(la, lb, m, S, n, ufp, maxr); ctx->launches++;
-    k_level_reset<<<gm, 256, 0, st>>>(la, lb, m, S, ufp, maxr, seen, acc); ctx->launches++;
+    k_level_union<<<gm, 256, 0, st>>>(la, lb, m, S, u, ctx->dev_err); ctx->launches++;
+    k_level_tag<<<gm, 256, 0, st>>>(la, lb, m, S, n, u, size); ctx->launches++;
+    k_level_produce<<<gm, 256, 0, st>>>(la, m, S, n, u, size); ctx->launches++;
+    k_level_relabel<<<gm, 256, 0, st>>>(la, lb, m, S, n, u); ctx->launches++;
+    k_level_reset<<<gm, 256, 0, st>>>(la, lb, m, S, u); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
   k_link_out<<<gm, 256, 0, st>>>(mst, la, lb, size, m, n, out); ctx->launches++;
