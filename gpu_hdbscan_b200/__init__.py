@@ -64,6 +64,11 @@ class Context:
         # run on torch's current stream so torch allocations order correctly
         _lib.check(self.L.hdb_set_stream(self.h, C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
 
+    def set_join_tiles(self, tiles: int):
+        """FP32 local join form: 1 or 2 distance tiles of 4 x 4 per lane, or 0
+        to time both per shape and keep the faster (the default)."""
+        _lib.check(self.L.hdb_set_join_tiles(self.h, int(tiles)))
+
     def close(self):
         if getattr(self, "h", None):
             self.L.hdb_destroy(self.h)

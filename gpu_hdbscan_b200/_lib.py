@@ -22,7 +22,8 @@ HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
 
 # Every symbol include/hdb/hdb.h declares.
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
-           "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances", "hdb_enhanced_knng", "hdb_mst",
+           "hdb_set_join_tiles", "hdb_nndescent", "hdb_knn_split", "hdb_fix_distances",
+           "hdb_enhanced_knng", "hdb_mst",
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_with_graph", "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
            "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised",
@@ -59,7 +60,7 @@ class RunStats(C.Structure):
                 ("join_ms", C.c_float), ("join_launches", C.c_int32),
                 ("join_rows_gathered", C.c_int64), ("join_candidates", C.c_int64),
                 ("gpu_launches", C.c_int64), ("mst_multiplier", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("join_config", C.c_int32)]
 
 
 class Instance(C.Structure):
@@ -87,6 +88,7 @@ def load(path: str = LIB_PATH):
         "hdb_create": (C.c_int, [C.POINTER(_P), _I32]),
         "hdb_destroy": (C.c_int, [_P]),
         "hdb_set_stream": (C.c_int, [_P, _P]),
+        "hdb_set_join_tiles": (C.c_int, [_P, _I32]),
         "hdb_nndescent": (C.c_int, [_P, _P, _I64, _I32, C.POINTER(KnnParams), _P]),
         "hdb_knn_merge": (C.c_int, [_P, _P, _I64, _P, _P, _I64, _P, _I32,
                                     C.POINTER(KnnParams), _P]),

@@ -638,6 +638,7 @@ hdb_status run_single(hdb_ctx *h, const float *X, int64_t n, int32_t d, const hd
       fill_times(ctx, &rs, true);
       rs.join_ms = (float)js.ms;
       rs.join_launches = (int32_t)js.launches;
+      rs.join_config = js.config;
       rs.join_rows_gathered = js.rows_gathered;
       rs.join_candidates = js.candidates;
       rs.gpu_launches = ctx->launches - launches0;
@@ -715,6 +716,7 @@ hdb_status run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count, const hdb
       rs.ms_total = elapsed(ctx->ev[0], ctx->ev[6]);
       rs.join_ms = (float)js.ms;
       rs.join_launches = (int32_t)js.launches;
+      rs.join_config = js.config;
       rs.join_rows_gathered = js.rows_gathered;
       rs.join_candidates = js.candidates;
       rs.gpu_launches = ctx->launches - launches0;

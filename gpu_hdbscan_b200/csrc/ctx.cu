@@ -139,6 +139,7 @@ HDB_API hdb_status hdb_create(hdb_ctx **out, int32_t device) {
     Context &c = h->c;
     c.device = device;
     c.num_sms = prop.multiProcessorCount;
+    c.l2_bytes = prop.l2CacheSize;
     try {
       HDB_CUDA(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
       c.stream = c.own_stream;
@@ -183,6 +184,14 @@ HDB_API hdb_status hdb_set_stream(hdb_ctx *h, void *stream) {
     // cached scratch blocks were last used in the old stream's order
     if (h->c.stream) HDB_CUDA(cudaStreamSynchronize(h->c.stream));
     h->c.stream = stream ? static_cast<cudaStream_t>(stream) : h->c.own_stream;
+  });
+}
+
+HDB_API hdb_status hdb_set_join_tiles(hdb_ctx *h, int32_t tiles) {
+  return guard([&] {
+    HDB_REQUIRE(h != nullptr, HDB_ERR_ARG, "hdb_set_join_tiles: NULL context");
+    HDB_REQUIRE(tiles >= 0 && tiles <= 2, HDB_ERR_ARG, "hdb_set_join_tiles: tiles must be 0, 1 or 2");
+    h->c.join_tiles = tiles;
   });
 }
 

@@ -111,6 +111,10 @@ constexpr size_t kPinnedErrOffset = 3072;
 struct Context {
   int device = 0;
   int num_sms = 148;
+  int64_t l2_bytes = 126 << 20;
+  // FP32 local join tile slots per lane: 0 = tuned per shape, 1 or 2 forced
+  // (hdb_set_join_tiles)
+  int join_tiles = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   uint32_t *dev_err = nullptr;   // [4] device error words

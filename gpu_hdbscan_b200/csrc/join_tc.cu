@@ -567,6 +567,41 @@ __device__ __forceinline__ uint32_t row_min32(const uint32_t (&v)[32], const flo
   return min(min(best[0], best[1]), min(best[2], best[3]));
 }
 
+// row_min32 of this lane's row (keys carry the column) and, from the same
+// distances, the minimum of every column over the warp's 32 rows: on return
+// lane l holds column l's minimum, keyed by the row's lane.  The column minima
+// take 31 shuffles: at each step a lane keeps half of its live columns and
+// takes the other lane's values for them (recursive halving).
+__device__ __forceinline__ uint32_t row_col_min32(uint32_t (&v)[32], const float *cn, float na,
+                                                  float dscale, int lane, uint32_t &colmin) {
+  uint32_t best[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+#pragma unroll
+  for (int c4 = 0; c4 < 8; c4++) {
+    const float4 nc = reinterpret_cast<const float4 *>(cn)[c4];
+    const float ncs[4] = {nc.x, nc.y, nc.z, nc.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int c = 4 * c4 + e;
+      const float dd = fmaxf(__fmaf_rn(dscale, __uint_as_float(v[c]), __fadd_rn(na, ncs[e])), 0.0f);
+      const uint32_t db = __float_as_uint(dd) & ~63u;
+      best[e] = min(best[e], db | (uint32_t)c);
+      v[c] = db | (uint32_t)lane;
+    }
+  }
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool up = (lane & s) != 0;
+#pragma unroll
+    for (int i = 0; i < s; i++) {
+      const uint32_t send = up ? v[i] : v[i + s];
+      const uint32_t keep = up ? v[i + s] : v[i];
+      v[i] = min(keep, __shfl_xor_sync(0xffffffffu, send, s));
+    }
+  }
+  colmin = v[0];
+  return min(min(best[0], best[1]), min(best[2], best[3]));
+}
+
 template <bool kProbe>
 __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n, int64_t ntiles,
                          unsigned long long &cands) {
@@ -599,11 +634,11 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     uint32_t v0[32], v1[32];
     const uint32_t taddr = tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(b * kAccCols + 64 * j);
     tmem_ld32(taddr, v0);
-    if (kProbe || isnew) {  // both loads in flight, one wait
+    if (kProbe) {  // both loads in flight, one wait
       tmem_ld32(taddr + 32, v1);
       tmem_wait_ld2(v0, v1);
     } else {
-      tmem_wait_ld(v0);
+      tmem_wait_ld(v0);  // the new columns: the old ones come from the old rows' warp
     }
     tc_fence_before();
     __syncwarp();
@@ -620,14 +655,20 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
       if (lane == 0) mbar_arrive(&sh.mempty[m]);
       continue;
     }
+    // new rows: their closest other new row.  Old rows: their closest new
+    // row, and -- the new x old block being the transpose of the old x new
+    // one -- the closest old row of every new row, as column minima over the
+    // old rows; lane l then speaks for new row l.
     uint32_t k1, k2 = 0xffffffffu;
-    int32_t id1 = -1, id2 = -1;
+    int32_t id1 = -1, id2 = -1, tgt2 = -1;
+    float wst2 = 0.0f;
     if (isnew) {
-      k1 = row_min32<true>(v0, cn, na, a.dscale, lane);       // closest other new row
-      k2 = row_min32<false>(v1, cn + 32, na, a.dscale, -1);   // closest old row
-      if (k2 < kNoKey) id2 = M.ids[64 * j + 32 + (k2 & 63u)];
+      k1 = row_min32<true>(v0, cn, na, a.dscale, lane);
     } else {
-      k1 = row_min32<false>(v0, cn, na, a.dscale, -1);        // closest new row
+      k1 = row_col_min32(v0, cn, na, a.dscale, lane, k2);
+      if (k2 < kNoKey) id2 = M.ids[64 * j + 32 + (k2 & 63u)];
+      tgt2 = M.ids[64 * j + lane];
+      wst2 = M.wst[64 * j + lane];
     }
     if (k1 < kNoKey) id1 = M.ids[64 * j + (k1 & 63u)];
     __syncwarp();
@@ -636,8 +677,9 @@ __device__ void epilogue(const JoinArgs &a, Shared &sh, uint32_t tmem, int64_t n
     // that is sorted by target before the next merge: one reservation per
     // warp instead of a returning inbox atomic per candidate
     const float d1 = __uint_as_float(k1 & ~63u), d2 = __uint_as_float(k2 & ~63u);
-    const bool c1 = vrow && id1 >= 0 && d1 < wst, c2 = vrow && id2 >= 0 && d2 < wst;
-    cands += append_candidates(a.ib, cur, (uint32_t)n, c1, myid, pack(d1, id1), c2, myid,
+    const bool c1 = vrow && id1 >= 0 && d1 < wst;
+    const bool c2 = !isnew && lane < nn && id2 >= 0 && d2 < wst2;
+    cands += append_candidates(a.ib, cur, (uint32_t)n, c1, myid, pack(d1, id1), c2, tgt2,
                                pack(d2, id2));
   }
   if (!kProbe) list_fill(a.ib, cur.pos, cur.end, (uint32_t)n);  // the rest of the last chunk

@@ -17,8 +17,12 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "hdb_internal.cuh"
@@ -521,7 +525,6 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
 // of every staged row.  Rows are staged a chunk at a time, so a warp needs
 // ~9 KB whatever d is and an SM keeps 16 warps of joins in flight.
 constexpr int kJc = 32;              // dimensions per staged chunk
-constexpr int kJoinTiles = 2;        // 4 x 4 register tiles per lane and pass (64 per pass)
 constexpr int kJoinWarps = 8;
 struct JoinSmem {
   static constexpr int kBest = 96;   // u64 entries
@@ -611,7 +614,11 @@ __device__ __forceinline__ int tile_of(int t, int rg, int cgn, int cgo, int &r0,
 // :1328-1383 launched without the new x new kernel, UpdateGraphForMerge
 // :1582-1640) leaves out the new x new tiles: new neighbours get their closest
 // old one only.
-__global__ void __launch_bounds__(32 * kJoinWarps, 2)
+// kTiles: 4 x 4 register tiles per lane and pass (32 * kTiles per pass over
+// the staged rows); one tile needs 80 registers and fits three blocks per SM,
+// two need 122 and fit two -- the FP32 join tuner picks per (d, k, S).
+template <int kTiles>
+__global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
     k_join(const float *__restrict__ X, int64_t n, int d, int S, const int32_t *__restrict__ newS,
            const int32_t *__restrict__ oldS, const int8_t *__restrict__ nf,
            const int8_t *__restrict__ of, int32_t *__restrict__ nrev, int32_t *__restrict__ orev,
@@ -669,13 +676,13 @@ __global__ void __launch_bounds__(32 * kJoinWarps, 2)
     const int rg = (nn + 3) >> 2;                              // row groups (new rows)
     const int cgn = cross_only ? 0 : rg, cgo = (no + 3) >> 2;  // column groups: new, old
     const int tiles = (cgn > 0 ? rg * (rg + 1) / 2 : 0) + rg * cgo;
-    // up to 64 tiles per pass through the rows (rows with more samples
-    // than that -- at most 100 tiles -- take a second pass)
-    for (int t0 = 0; t0 < tiles; t0 += 32 * kJoinTiles) {
-      int r0[kJoinTiles], c0[kJoinTiles], kind[kJoinTiles];
-      float acc[kJoinTiles][4][4];
+    // up to 32 * kTiles tiles per pass through the rows (rows with more
+    // samples take further passes; at most 100 tiles)
+    for (int t0 = 0; t0 < tiles; t0 += 32 * kTiles) {
+      int r0[kTiles], c0[kTiles], kind[kTiles];
+      float acc[kTiles][4][4];
 #pragma unroll
-      for (int u = 0; u < kJoinTiles; u++) {
+      for (int u = 0; u < kTiles; u++) {
         const int t = t0 + lane + 32 * u;
         kind[u] = t < tiles ? tile_of(t, rg, cgn, cgo, r0[u], c0[u]) : 0;
         if (kind[u] == 0) { r0[u] = 0; c0[u] = 0; }
@@ -689,7 +696,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, 2)
         __syncwarp();  // the previous chunk is no longer read
         stage_chunk(X, d, cd, nq, ids, nn, no, Xs, vec);
 #pragma unroll
-        for (int u = 0; u < kJoinTiles; u++) {
+        for (int u = 0; u < kTiles; u++) {
           if (kind[u] == 0) continue;
           // the four rows of a tile side share one piece permutation
           const int ka = (r0[u] >> 2) & 7, kc = (c0[u] >> 2) & 7;
@@ -719,7 +726,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, 2)
       }
       // tile minima -> per-row best candidates
 #pragma unroll
-      for (int u = 0; u < kJoinTiles; u++) {
+      for (int u = 0; u < kTiles; u++) {
         if (kind[u] == 0) continue;
         const bool oldcols = kind[u] == 3;
         const int ncol = oldcols ? no : nn;
@@ -1320,6 +1327,171 @@ static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
   HDB_CUDA(cudaMemsetAsync(ib.counters + 3, 0, sizeof(unsigned long long), st));
 }
 
+namespace {
+
+// Device state of one NN-Descent run over n rows: the graph lists, the
+// samples of an iteration and the join's inboxes and candidate list.
+// list_only: the tensor-core join, which keeps no inboxes and appends a whole
+// iteration's candidates to the list.
+struct NndState {
+  Buf<int32_t> gid, newS, oldS, nrev, orev, inbox_cnt;
+  Buf<float> gdist, worst;
+  Buf<int8_t> nf, of;
+  Buf<uint64_t> inbox, ovf_key;
+  Buf<unsigned long long> ovf, dropped;
+  Buf<uint32_t> ovf_tgt, ostart, oend;
+  Inbox ib;
+
+  NndState(Context *ctx, int64_t n, int k, int S, bool list_only) {
+    cudaStream_t st = ctx->stream;
+    gid = Buf<int32_t>(ctx, n * k);
+    gdist = Buf<float>(ctx, n * k);
+    worst = Buf<float>(ctx, n);
+    newS = Buf<int32_t>(ctx, n * 2 * S);
+    oldS = Buf<int32_t>(ctx, n * 2 * S);
+    nrev = Buf<int32_t>(ctx, n);
+    orev = Buf<int32_t>(ctx, n);
+    inbox_cnt = Buf<int32_t>(ctx, n);
+    nf = Buf<int8_t>(ctx, n);
+    of = Buf<int8_t>(ctx, n);
+    inbox = Buf<uint64_t>(ctx, list_only ? 1 : (size_t)n * kInboxCap);
+    ovf = Buf<unsigned long long>(ctx, n);
+    dropped = Buf<unsigned long long>(ctx, 4);
+    // room for a pass's candidates; the tensor-core join's warps also leave
+    // the unused tail of their last list chunk (at most one chunk per
+    // epilogue warp)
+    const int64_t rows = list_only ? 64 : 16;
+    const int64_t cap = (n * rows > (1 << 22) ? n * rows : (1 << 22)) +
+                        (list_only ? (int64_t)8 * ctx->num_sms * kListChunk : 0);
+    ovf_tgt = Buf<uint32_t>(ctx, cap);
+    ovf_key = Buf<uint64_t>(ctx, cap);
+    ostart = Buf<uint32_t>(ctx, n);
+    oend = Buf<uint32_t>(ctx, n);
+    HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
+    HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
+    ib = Inbox{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, cap};
+    HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
+    HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
+    clear_inboxes(ctx, n);
+  }
+  // the inbox state a join starts an iteration from: empty inboxes, no
+  // candidates in the list, nothing dropped
+  void clear_inboxes(Context *ctx, int64_t n) {
+    cudaStream_t st = ctx->stream;
+    HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
+    HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
+    HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+  }
+};
+
+// One FP32 local join over s's samples with `tiles` 4 x 4 tiles per lane.
+void fp32_join(Context *ctx, int tiles, const float *X, int64_t n, int d, int S, const NndState &s,
+               int cross_only) {
+  const int jw = kJoinWarps;
+  const size_t smem = JoinSmem::kBytes * jw;
+  const int grid = grid_for(ctx, n, jw, 16);
+  cudaStream_t st = ctx->stream;
+  if (tiles == 1) {
+    HDB_CUDA(cudaFuncSetAttribute(k_join<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_join<1><<<grid, 32 * jw, smem, st>>>(X, n, d, S, s.newS, s.oldS, s.nf, s.of, s.nrev, s.orev,
+                                           s.worst, s.ib, cross_only);
+  } else {
+    HDB_CUDA(cudaFuncSetAttribute(k_join<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_join<2><<<grid, 32 * jw, smem, st>>>(X, n, d, S, s.newS, s.oldS, s.nf, s.of, s.nrev, s.orev,
+                                           s.worst, s.ib, cross_only);
+  }
+  ctx->launches++;
+}
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  EventPair() {
+    HDB_CUDA(cudaEventCreate(&a));
+    HDB_CUDA(cudaEventCreate(&b));
+  }
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+std::mutex g_tune_mutex;
+// (device, d, k, S, whether the rows fit in L2) -> tile slots
+std::map<std::array<int, 5>, int> g_join_tiles;
+
+}  // namespace
+
+// Tile slots per lane of the FP32 local join: the one forced on the context,
+// else the one tuned for this shape.  An untuned shape is timed on the first
+// m rows of Xw (the caller's rows in locality order; m = 64K..1M, enough to
+// leave L2 at d >= 64): the initial graph of those rows, one iteration
+// (sample, join, merge) so that the rows hold old and new entries as in the
+// later iterations, the second sample, then both forms -- k_join<1> (80
+// registers, three blocks per SM) and k_join<2> (122 registers, two blocks
+// per SM) -- three times each, alternating, from the same sample and inbox
+// state, the first round untimed.  The faster form is kept for the process.
+// Without Xw (the merge) an untuned shape takes two.  The trial's launches
+// count in ctx->launches.
+int fp32_join_tiles(Context *ctx, int d, int k, int S, bool resident, const float *Xw, int64_t n) {
+  if (ctx->join_tiles) return ctx->join_tiles;
+  const std::array<int, 5> key{ctx->device, d, k, S, resident ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    auto it = g_join_tiles.find(key);
+    if (it != g_join_tiles.end()) return it->second;
+  }
+  if (!Xw) return 2;
+  cudaStream_t st = ctx->stream;
+  const int64_t want = (int64_t(256) << 20) / (4 * (int64_t)d);
+  const int64_t m = std::min<int64_t>(
+      n, std::max<int64_t>(65536, std::min<int64_t>(int64_t(1) << 20, want)));
+  NndState t(ctx, m, k, S, false);
+  Buf<int32_t> nrev0(ctx, m), orev0(ctx, m);
+  const int wpb = 8;
+  const int grid_rows = grid_for(ctx, m, wpb, 16);
+  const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(Xw, m, d, k, Segments{}, nullptr, nullptr, t.gid,
+                                                  t.gdist, t.worst);
+  ctx->launches++;
+  HDB_CHECK_LAUNCH();
+  for (int it = 0; it < 2; it++) {
+    if (it == 1) {
+      fp32_join(ctx, 2, Xw, m, d, S, t, 0);
+      HDB_CHECK_LAUNCH();
+      sort_overflow(ctx, t.ib, m);
+    }
+    k_sample<<<grid_rows, 32 * wpb, 0, st>>>(m, k, S, it, t.gid, t.gdist, t.worst, t.ib, t.newS,
+                                             t.oldS, t.nf, t.of, t.nrev, t.orev, 0);
+    ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
+  // the join clears the reverse-sample counts it reads: each trial starts
+  // from a copy
+  HDB_CUDA(cudaMemcpyAsync(nrev0, t.nrev, m * 4, cudaMemcpyDeviceToDevice, st));
+  HDB_CUDA(cudaMemcpyAsync(orev0, t.orev, m * 4, cudaMemcpyDeviceToDevice, st));
+  EventPair ev;
+  double ms[3] = {0.0, 0.0, 0.0};
+  for (int rep = 0; rep < 3; rep++) {
+    for (int tiles = 1; tiles <= 2; tiles++) {
+      HDB_CUDA(cudaMemcpyAsync(t.nrev, nrev0, m * 4, cudaMemcpyDeviceToDevice, st));
+      HDB_CUDA(cudaMemcpyAsync(t.orev, orev0, m * 4, cudaMemcpyDeviceToDevice, st));
+      t.clear_inboxes(ctx, m);
+      HDB_CUDA(cudaEventRecord(ev.a, st));
+      fp32_join(ctx, tiles, Xw, m, d, S, t, 0);
+      HDB_CUDA(cudaEventRecord(ev.b, st));
+      HDB_CHECK_LAUNCH();
+      HDB_CUDA(cudaEventSynchronize(ev.b));
+      float e = 0.0f;
+      HDB_CUDA(cudaEventElapsedTime(&e, ev.a, ev.b));
+      if (rep > 0) ms[tiles] += e;
+    }
+  }
+  const int pick = ms[1] < ms[2] ? 1 : 2;
+  std::lock_guard<std::mutex> g(g_tune_mutex);
+  g_join_tiles[key] = pick;
+  return pick;
+}
+
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js, const Segments &seg) {
   const int k = p.k, S = p.sample_num;
@@ -1333,11 +1505,6 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
                   p.precision == HDB_PREC_FP16,
               HDB_ERR_ARG, "NN-Descent: unknown precision");
   cudaStream_t st = ctx->stream;
-  Buf<int32_t> gid(ctx, n * k);
-  Buf<float> gdist(ctx, n * k), worst(ctx, n);
-  Buf<int32_t> newS(ctx, n * 2 * S), oldS(ctx, n * 2 * S), nrev(ctx, n), orev(ctx, n),
-      inbox_cnt(ctx, n);
-  Buf<int8_t> nf(ctx, n), of(ctx, n);
   // The tensor-core join appends every candidate to the list that
   // sort_overflow groups by target for the merge (a returning inbox atomic per
   // candidate cost it more than the sort), so it needs no inboxes and a list
@@ -1346,23 +1513,12 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   // atomics (10M x 12: 737 vs 810 ms a step).
   const bool tc_form = (p.precision == HDB_PREC_BF16 || p.precision == HDB_PREC_FP16) &&
                        tc_dpad(d) <= kTcMaxDpad;
-  Buf<uint64_t> inbox(ctx, tc_form ? 1 : (size_t)n * kInboxCap);
-  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
-  // room for a pass's candidates; the tensor-core join's warps also leave the
-  // unused tail of their last list chunk (at most one chunk per epilogue warp)
-  const int64_t ovf_rows = tc_form ? 64 : 16;
-  const int64_t ovf_cap = (n * ovf_rows > (1 << 22) ? n * ovf_rows : (1 << 22)) +
-                          (tc_form ? (int64_t)8 * ctx->num_sms * kListChunk : 0);
-  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
-  Buf<uint64_t> ovf_key(ctx, ovf_cap);
-  HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
-  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, ovf_cap};
-  HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
-  HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+  NndState s(ctx, n, k, S, tc_form);
+  int32_t *gid = s.gid, *newS = s.newS, *oldS = s.oldS, *nrev = s.nrev, *orev = s.orev;
+  float *gdist = s.gdist, *worst = s.worst;
+  int8_t *nf = s.nf, *of = s.of;
+  const Inbox &ib = s.ib;
+  unsigned long long *dropped = s.dropped;
   std::vector<cudaEvent_t> jev;
   if (js) {
     jev.resize(2 * (size_t)p.iterations);
@@ -1399,10 +1555,6 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   }
   const float *Xw = Xp;
   Buf<hdb_nnd_element> Gp(ctx, (size_t)n * k);
-  const int jw = kJoinWarps;
-  const size_t smem_join = JoinSmem::kBytes * jw;
-  HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
-  const int grid_join = grid_for(ctx, n, jw, 16);
   // 16-bit forms: BF16, or FP16 of the rows scaled by one power of two; the
   // tensor-core tile pipeline (tcgen05) up to 256 padded dimensions, the
   // mma.sync join beyond
@@ -1459,6 +1611,10 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
       grid_bf = grid_for(ctx, n, jw16, 64);
     }
   }
+  // FP32 form: the join's tile slots per lane, tuned per shape
+  const int tiles =
+      bf16 ? 0 : fp32_join_tiles(ctx, d, k, S, n * d * 4 <= ctx->l2_bytes, Xw, n);
+  if (js) js->config = tiles;
   for (int it = 0; it < p.iterations; it++) {
     k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib,
                                                        newS, oldS, nf, of, nrev, orev, 0); ctx->launches++;
@@ -1474,9 +1630,8 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
         k_join_bf16<false><<<grid_bf, 32 * jw16, smem_bf, st>>>(Xb, nrm, n, dpad, S, dscale, newS,
                                                                 oldS, nf, of, nrev, orev, worst, ib);
       else
-        k_join<<<grid_join, 32 * jw, smem_join, st>>>(Xw, n, d, S, newS, oldS, nf, of, nrev, orev,
-                                                      worst, ib, 0);
-      ctx->launches++;
+        fp32_join(ctx, tiles, Xw, n, d, S, s, 0);
+      if (bf16) ctx->launches++;
     }
     if (js) HDB_CUDA(cudaEventRecord(jev[2 * it + 1], st));
     HDB_CHECK_LAUNCH();
@@ -1534,24 +1689,11 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
   HDB_CUDA(cudaMemcpyAsync(X.get(), X1, (size_t)n1 * d * sizeof(float), cudaMemcpyDeviceToDevice, st));
   HDB_CUDA(cudaMemcpyAsync(X.get() + (size_t)n1 * d, X2, (size_t)n2 * d * sizeof(float),
                            cudaMemcpyDeviceToDevice, st));
-  Buf<int32_t> gid(ctx, n * k);
-  Buf<float> gdist(ctx, n * k), worst(ctx, n);
-  Buf<int32_t> newS(ctx, n * 2 * S), oldS(ctx, n * 2 * S), nrev(ctx, n), orev(ctx, n),
-      inbox_cnt(ctx, n);
-  Buf<int8_t> nf(ctx, n), of(ctx, n);
-  Buf<uint64_t> inbox(ctx, (size_t)n * kInboxCap);
-  Buf<unsigned long long> ovf(ctx, n), dropped(ctx, 4);
-  const int64_t ovf_cap = n * 16 > (1 << 22) ? n * 16 : (1 << 22);
-  Buf<uint32_t> ovf_tgt(ctx, ovf_cap), ostart(ctx, n), oend(ctx, n);
-  Buf<uint64_t> ovf_key(ctx, ovf_cap);
-  HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
-  Inbox ib{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, ovf_cap};
-  HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
-  HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
-  HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+  NndState s(ctx, n, k, S, false);
+  int32_t *gid = s.gid;
+  float *gdist = s.gdist, *worst = s.worst;
+  const Inbox &ib = s.ib;
+  unsigned long long *dropped = s.dropped;
 
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
@@ -1566,20 +1708,17 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
   HDB_REQUIRE(!(e & DEVERR_SELF_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row lists itself");
   HDB_REQUIRE(!(e & DEVERR_DUP_ID), HDB_ERR_ARG, "KNNMerge: a subgraph row repeats an id");
 
-  const int jw = kJoinWarps;
-  const size_t smem_join = JoinSmem::kBytes * jw;
-  HDB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_join));
-  const int grid_join = grid_for(ctx, n, jw, 16);
+  // the merge takes the forced tile slots, else the ones tuned for this
+  // shape by an earlier nndescent call, else two
+  const int tiles = fp32_join_tiles(ctx, d, k, S, n * d * 4 <= ctx->l2_bytes, nullptr, 0);
   // NNDescentForMerge (nndescent.cu:1999-2087): PrepareForUpdateForMerge +
   // UpdateGraphForMerge per iteration
   for (int it = 0; it < p.iterations; it++) {
-    k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib, newS, oldS,
-                                             nf, of, nrev, orev, n1);
+    k_sample<<<grid_rows, 32 * wpb, 0, st>>>(n, k, S, it > 0, gid, gdist, worst, ib, s.newS,
+                                             s.oldS, s.nf, s.of, s.nrev, s.orev, n1);
     ctx->launches++;
     HDB_CHECK_LAUNCH();
-    k_join<<<grid_join, 32 * jw, smem_join, st>>>(X, n, d, S, newS, oldS, nf, of, nrev, orev,
-                                                  worst, ib, 1);
-    ctx->launches++;
+    fp32_join(ctx, tiles, X, n, d, S, s, 1);
     HDB_CHECK_LAUNCH();
     sort_overflow(ctx, ib, n);
     HDB_CHECK_LAUNCH();

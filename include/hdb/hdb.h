@@ -111,7 +111,8 @@ typedef struct {
   int64_t join_candidates;      /* candidates that passed the k-th distance filter */
   int64_t gpu_launches;         /* kernel launches issued by the call */
   int32_t mst_multiplier;       /* mst_gpu = 1: the weight scale exponent m (single runs) */
-  int32_t reserved;
+  int32_t join_config;          /* FP32 local join: 4 x 4 distance tiles per lane (1 or 2),
+                                   forced (hdb_set_join_tiles) or tuned; 0 for a 16-bit join */
 } hdb_run_stats;
 
 typedef struct hdb_ctx hdb_ctx;
@@ -124,6 +125,14 @@ HDB_API hdb_status hdb_destroy(hdb_ctx *ctx);
 /* Run the context's work on a caller stream (cudaStream_t); NULL restores the
  * context's own stream. */
 HDB_API hdb_status hdb_set_stream(hdb_ctx *ctx, void *stream);
+/* FP32 local join form (no reference counterpart: the reference's join,
+ * nndescent.cu:1487-1580, has one form).  tiles = 1 or 2 distance tiles of
+ * 4 x 4 per lane forces that form (1: fewer registers, three blocks per SM;
+ * 2: two blocks per SM, fewer passes over the staged rows); 0 (the default)
+ * times both once per (device, d, k, SAMPLE_NUM, rows fit in L2) on the
+ * first FP32 NN-Descent of that shape and keeps the faster for the process.
+ * Both forms give the same graph. */
+HDB_API hdb_status hdb_set_join_tiles(hdb_ctx *ctx, int32_t tiles);
 
 /* gpuknn::NNDescent, gpuknn/nndescent.cuh:40-42 (nndescent.cu:2088-2199):
  * X [n, d] float32 row-major -> G [n, k] NNDElement rows sorted by ascending

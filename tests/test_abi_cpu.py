@@ -36,6 +36,8 @@ def test_null_context_is_an_argument_error(libpath):
     L = _lib.load(libpath)
     assert L.hdb_set_stream(None, None) == _lib.HDB_ERR_ARG
     assert b"NULL" in L.hdb_last_error()
+    assert L.hdb_set_join_tiles(None, 1) == _lib.HDB_ERR_ARG
+    assert b"NULL" in L.hdb_last_error()
     assert L.hdb_destroy(None) == _lib.HDB_OK
 
 
