@@ -1,5 +1,6 @@
 // extern "C" entry points of libhdb_b200 (include/hdb/hdb.h) and the
 // end-to-end pipeline in the reference's HDBSCAN/_new.cu order.
+#include <algorithm>
 #include <map>
 #include <vector>
 
@@ -693,14 +694,31 @@ hdb_status run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count, const hdb
     hdb_run_stats rs = {};
     JoinStats js;
     HDB_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
-    // consecutive instances of one d, up to kBatchPoints points per batch
-    // (bounds the per-point working memory of NN-Descent, ~1.5 KB a point)
-    constexpr int64_t kBatchPoints = int64_t(1) << 25;
+    // consecutive instances of one d, as many points per batch as the free
+    // device memory holds (at most 2^25): 70 % of what the driver has free
+    // plus the context's idle cached blocks, over the batch's bytes per point
+    // at its peak (NN-Descent, or the graph / MST stages when the kNN graphs
+    // are given), plus the batch's own arrays
+    size_t free_b = 0, total_b = 0;
+    HDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double avail = 0.7 * ((double)free_b + (double)ctx->cache_bytes);
     for (auto &g : groups) {
+      const int64_t d = g.first;
+      const int64_t graph_bpp = 40 * (int64_t)k;  // CSR + MST keys, E ~ 1.5 k per point
+      const int64_t nnd_bpp = from_knn ? 0 : nndescent_bytes_per_point(g.first, p.knn);
+      const int64_t bpp = std::max(nnd_bpp, graph_bpp) + 12 * (int64_t)k + 16 + 4 * d;
+      const int64_t cap = std::max<int64_t>(
+          int64_t(1) << 16, std::min<int64_t>(int64_t(1) << 25, (int64_t)(avail / (double)bpp)));
+      // batches of about equal size, so that they reuse the same cached blocks
+      // (unequal ones would free and allocate multi-GB blocks every call)
+      int64_t group_points = 0;
+      for (int32_t i : g.second) group_points += insts[i].n;
+      const int64_t nb = (group_points + cap - 1) / cap;
+      const int64_t batch_points = (group_points + nb - 1) / nb;
       std::vector<int32_t> part;
       int64_t pts = 0;
       for (int32_t i : g.second) {
-        if (!part.empty() && pts + insts[i].n > kBatchPoints) {
+        if (!part.empty() && pts + insts[i].n > batch_points) {
           run_batch_group(ctx, insts, part, g.first, p, &rs, &js, from_knn);
           part.clear();
           pts = 0;

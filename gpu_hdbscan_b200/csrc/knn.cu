@@ -72,47 +72,69 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
 // the reference's sequential FP32 difference sum (nndescent.cu:1086-1093),
 // sum = fmaf(a_j - b_j, a_j - b_j, sum) for j = 0..d-1.
 constexpr int kStageCols = 32;
-constexpr int kStageLd = kStageCols + 1;                  // conflict-free column walk
-constexpr int kStageFloats = kStageCols + 32 * kStageLd;  // own segment + 32 rows
+constexpr int kStageLd = kStageCols + 1;                    // conflict-free column walk
+constexpr int kRingSlot = kStageCols + 32 * kStageCols;     // 16-byte form: own + 32 rows
+constexpr int kStageFloats = 2 * kRingSlot;                 // >= kStageCols + 32 * kStageLd
 
-// 16-byte form for d % 4 == 0 (rows 16-byte aligned): per chunk, lane i loads
-// piece q = i & 7 of rows i >> 3, + 4, ... (eight 16-byte loads in flight per
-// lane) into rows of 32 floats whose pieces are permuted by the row
-// (piece q of row r at q ^ (r & 7)), so the lanes' walks of their own rows
-// read distinct bank groups.  Same sums as below, element by element.
+// 16-byte form for d % 4 == 0 (rows 16-byte aligned): a two-slot ring of
+// chunks filled by cp.async, so the next chunk of the 33 rows is in flight
+// while this one is summed.  Per chunk, lane i copies piece q = i & 7 of rows
+// i >> 3, + 4, ... (eight 16-byte copies per lane) into rows of 32 floats
+// whose pieces are permuted by the row (piece q of row r at q ^ (r & 7)), so
+// the lanes' walks of their own rows read distinct bank groups.  Same sums as
+// below, element by element.
 __device__ __forceinline__ float diffsum_staged_v4(const float *__restrict__ X, int d, int64_t row,
                                                    int32_t id, bool active, float *__restrict__ sm) {
   const int lane = lane_id();
-  float *own = sm;
-  float *nb = sm + kStageCols;
   const uint32_t act = __ballot_sync(0xffffffffu, active);
   const int q = lane & 7, rb = lane >> 3;
   int32_t rid[8];
 #pragma unroll
   for (int t = 0; t < 8; t++) rid[t] = __shfl_sync(0xffffffffu, id, rb + 4 * t);
-  float s = 0.0f;
-  for (int c0 = 0; c0 < d; c0 += kStageCols) {
-    const int nq = min(kStageCols, d - c0) >> 2;  // 16-byte pieces in this chunk
-    __syncwarp();
-    if (lane < 4 * nq) own[lane] = X[row * d + c0 + lane];
+  const int nchunks = (d + kStageCols - 1) / kStageCols;
+  // chunk c into ring slot c & 1: the own row's segment and the rows' pieces
+  auto issue = [&](int c) {
+    const int c0 = c * kStageCols;
+    const int nq = min(kStageCols, d - c0) >> 2;
+    float *own = sm + (c & 1) * kRingSlot;
+    float *nb = own + kStageCols;
+    if (lane < nq) {
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(own + 4 * lane);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                   "l"(X + row * d + c0 + 4 * lane)
+                   : "memory");
+    }
     if (q < nq) {
-      float4 t4[8];
 #pragma unroll
       for (int t = 0; t < 8; t++) {
         const int r = rb + 4 * t;
-        t4[t] = ((act >> r) & 1u)
-                    ? __ldg(reinterpret_cast<const float4 *>(X + (int64_t)rid[t] * d + c0) + q)
-                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      }
-#pragma unroll
-      for (int t = 0; t < 8; t++) {
-        const int r = rb + 4 * t;
-        *reinterpret_cast<float4 *>(nb + r * kStageCols + 4 * (q ^ (r & 7))) = t4[t];
+        if ((act >> r) & 1u) {
+          const uint32_t dst =
+              (uint32_t)__cvta_generic_to_shared(nb + r * kStageCols + 4 * (q ^ (r & 7)));
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                       "l"(X + (int64_t)rid[t] * d + c0 + 4 * q)
+                       : "memory");
+        }
       }
     }
-    __syncwarp();
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  __syncwarp();  // the ring's previous contents are no longer read
+  issue(0);
+  float s = 0.0f;
+  for (int c = 0; c < nchunks; c++) {
+    if (c + 1 < nchunks) {
+      __syncwarp();  // slot (c + 1) & 1 held chunk c - 1, summed by every lane
+      issue(c + 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncwarp();  // every lane's copies of chunk c have landed
     if (active) {
-      const float *mine = nb + lane * kStageCols;
+      const int nq = min(kStageCols, d - c * kStageCols) >> 2;
+      const float *own = sm + (c & 1) * kRingSlot;
+      const float *mine = own + kStageCols + lane * kStageCols;
       for (int p = 0; p < nq; p++) {
         const float4 b = *reinterpret_cast<const float4 *>(mine + 4 * (p ^ (lane & 7)));
         const float4 a = *reinterpret_cast<const float4 *>(own + 4 * p);
@@ -127,6 +149,7 @@ __device__ __forceinline__ float diffsum_staged_v4(const float *__restrict__ X, 
       }
     }
   }
+  __syncwarp();
   return s;
 }
 
@@ -183,7 +206,7 @@ __device__ __forceinline__ float diffsum_staged(const float *__restrict__ X, int
 // the ids are drawn for the caller's row from the caller's numbering and then
 // mapped, so the lists are exactly the caller-numbered initial graph
 // renumbered (instances keep their ranges under the renumbering).
-__global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Segments seg,
+__global__ void __launch_bounds__(256, 3) k_init(const float *__restrict__ X, int64_t n, int d, int k, Segments seg,
                        const uint32_t *__restrict__ order, const int32_t *__restrict__ inv,
                        int32_t *__restrict__ gid, float *__restrict__ gdist,
                        float *__restrict__ worst) {
@@ -240,7 +263,7 @@ __global__ void k_init(const float *__restrict__ X, int64_t n, int d, int k, Seg
 // the other set are the new ones.  Own-subgraph ids outside their set, self
 // ids and repeats set DEVERR_ID_RANGE / SELF / DUP and are replaced by a
 // valid id of the set so that no gather leaves X.
-__global__ void k_merge_init(const float *__restrict__ X, int64_t n, int d, int k, int64_t n1,
+__global__ void __launch_bounds__(256, 3) k_merge_init(const float *__restrict__ X, int64_t n, int d, int k, int64_t n1,
                              const hdb_nnd_element *__restrict__ G1,
                              const hdb_nnd_element *__restrict__ G2, int32_t *__restrict__ gid,
                              float *__restrict__ gdist, float *__restrict__ worst,
@@ -1084,7 +1107,7 @@ __global__ void __launch_bounds__(128) k_join_bf16(const uint16_t *__restrict__ 
 // FP32 re-rank of every kept neighbour (one warp per row): the reference's
 // difference sum for each (row, neighbour) pair, rows re-sorted by (distance,
 // id); old/new flags travel with their ids.
-__global__ void k_rerank(const float *__restrict__ X, int64_t n, int d, int k,
+__global__ void __launch_bounds__(256, 3) k_rerank(const float *__restrict__ X, int64_t n, int d, int k,
                          hdb_nnd_element *__restrict__ G) {
   extern __shared__ float smem_stage[];
   const int lane = lane_id();
@@ -1329,6 +1352,14 @@ static void sort_overflow(Context *ctx, const Inbox &ib, int64_t n) {
 
 namespace {
 
+// Dynamic shared memory of the kernels that stage rows for difference sums
+// (two ring slots of 33 rows x 32 dimensions per warp: 66 KB for 8 warps).
+void stage_smem_attrs(size_t bytes) {
+  HDB_CUDA(cudaFuncSetAttribute(k_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  HDB_CUDA(cudaFuncSetAttribute(k_merge_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  HDB_CUDA(cudaFuncSetAttribute(k_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 // Device state of one NN-Descent run over n rows: the graph lists, the
 // samples of an iteration and the join's inboxes and candidate list.
 // list_only: the tensor-core join, which keeps no inboxes and appends a whole
@@ -1450,6 +1481,7 @@ int fp32_join_tiles(Context *ctx, int d, int k, int S, bool resident, const floa
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, m, wpb, 16);
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  stage_smem_attrs(smem_stage);
   k_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(Xw, m, d, k, Segments{}, nullptr, nullptr, t.gid,
                                                   t.gdist, t.worst);
   ctx->launches++;
@@ -1492,6 +1524,20 @@ int fp32_join_tiles(Context *ctx, int d, int k, int S, bool resident, const floa
   return pick;
 }
 
+int64_t nndescent_bytes_per_point(int32_t d, const hdb_knn_params &p) {
+  const int64_t k = p.k, S = p.sample_num;
+  const bool half = p.precision == HDB_PREC_BF16 || p.precision == HDB_PREC_FP16;
+  const bool tc = half && tc_dpad(d) <= kTcMaxDpad;
+  const int64_t dpad = tc ? tc_dpad(d) : (d + 15) & ~15;
+  int64_t b = 4 * (int64_t)d;                    // X in locality order
+  if (half) b += 2 * dpad + 4;                   // 16-bit rows + norms
+  b += 8 * k + 4 + 16 * S + 30;                  // lists, worst, samples, counters
+  if (!tc) b += 8 * kInboxCap;                   // per-row inboxes
+  b += 2 * 12 * (tc ? 64 : 16);                  // candidate list + sort buffers
+  b += 8 * k;                                    // graph in locality order
+  return b;
+}
+
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js, const Segments &seg) {
   const int k = p.k, S = p.sample_num;
@@ -1528,6 +1574,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  stage_smem_attrs(smem_stage);
   // renumber the points in locality order (k_loc_project); X stays the
   // caller's, the iterations work on Xw and the renumbered lists, and the
   // initial graph is drawn straight into the new numbering
@@ -1698,6 +1745,7 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, n, wpb, 16);
   const size_t smem_stage = (size_t)wpb * kStageFloats * sizeof(float);
+  stage_smem_attrs(smem_stage);
   k_merge_init<<<grid_rows, 32 * wpb, smem_stage, st>>>(X, n, d, k, n1, G1, G2, gid, gdist, worst,
                                                         ctx->dev_err);
   ctx->launches++;

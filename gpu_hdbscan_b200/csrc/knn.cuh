@@ -17,6 +17,10 @@ struct JoinStats {
 void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn_params &p,
                hdb_nnd_element *G, int64_t *dropped_out, JoinStats *js = nullptr,
                const Segments &seg = Segments{});
+// Device bytes per point that nndescent holds at its peak: X in locality
+// order, the 16-bit rows, lists, samples, inboxes, the candidate list and its
+// sort buffers, the graph before it is mapped back.
+int64_t nndescent_bytes_per_point(int32_t d, const hdb_knn_params &p);
 // Merge of the kNN graphs of two point sets into the graph of their union
 // (hdb_knn_merge): FP32 join, old samples from the row's own set only.
 void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element *G1,
