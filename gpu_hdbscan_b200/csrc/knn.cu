@@ -335,6 +335,7 @@ __global__ void __launch_bounds__(256, 3) k_merge_init(const float *__restrict__
 // entries above it moving up one lane and the last one dropping out.  The
 // result is the first k distinct ids of the union in key order, whatever the
 // order of the candidates.  Inserted entries carry the "new" flag.
+template <bool kCheckIds = true>
 __device__ __forceinline__ void insert_chunk(int k, uint64_t &rkey, int32_t &lab, uint64_t cand) {
   const int lane = lane_id();
   const bool have = lane < k;
@@ -347,7 +348,7 @@ __device__ __forceinline__ void insert_chunk(int k, uint64_t &rkey, int32_t &lab
     const int pos = __popc(__ballot_sync(0xffffffffu, have && rkey < c));
     if (pos >= k) continue;
     const int32_t cid = pk_id(c);
-    if (__any_sync(0xffffffffu, have && pk_id(rkey) == cid)) continue;
+    if (kCheckIds && __any_sync(0xffffffffu, have && pk_id(rkey) == cid)) continue;
     const uint64_t up = __shfl_up_sync(0xffffffffu, rkey, 1);
     const int32_t uplab = __shfl_up_sync(0xffffffffu, lab, 1);
     if (lane == pos) {
@@ -375,94 +376,123 @@ __device__ __forceinline__ int rank_in_lanes(uint64_t sorted, int m, uint64_t x)
   return lo;
 }
 
-// The same merge as insert_chunk for a chunk with many candidates: ids
-// already listed and repeats within the chunk are dropped first (one value
-// per pair, so repeats carry equal keys), the survivors are sorted across
-// the lanes, each side of the merge finds its rank in the other by binary
-// search, and the first k entries are placed through per-warp shared memory
-// (sk: 32 keys, sl: 32 labels).  Chunks with few candidates take the
-// one-at-a-time insertion, which is cheaper there.
-__device__ __forceinline__ void merge_chunk(int k, uint64_t &rkey, int32_t &lab, uint64_t cand,
-                                            uint64_t *sk, int32_t *sl) {
+// Per-warp shared memory of the merge: an open-addressing table of the ids
+// seen (128 slots, -1 empty), the compacted survivors of a batch, and the
+// merged row.
+constexpr int kMergeTable = 128;
+struct MergeSmem {
+  int32_t tbl[kMergeTable];
+  uint64_t stage[64];
+  uint64_t sk[32];
+  int32_t sl[32];
+};
+
+// Inserts id into the table; true if it was not there yet.  A batch puts at
+// most 32 + 64 ids into the 128 slots, so a free slot is always found.
+__device__ __forceinline__ bool table_insert(int32_t *tbl, int32_t id) {
+  uint32_t h = ((uint32_t)id * 0x9E3779B1u) >> 25;
+  for (int probe = 0; probe < kMergeTable; probe++) {
+    const int32_t prev = atomicCAS(&tbl[h], -1, id);
+    if (prev == -1) return true;
+    if (prev == id) return false;
+    h = (h + 1) & (kMergeTable - 1);
+  }
+  return false;
+}
+
+// Offers up to 64 candidates (c0, c1 per lane; ~0 for none) to the row held
+// one sorted entry per lane (lane < k; key = (distance, id)), with the same
+// result as insert_chunk on each of them.  Candidates at or above the row's
+// k-th key cannot enter (the k-th key never grows).  The others go through a
+// per-warp hash table holding the row's ids first, so a candidate whose id
+// is listed or was already offered in the batch drops out (a pair's repeats
+// carry equal keys, so which one stays does not matter); the survivors are
+// compacted and either inserted one at a time (few) or sorted across the
+// lanes and merged by rank -- each side finds its rank in the other by binary
+// search -- with the first k entries placed through shared memory.
+__device__ __forceinline__ void merge_batch(int k, uint64_t &rkey, int32_t &lab, uint64_t c0,
+                                            uint64_t c1, MergeSmem &ms) {
   const int lane = lane_id();
   const bool have = lane < k;
   const uint64_t kth = __shfl_sync(0xffffffffu, rkey, k - 1);
-  bool ok = cand < kth;
-  if (__ballot_sync(0xffffffffu, ok) == 0) return;
-  const int32_t cid = pk_id(cand);
-  const int32_t rid = pk_id(rkey);
-  const uint32_t okm = __ballot_sync(0xffffffffu, ok);
-  if (__popc(okm) <= 8) {
-    // few candidates below the k-th key (the common case once rows settle):
-    // one vote of the row per candidate
-    for (uint32_t m = okm; m; m &= m - 1) {
-      const int t = __ffs(m) - 1;
-      const int32_t c = __shfl_sync(0xffffffffu, cid, t);
-      if (__any_sync(0xffffffffu, have && rid == c) && lane == t) ok = false;
-    }
-  } else {
-    for (int t = 0; t < k; t++) {
-      const int32_t r = __shfl_sync(0xffffffffu, rid, t);  // every lane takes part
-      ok = ok && cid != r;
-    }
-  }
-  const uint32_t same = __match_any_sync(0xffffffffu, ok ? cid : -1 - lane);
-  ok = ok && (__ffs(same) - 1 == lane);
-  const int nc = __popc(__ballot_sync(0xffffffffu, ok));
-  if (nc == 0) return;
-  if (nc <= 12) {
-    insert_chunk(k, rkey, lab, ok ? cand : ~0ull);
-    return;
-  }
-  const uint64_t c = warp_sort32(ok ? cand : ~0ull);  // survivors in lanes 0..nc-1
-  const int pos_r = lane + rank_in_lanes(c, nc, rkey);  // row entry: its merged rank
-  const int pos_c = lane + rank_in_lanes(rkey, k, c);   // candidate: its merged rank
+  bool ok0 = c0 < kth, ok1 = c1 < kth;
+  if (!__any_sync(0xffffffffu, ok0 || ok1)) return;
+#pragma unroll
+  for (int j = 0; j < kMergeTable / 32; j++) ms.tbl[lane + 32 * j] = -1;
   __syncwarp();
-  if (have && pos_r < k) {
-    sk[pos_r] = rkey;
-    sl[pos_r] = lab;
-  }
-  if (lane < nc && pos_c < k) {
-    sk[pos_c] = c;
-    sl[pos_c] = pk_id(c);  // inserted as "new"
-  }
+  if (have) table_insert(ms.tbl, pk_id(rkey));
   __syncwarp();
-  if (have) {
-    rkey = sk[lane];
-    lab = sl[lane];
+  if (ok0) ok0 = table_insert(ms.tbl, pk_id(c0));
+  if (ok1) ok1 = table_insert(ms.tbl, pk_id(c1));
+  const uint32_t b0 = __ballot_sync(0xffffffffu, ok0), b1 = __ballot_sync(0xffffffffu, ok1);
+  const int nsurv = __popc(b0) + __popc(b1);
+  if (nsurv == 0) return;
+  const uint32_t lt = lanemask_lt();
+  if (ok0) ms.stage[__popc(b0 & lt)] = c0;
+  if (ok1) ms.stage[__popc(b0) + __popc(b1 & lt)] = c1;
+  __syncwarp();
+  for (int base = 0; base < nsurv; base += 32) {
+    const int nc = min(32, nsurv - base);
+    const uint64_t cand = lane < nc ? ms.stage[base + lane] : ~0ull;
+    if (nc <= 12) {
+      insert_chunk<false>(k, rkey, lab, cand);
+      continue;
+    }
+    const uint64_t c = warp_sort32(cand);                // survivors in lanes 0..nc-1
+    const int pos_r = lane + rank_in_lanes(c, nc, rkey);  // row entry: its merged rank
+    const int pos_c = lane + rank_in_lanes(rkey, k, c);   // candidate: its merged rank
+    __syncwarp();
+    if (have && pos_r < k) {
+      ms.sk[pos_r] = rkey;
+      ms.sl[pos_r] = lab;
+    }
+    if (lane < nc && pos_c < k) {
+      ms.sk[pos_c] = c;
+      ms.sl[pos_c] = pk_id(c);  // inserted as "new"
+    }
+    __syncwarp();
+    if (have) {
+      rkey = ms.sk[lane];
+      lab = ms.sl[lane];
+    }
   }
 }
 
-// Merge of everything offered to a row (inbox, overflow segment, best
-// dropped) into its sorted list (one warp).  On return, lane j (< k) holds the
-// j-th entry of the merged row.
+// Merge of everything offered to a row (inbox, best dropped, the row's
+// segment of the sorted candidate list) into its sorted list (one warp), in
+// batches of 64.  On return, lane j (< k) holds the j-th entry of the merged
+// row.  The tensor-core form keeps no inboxes (ib.inboxes = 0).
 __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, float &dist,
-                                          const Inbox &ib, uint64_t *sk, int32_t *sl) {
+                                          const Inbox &ib, MergeSmem &ms) {
   const int lane = lane_id();
-  int cnt = ib.cnt[row];
-  const uint64_t ov = ib.best[row];
+  int cnt = ib.inboxes ? ib.cnt[row] : 0;
+  const uint64_t ov = ib.inboxes ? ib.best[row] : ~0ull;
   const uint32_t o0 = ib.ostart[row], o1 = ib.oend[row];
   if (cnt == 0 && ov == ~0ull && o0 == o1) return;
-  if (cnt > kInboxCap) cnt = kInboxCap;
   __syncwarp();
   if (lane == 0) {
-    ib.cnt[row] = 0;
+    if (cnt != 0) ib.cnt[row] = 0;
     if (ov != ~0ull) ib.best[row] = ~0ull;
     if (o0 != o1) { ib.ostart[row] = 0; ib.oend[row] = 0; }
   }
+  if (cnt > kInboxCap) cnt = kInboxCap;
   const bool have = lane < k;
   uint64_t rkey = have ? pack(dist, decode(lab)) : ~0ull;
-  // the inbox (<= 127 slots) in four coalesced loads, all in flight at once
+  // candidate i of the row: inbox slots, then the best dropped, then the
+  // segment of the sorted list
   const uint64_t *inbox = ib.slots + row * kInboxCap;
-  uint64_t c[4];
-#pragma unroll
-  for (int q = 0; q < 4; q++) c[q] = 32 * q + lane < cnt ? inbox[32 * q + lane] : ~0ull;
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-    if (32 * q < cnt) merge_chunk(k, rkey, lab, c[q], sk, sl);
-  if (ov != ~0ull) insert_chunk(k, rkey, lab, lane == 0 ? ov : ~0ull);
-  for (uint32_t base = o0; base < o1; base += 32)
-    merge_chunk(k, rkey, lab, base + lane < o1 ? ib.ovf_key[base + lane] : ~0ull, sk, sl);
+  const int64_t nov = ov != ~0ull ? 1 : 0;
+  const int64_t m = (int64_t)cnt + nov + (int64_t)(o1 - o0);
+  auto at = [&](int64_t i) -> uint64_t {
+    if (i < cnt) return inbox[i];
+    if (i < cnt + nov) return ov;
+    return ib.ovf_key[o0 + (i - cnt - nov)];
+  };
+  for (int64_t base = 0; base < m; base += 64) {
+    const uint64_t c0 = base + lane < m ? at(base + lane) : ~0ull;
+    const uint64_t c1 = base + 32 + lane < m ? at(base + 32 + lane) : ~0ull;
+    merge_batch(k, rkey, lab, c0, c1, ms);
+  }
   if (have) dist = pk_dist(rkey);
 }
 
@@ -478,16 +508,14 @@ __global__ void k_sample(int64_t n, int k, int S, int do_merge, int32_t *__restr
                          int32_t *__restrict__ nrev, int32_t *__restrict__ orev, int64_t split) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
-  __shared__ uint64_t merge_keys[8][32];  // per-warp merge scratch (8 warps per block)
-  __shared__ int32_t merge_labs[8][32];
-  uint64_t *sk = merge_keys[threadIdx.x >> 5];
-  int32_t *sl = merge_labs[threadIdx.x >> 5];
+  __shared__ MergeSmem merge_smem[8];  // per-warp merge scratch (8 warps per block)
+  MergeSmem &ms = merge_smem[threadIdx.x >> 5];
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    if (do_merge) merge_row(row, k, lab, dist, ib, sk, sl);
+    if (do_merge) merge_row(row, k, lab, dist, ib, ms);
     const int32_t id = decode(lab);
     const bool isnew = have && lab >= 0;
     const bool isold = have && lab < 0 && (split <= 0 || ((row < split) == (id < split)));
@@ -523,16 +551,14 @@ __global__ void k_finalize(int64_t n, int k, const int32_t *__restrict__ gid,
                            hdb_nnd_element *__restrict__ out) {
   const int lane = lane_id();
   const int wpb = blockDim.x >> 5;
-  __shared__ uint64_t merge_keys[8][32];  // per-warp merge scratch (8 warps per block)
-  __shared__ int32_t merge_labs[8][32];
-  uint64_t *sk = merge_keys[threadIdx.x >> 5];
-  int32_t *sl = merge_labs[threadIdx.x >> 5];
+  __shared__ MergeSmem merge_smem[8];  // per-warp merge scratch (8 warps per block)
+  MergeSmem &ms = merge_smem[threadIdx.x >> 5];
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     const bool have = lane < k;
     int32_t lab = have ? gid[row * k + lane] : 0;
     float dist = have ? gdist[row * k + lane] : 0.0f;
-    merge_row(row, k, lab, dist, ib, sk, sl);
+    merge_row(row, k, lab, dist, ib, ms);
     if (have) {
       hdb_nnd_element e;
       e.distance_ = dist;
@@ -1400,7 +1426,7 @@ struct NndState {
     oend = Buf<uint32_t>(ctx, n);
     HDB_CUDA(cudaMemsetAsync(ostart, 0, n * 4, st));
     HDB_CUDA(cudaMemsetAsync(oend, 0, n * 4, st));
-    ib = Inbox{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, cap};
+    ib = Inbox{inbox_cnt, inbox, ovf, ovf_tgt, ovf_key, ostart, oend, dropped, cap, list_only ? 0 : 1};
     HDB_CUDA(cudaMemsetAsync(nrev, 0, n * 4, st));
     HDB_CUDA(cudaMemsetAsync(orev, 0, n * 4, st));
     clear_inboxes(ctx, n);

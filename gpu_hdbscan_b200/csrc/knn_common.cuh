@@ -34,6 +34,7 @@ struct Inbox {
   uint32_t *ostart, *oend;       // [n] segment of each row in the sorted overflow list
   unsigned long long *counters;  // [0] dropped [1] rows gathered [2] candidates [3] overflow
   int64_t ovf_cap;
+  int32_t inboxes;               // 0: no per-row inboxes (the tensor-core join's list only)
 };
 
 // Space of the candidate list a warp writes into: [pos, end), taken from the
