@@ -224,21 +224,29 @@ __global__ void __launch_bounds__(256, 3) k_init(const float *__restrict__ X, in
     }
     const int64_t lrow = (order ? (int64_t)order[row] : row) - base;
     // InitKNNGraphIndexKernel (nndescent.cu:1673-1692): xorshift64star(pos) % n,
-    // advanced past the row itself -- and here also past ids already taken.
-    int64_t label = (int64_t)(xorshift64star((uint64_t)(lrow * k + lane)) % (uint64_t)cnt);
-    for (int t = 0; t < k; t++) {
-      while (true) {
-        int64_t c = __shfl_sync(0xffffffffu, label, t);
-        bool dup = (lane < t) && (label == c);
-        if (c != lrow && __ballot_sync(0xffffffffu, dup) == 0) break;
-        if (lane == t) label = (label + 1) % cnt;
-      }
+    // advanced past the row itself -- and here also past ids already taken:
+    // slot t takes the first of its draw, draw + 1, ... (mod n) that is
+    // neither the row nor taken by a slot before it.  All slots advance
+    // together, each while it equals the row or an earlier slot's current id
+    // (one match_any per round); a slot never steps over its final id that
+    // way (the ids it steps over are the row or earlier slots' final ids), so
+    // the fixed point is that sequential result.  A slot steps at most k
+    // times, so k * (k + 1) / 2 rounds bound the loop.
+    const int32_t lrow32 = (int32_t)lrow, cnt32 = (int32_t)cnt;
+    int32_t label = (int32_t)(xorshift64star((uint64_t)(lrow * k + lane)) % (uint64_t)cnt);
+    const uint32_t below = lanemask_lt();
+    for (int round = 0; round <= kMaxK * (kMaxK + 1) / 2; round++) {
+      // lanes past k carry values no id takes
+      const uint32_t same = __match_any_sync(0xffffffffu, lane < k ? label : (int32_t)(0x80000000u | lane));
+      const bool step = lane < k && (label == lrow32 || (same & below) != 0);
+      if (__ballot_sync(0xffffffffu, step) == 0) break;
+      if (step) label = label + 1 == cnt32 ? 0 : label + 1;
     }
-    label += base;
-    if (order && lane < k) label = inv[label];
-    const float ds = diffsum_staged(X, d, row, (int32_t)label, lane < k, sm);
+    int64_t lab64 = (int64_t)label + base;
+    if (order && lane < k) lab64 = inv[lab64];
+    const float ds = diffsum_staged(X, d, row, (int32_t)lab64, lane < k, sm);
     uint64_t key = ~0ull;
-    if (lane < k) key = pack(ds, (int32_t)label);
+    if (lane < k) key = pack(ds, (int32_t)lab64);
     key = warp_sort32(key);
     if (lane < k) {
       gid[row * k + lane] = pk_id(key);  // all "new"
