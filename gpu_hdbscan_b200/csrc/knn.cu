@@ -71,6 +71,13 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
 // and each lane then walks its own row's staged segment in dimension order:
 // the reference's sequential FP32 difference sum (nndescent.cu:1086-1093),
 // sum = fmaf(a_j - b_j, a_j - b_j, sum) for j = 0..d-1.
+// Two FP32 differences b - a with one packed instruction: b + (-a), per
+// component the same rounding as __fsub_rn(b, a) = -__fsub_rn(a, b), so its
+// square is the square of the reference's a - b, bit for bit.
+__device__ __forceinline__ float2 neg_diff2(float2 b, float2 a) {
+  return __fadd2_rn(b, make_float2(-a.x, -a.y));
+}
+
 constexpr int kStageCols = 32;
 constexpr int kStageLd = kStageCols + 1;                    // conflict-free column walk
 constexpr int kRingSlot = kStageCols + 32 * kStageCols;     // 16-byte form: own + 32 rows
@@ -138,14 +145,12 @@ __device__ __forceinline__ float diffsum_staged_v4(const float *__restrict__ X, 
       for (int p = 0; p < nq; p++) {
         const float4 b = *reinterpret_cast<const float4 *>(mine + 4 * (p ^ (lane & 7)));
         const float4 a = *reinterpret_cast<const float4 *>(own + 4 * p);
-        float df = __fsub_rn(a.x, b.x);
-        s = __fmaf_rn(df, df, s);
-        df = __fsub_rn(a.y, b.y);
-        s = __fmaf_rn(df, df, s);
-        df = __fsub_rn(a.z, b.z);
-        s = __fmaf_rn(df, df, s);
-        df = __fsub_rn(a.w, b.w);
-        s = __fmaf_rn(df, df, s);
+        const float2 d01 = neg_diff2(make_float2(b.x, b.y), make_float2(a.x, a.y));
+        const float2 d23 = neg_diff2(make_float2(b.z, b.w), make_float2(a.z, a.w));
+        s = __fmaf_rn(d01.x, d01.x, s);
+        s = __fmaf_rn(d01.y, d01.y, s);
+        s = __fmaf_rn(d23.x, d23.x, s);
+        s = __fmaf_rn(d23.y, d23.y, s);
       }
     }
   }
@@ -768,14 +773,12 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
               const float4 xa = *reinterpret_cast<const float4 *>(pa + i * kJc);
 #pragma unroll
               for (int j = 0; j < 4; j++) {
-                float df = __fsub_rn(xa.x, xc[j].x);
-                float s_ = __fmaf_rn(df, df, acc[u][i][j]);
-                df = __fsub_rn(xa.y, xc[j].y);
-                s_ = __fmaf_rn(df, df, s_);
-                df = __fsub_rn(xa.z, xc[j].z);
-                s_ = __fmaf_rn(df, df, s_);
-                df = __fsub_rn(xa.w, xc[j].w);
-                acc[u][i][j] = __fmaf_rn(df, df, s_);
+                const float2 d01 = neg_diff2(make_float2(xc[j].x, xc[j].y), make_float2(xa.x, xa.y));
+                const float2 d23 = neg_diff2(make_float2(xc[j].z, xc[j].w), make_float2(xa.z, xa.w));
+                float s_ = __fmaf_rn(d01.x, d01.x, acc[u][i][j]);
+                s_ = __fmaf_rn(d01.y, d01.y, s_);
+                s_ = __fmaf_rn(d23.x, d23.x, s_);
+                acc[u][i][j] = __fmaf_rn(d23.y, d23.y, s_);
               }
             }
           }
