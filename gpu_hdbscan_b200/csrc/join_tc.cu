@@ -169,6 +169,26 @@ __device__ __noinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity,
   }
 }
 
+// Waits until *cnt (how many uses of a ring entry have been armed) reaches
+// `need`.  A parity wait can tell only the barrier's current phase from the
+// one before, so a waiter must never be two phases ahead: a producer first
+// waits here for the entry's previous use to be armed -- by whichever
+// producer had it -- and only then for that use's release.  Bounded like
+// mbar_wait.
+__device__ __noinline__ bool wait_armed(const uint32_t *cnt, uint32_t need, volatile int *abort) {
+  const volatile uint32_t *c = cnt;
+  if (*c >= need) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1;; it++) {
+    if (*c >= need) return true;
+    if (it > 8) __nanosleep(32);
+    if ((it & 15) == 0) {
+      if (abort && *abort) return false;
+      if (globaltimer() - t0 > kWaitNs) return false;
+    }
+  }
+}
+
 __device__ __forceinline__ void give_up(Shared &sh, uint32_t *err) {
   *reinterpret_cast<volatile int *>(&sh.abort) = 1;
   atomicOr(err, DEVERR_TIMEOUT);
@@ -438,7 +458,8 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
   for (uint32_t i = p; t < ntiles; t += step, i += kProducers) {
     const int m = i % kMetaSlots;
     const uint32_t muse = i / kMetaSlots;
-    if (!__all_sync(0xffffffffu, mbar_wait(&sh.mempty[m], (muse & 1) ^ 1, &sh.abort))) {
+    if (!__all_sync(0xffffffffu, wait_armed(&sh.marmed[m], muse, &sh.abort) &&
+                                     mbar_wait(&sh.mempty[m], (muse & 1) ^ 1, &sh.abort))) {
       give_up(sh, a.err);
       break;
     }
@@ -476,7 +497,8 @@ __device__ void producer(int p, const CUtensorMap *xmap, const JoinArgs &a, Shar
       const uint32_t g = i * (uint32_t)kbc + kb;
       const int s = g % kStages;
       const uint32_t use = g / kStages;
-      if (!__all_sync(0xffffffffu, mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort))) {
+      if (!__all_sync(0xffffffffu, wait_armed(&sh.armed[s], use, &sh.abort) &&
+                                       mbar_wait(&sh.empty[s], (use & 1) ^ 1, &sh.abort))) {
         ok = false;
         break;
       }
