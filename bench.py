@@ -55,7 +55,8 @@ def parse_args():
     ap.add_argument("--loop-instances", type=int, default=256,
                     help="batched workloads: instances timed in the per-instance loop comparison")
     ap.add_argument("--no-compare", action="store_true",
-                    help="skip timing the other form (plain FP32 vs BF16-TC)")
+                    help="skip timing the other form (plain FP32 vs BF16-TC) and, for "
+                         "batched workloads, the per-instance loop")
     ap.add_argument("--recall-queries", type=int, default=1000)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="points in the CPU baseline sample (0: sized per workload)")
@@ -633,8 +634,9 @@ def run_ours_batch(args, bw):
 
     # per-instance loop (hdb_run per instance) against the batch on the same
     # instances; the loop skips the instances the batch found disconnected
-    # (hdb_run stops on them, as the reference does)
-    m = min(args.loop_instances, len(views))
+    # (hdb_run stops on them, as the reference does).  --no-compare (and
+    # --bare) leave it out: it launches ~1,000 kernels per instance.
+    m = 0 if args.no_compare else min(args.loop_instances, len(views))
     sub = [v for v, s_ in zip(views[:m], stats[-1]["instance_status"][:m]) if s_ == 0]
     n_sub = sum(len(v) for v in sub)
     loop_failed = []
@@ -649,12 +651,14 @@ def run_ours_batch(args, bw):
                     raise
                 loop_failed.append(1)
 
-    lms, _ = timed(loop_once, 1, 1)
-    bms, _ = timed(lambda: ctx.hdbscan_batched(sub, **kw_b), 1, 1)
-    loop = {"instances": len(sub), "points": n_sub,
-            "loop_points_per_s": round(n_sub / (lms / 1e3), 1), "loop_ms": round(lms, 3),
-            "batched_points_per_s": round(n_sub / (bms / 1e3), 1), "batched_ms": round(bms, 3),
-            "speedup": round(lms / bms, 3), "loop_disconnected": len(loop_failed)}
+    loop = None
+    if sub:
+        lms, _ = timed(loop_once, 1, 1)
+        bms, _ = timed(lambda: ctx.hdbscan_batched(sub, **kw_b), 1, 1)
+        loop = {"instances": len(sub), "points": n_sub,
+                "loop_points_per_s": round(n_sub / (lms / 1e3), 1), "loop_ms": round(lms, 3),
+                "batched_points_per_s": round(n_sub / (bms / 1e3), 1), "batched_ms": round(bms, 3),
+                "speedup": round(lms / bms, 3), "loop_disconnected": len(loop_failed)}
 
     e2e = None
     if not args.no_e2e:
