@@ -474,12 +474,12 @@ __device__ __forceinline__ void merge_batch(int k, uint64_t &rkey, int32_t &lab,
 // Merge of everything offered to a row (inbox, best dropped, the row's
 // segment of the sorted candidate list) into its sorted list (one warp), in
 // batches of 64.  On return, lane j (< k) holds the j-th entry of the merged
-// row.  The tensor-core form keeps no inboxes (ib.inboxes = 0).
+// row.  The list forms keep no inboxes (ib.inboxes = 0).
 __device__ __forceinline__ void merge_row(int64_t row, int k, int32_t &lab, float &dist,
                                           const Inbox &ib, MergeSmem &ms) {
   const int lane = lane_id();
   int cnt = ib.inboxes ? ib.cnt[row] : 0;
-  const uint64_t ov = ib.inboxes ? ib.best[row] : ~0ull;
+  const uint64_t ov = ib.best[row];  // the best candidate that found no room (normally none)
   const uint32_t o0 = ib.ostart[row], o1 = ib.oend[row];
   if (cnt == 0 && ov == ~0ull && o0 == o1) return;
   __syncwarp();
@@ -695,6 +695,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
   float *Xs = reinterpret_cast<float *>(base + JoinSmem::kBest * 8 + JoinSmem::kIds * 4);
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   unsigned long long w_rows = 0, w_cands = 0;
+  ListCursor cur;  // this warp's space in the candidate list
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
     // counts and both sample lists in one memory round trip
@@ -819,20 +820,22 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
       }
     }  // passes
     __syncwarp();
-    int pushed = 0;
-    if (lane < nn) {
-      const int32_t x = ids[lane];
-      const uint64_t b1 = best1[lane], b2 = best2[lane];
-      if (b1 != ~0ull) pushed += push_candidate(x, pk_id(b1), pk_dist(b1), worst, ib);
-      if (b2 != ~0ull) pushed += push_candidate(x, pk_id(b2), pk_dist(b2), worst, ib);
-    }
-    if (lane < no) {
-      const uint64_t b3 = best3[lane];
-      if (b3 != ~0ull) pushed += push_candidate(ids[32 + lane], pk_id(b3), pk_dist(b3), worst, ib);
-    }
-    w_cands += pushed;
+    // the candidates that can enter their target's list go to the candidate
+    // list, which is sorted by target before the merge (space reserved 1024
+    // slots at a time per warp; no returning atomic per candidate)
+    const int32_t x = lane < nn ? ids[lane] : 0;
+    const uint64_t b1 = lane < nn ? best1[lane] : ~0ull, b2 = lane < nn ? best2[lane] : ~0ull;
+    const float wx = lane < nn ? worst[x] : 0.0f;
+    const int32_t x3 = lane < no ? ids[32 + lane] : 0;
+    const uint64_t b3 = lane < no ? best3[lane] : ~0ull;
+    const float wx3 = lane < no ? worst[x3] : 0.0f;
+    const bool v1 = b1 != ~0ull && pk_dist(b1) < wx, v2 = b2 != ~0ull && pk_dist(b2) < wx;
+    const bool v3 = b3 != ~0ull && pk_dist(b3) < wx3;
+    w_cands += append_candidates(ib, cur, (uint32_t)n, v1, x, b1, v2, x, b2);
+    w_cands += append_candidates(ib, cur, (uint32_t)n, v3, x3, b3, false, 0, 0ull);
     __syncwarp();
   }
+  list_fill(ib, cur.pos, cur.end, (uint32_t)n);  // the rest of the last chunk
   // per-warp totals, one atomic each (no block-wide barrier)
 #pragma unroll
   for (int o = 16; o; o >>= 1) w_cands += __shfl_xor_sync(0xffffffffu, w_cands, o);
@@ -1425,12 +1428,12 @@ struct NndState {
     inbox = Buf<uint64_t>(ctx, list_only ? 1 : (size_t)n * kInboxCap);
     ovf = Buf<unsigned long long>(ctx, n);
     dropped = Buf<unsigned long long>(ctx, 4);
-    // room for a pass's candidates; the tensor-core join's warps also leave
-    // the unused tail of their last list chunk (at most one chunk per
-    // epilogue warp)
+    // room for a pass's candidates; the joins' warps also leave the unused
+    // tail of their last list chunk (at most one chunk per warp: 8 epilogue
+    // warps per SM in the tensor-core join, up to 24 in the FP32 join)
     const int64_t rows = list_only ? 64 : 16;
     const int64_t cap = (n * rows > (1 << 22) ? n * rows : (1 << 22)) +
-                        (list_only ? (int64_t)8 * ctx->num_sms * kListChunk : 0);
+                        (list_only ? (int64_t)24 * ctx->num_sms * kListChunk : 0);
     ovf_tgt = Buf<uint32_t>(ctx, cap);
     ovf_key = Buf<uint64_t>(ctx, cap);
     ostart = Buf<uint32_t>(ctx, n);
@@ -1457,7 +1460,10 @@ void fp32_join(Context *ctx, int tiles, const float *X, int64_t n, int d, int S,
                int cross_only) {
   const int jw = kJoinWarps;
   const size_t smem = JoinSmem::kBytes * jw;
-  const int grid = grid_for(ctx, n, jw, 16);
+  // the blocks that fit on the GPU at once (a grid-stride loop over the rows):
+  // each warp holds one chunk of list space, so their number bounds what the
+  // list loses to unused chunk tails
+  const int grid = grid_for(ctx, n, jw, tiles == 1 ? 3 : 2);
   cudaStream_t st = ctx->stream;
   if (tiles == 1) {
     HDB_CUDA(cudaFuncSetAttribute(k_join<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1513,7 +1519,7 @@ int fp32_join_tiles(Context *ctx, int d, int k, int S, bool resident, const floa
   const int64_t want = (int64_t(256) << 20) / (4 * (int64_t)d);
   const int64_t m = std::min<int64_t>(
       n, std::max<int64_t>(65536, std::min<int64_t>(int64_t(1) << 20, want)));
-  NndState t(ctx, m, k, S, false);
+  NndState t(ctx, m, k, S, true);
   Buf<int32_t> nrev0(ctx, m), orev0(ctx, m);
   const int wpb = 8;
   const int grid_rows = grid_for(ctx, m, wpb, 16);
@@ -1565,12 +1571,13 @@ int64_t nndescent_bytes_per_point(int32_t d, const hdb_knn_params &p) {
   const int64_t k = p.k, S = p.sample_num;
   const bool half = p.precision == HDB_PREC_BF16 || p.precision == HDB_PREC_FP16;
   const bool tc = half && tc_dpad(d) <= kTcMaxDpad;
+  const bool list = tc || !half;                 // the tensor-core and FP32 joins
   const int64_t dpad = tc ? tc_dpad(d) : (d + 15) & ~15;
   int64_t b = 4 * (int64_t)d;                    // X in locality order
   if (half) b += 2 * dpad + 4;                   // 16-bit rows + norms
   b += 8 * k + 4 + 16 * S + 30;                  // lists, worst, samples, counters
-  if (!tc) b += 8 * kInboxCap;                   // per-row inboxes
-  b += 2 * 12 * (tc ? 64 : 16);                  // candidate list + sort buffers
+  if (!list) b += 8 * kInboxCap;                 // per-row inboxes
+  b += 2 * 12 * (list ? 64 : 16);                // candidate list + sort buffers
   b += 8 * k;                                    // graph in locality order
   return b;
 }
@@ -1588,15 +1595,15 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
                   p.precision == HDB_PREC_FP16,
               HDB_ERR_ARG, "NN-Descent: unknown precision");
   cudaStream_t st = ctx->stream;
-  // The tensor-core join appends every candidate to the list that
-  // sort_overflow groups by target for the merge (a returning inbox atomic per
-  // candidate cost it more than the sort), so it needs no inboxes and a list
-  // for a whole iteration's candidates.  The SIMT joins, whose own work is
-  // cheaper, keep the inboxes: for them the sort would cost more than the
-  // atomics (10M x 12: 737 vs 810 ms a step).
+  // The tensor-core join and the FP32 join append every candidate to the
+  // list that sort_overflow groups by target for the merge (a returning inbox
+  // atomic per candidate cost them more than the sort), so they need no
+  // inboxes and a list for a whole iteration's candidates.  The mma.sync join
+  // (16-bit forms past 256 dimensions) keeps the per-row inboxes.
   const bool tc_form = (p.precision == HDB_PREC_BF16 || p.precision == HDB_PREC_FP16) &&
                        tc_dpad(d) <= kTcMaxDpad;
-  NndState s(ctx, n, k, S, tc_form);
+  const bool list_form = tc_form || p.precision == HDB_PREC_FP32;
+  NndState s(ctx, n, k, S, list_form);
   int32_t *gid = s.gid, *newS = s.newS, *oldS = s.oldS, *nrev = s.nrev, *orev = s.orev;
   float *gdist = s.gdist, *worst = s.worst;
   int8_t *nf = s.nf, *of = s.of;
@@ -1773,7 +1780,7 @@ void knn_merge(Context *ctx, const float *X1, int64_t n1, const hdb_nnd_element 
   HDB_CUDA(cudaMemcpyAsync(X.get(), X1, (size_t)n1 * d * sizeof(float), cudaMemcpyDeviceToDevice, st));
   HDB_CUDA(cudaMemcpyAsync(X.get() + (size_t)n1 * d, X2, (size_t)n2 * d * sizeof(float),
                            cudaMemcpyDeviceToDevice, st));
-  NndState s(ctx, n, k, S, false);
+  NndState s(ctx, n, k, S, true);
   int32_t *gid = s.gid;
   float *gdist = s.gdist, *worst = s.worst;
   const Inbox &ib = s.ib;
