@@ -1,6 +1,7 @@
 // Context management, error reporting and stream-ordered scratch memory.
 #include <cstdio>
 #include <cstring>
+#include <iterator>
 
 #include "hdb_internal.cuh"
 
@@ -57,19 +58,32 @@ static size_t size_class(size_t bytes) {
 
 void *Context::cache_take(size_t bytes, size_t *cls) {
   const size_t c = size_class(bytes);
-  *cls = c;
-  auto it = cache_free.find(c);
-  if (it != cache_free.end()) {
+  // the smallest idle block of this class or up to half again as large: a
+  // call whose sizes differ a little from the last one's reuses its blocks
+  // instead of asking the driver for new ones
+  auto it = cache_free.lower_bound(c);
+  if (it != cache_free.end() && it->first <= c + c / 2) {
+    *cls = it->first;
     void *p = it->second;
     cache_free.erase(it);
     return p;
   }
+  *cls = c;
   void *p = nullptr;
   cudaError_t e = cudaMalloc(&p, c);
-  if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and retry once
+  if (e == cudaErrorMemoryAllocation && !cache_free.empty()) {
+    // give idle blocks back, largest first, until the request fits (releasing
+    // all of them would make the next caller allocate them all again)
     cudaGetLastError();
-    cache_release();
-    e = cudaMalloc(&p, c);
+    cudaStreamSynchronize(stream);  // queued work may still use a free block
+    while (e == cudaErrorMemoryAllocation && !cache_free.empty()) {
+      auto last = std::prev(cache_free.end());
+      cudaFree(last->second);
+      cache_bytes -= last->first;
+      cache_free.erase(last);
+      cudaGetLastError();
+      e = cudaMalloc(&p, c);
+    }
   }
   HDB_CUDA(e);
   cache_bytes += c;

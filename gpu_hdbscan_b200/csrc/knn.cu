@@ -64,6 +64,25 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
   return v;
 }
 
+// warp_sort32 with a 32-bit payload that moves with its key (keys distinct
+// within the warp, or equal only where the payload does not matter).
+__device__ __forceinline__ void warp_sort32_with(uint64_t &v, int32_t &pl) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint64_t o = __shfl_xor_sync(0xffffffffu, v, stride);
+      const int32_t op = __shfl_xor_sync(0xffffffffu, pl, stride);
+      const bool up = ((lane & size) == 0);
+      const bool lower = (lane & stride) == 0;
+      const bool take = (lower == up) ? o < v : v < o;  // the other lane's key is the min / max
+      v = take ? o : v;
+      pl = take ? op : pl;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Exact sequential difference sums of one row against up to 32 other rows,
 // one per lane.  The 32 rows are staged through shared memory 32 dimensions
@@ -1159,17 +1178,12 @@ __global__ void __launch_bounds__(256, 3) k_rerank(const float *__restrict__ X, 
     if (lane < k) lab = G[row * k + lane].label_;
     const int32_t id = decode(lab);
     const float ds = diffsum_staged(X, d, row, id, lane < k, sm);
-    const uint64_t key = lane < k ? pack(ds, id) : ~0ull;
-    const uint64_t sorted = warp_sort32(key);
-    const int32_t sid = pk_id(sorted);
-    int32_t slab = sid;
-    for (int t = 0; t < k; t++) {
-      const int32_t l = __shfl_sync(0xffffffffu, lab, t);
-      if (decode(l) == sid) slab = l;
-    }
+    uint64_t key = lane < k ? pack(ds, id) : ~0ull;
+    int32_t slab = lab;  // the entry (with its old/new flag) moves with its key
+    warp_sort32_with(key, slab);
     if (lane < k) {
       hdb_nnd_element e;
-      e.distance_ = pk_dist(sorted);
+      e.distance_ = pk_dist(key);
       e.label_ = slab;
       G[row * k + lane] = e;
     }
@@ -1337,15 +1351,10 @@ __device__ __forceinline__ void remap_row(int k, int32_t in_lab, float in_dist,
   const int lane = lane_id();
   const bool have = lane < k;
   const int32_t id = have ? idmap[decode(in_lab)] : 0;
-  const bool old = have && in_lab < 0;
-  const uint64_t key = warp_sort32(have ? pack(in_dist, id) : ~0ull);
+  uint64_t key = have ? pack(in_dist, id) : ~0ull;
+  int32_t flag = have && in_lab < 0;  // moves with its key (ids are distinct within a row)
+  warp_sort32_with(key, flag);
   const int32_t mine = pk_id(key);
-  bool flag = false;
-  for (int t = 0; t < k; t++) {  // ids are distinct within a row
-    const int32_t idt = __shfl_sync(0xffffffffu, id, t);
-    const bool ot = __shfl_sync(0xffffffffu, old, t);
-    if (idt == mine) flag = ot;
-  }
   out_dist = pk_dist(key);
   out_lab = flag ? -mine - 1 : mine;
 }
