@@ -24,6 +24,12 @@ import ctypes as C
 from dataclasses import dataclass
 
 from . import _lib
+
+# hdb_instance (include/hdb/hdb.h) as a numpy record, laid out like _lib.Instance
+_INSTANCE_DTYPE = np.dtype({"names": ["X", "n", "d", "num_clusters", "labels", "G", "status",
+                                      "reserved"],
+                            "formats": ["<u8", "<i8", "<i4", "<i4", "<u8", "<u8", "<i4", "<i4"],
+                            "offsets": [0, 8, 16, 20, 24, 32, 40, 44], "itemsize": 48})
 from ._lib import (HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP16, HDB_PREC_FP32,
                    HDB_STAB_FP32, HDB_STAB_FP64, HdbError)
 
@@ -320,23 +326,35 @@ class Context:
         if Gs is not None:
             Gs = [torch.as_tensor(G).to(dtype=torch.int32).contiguous() if host
                   else G.to(device=self.device, dtype=torch.int32).contiguous() for G in Gs]
-        labels = [torch.empty(X.shape[0], dtype=torch.int32, device=dev) for X in Xs]
-        graphs = [torch.empty((X.shape[0], k, 2), dtype=torch.int32, device=dev) for X in Xs] \
-            if want_graphs else Gs
-        insts = (_lib.Instance * len(Xs))()
-        for i, X in enumerate(Xs):
-            insts[i].X = X.data_ptr()
-            insts[i].n = X.shape[0]
-            insts[i].d = X.shape[1]
-            insts[i].labels = labels[i].data_ptr()
-            insts[i].G = graphs[i].data_ptr() if graphs is not None else None
+        # one label buffer (and one graph buffer) for all instances, split into
+        # views, and the hdb_instance records filled column by column: per-call
+        # host work that does not grow by a Python loop of allocations
+        T = len(Xs)
+        ns = np.fromiter((X.shape[0] for X in Xs), dtype=np.int64, count=T)
+        off = np.zeros(T + 1, dtype=np.int64)
+        np.cumsum(ns, out=off[1:])
+        lab_all = torch.empty(int(off[-1]), dtype=torch.int32, device=dev)
+        labels = [lab_all[int(off[i]):int(off[i + 1])] for i in range(T)]
+        if want_graphs:
+            g_all = torch.empty((int(off[-1]), k, 2), dtype=torch.int32, device=dev)
+            graphs = [g_all[int(off[i]):int(off[i + 1])] for i in range(T)]
+        else:
+            graphs = Gs
+        rec = np.zeros(T, dtype=_INSTANCE_DTYPE)
+        rec["X"] = np.fromiter((X.data_ptr() for X in Xs), dtype=np.uint64, count=T)
+        rec["n"] = ns
+        rec["d"] = np.fromiter((X.shape[1] for X in Xs), dtype=np.int32, count=T)
+        rec["labels"] = np.uint64(lab_all.data_ptr()) + (off[:-1] * 4).astype(np.uint64)
+        if graphs is not None:
+            rec["G"] = np.fromiter((G_.data_ptr() for G_ in graphs), dtype=np.uint64, count=T)
+        insts = (_lib.Instance * T).from_buffer(rec)
         st = _lib.RunStats()
-        rc = fn(self.h, insts, len(Xs), C.byref(p), C.byref(st))
+        rc = fn(self.h, insts, T, C.byref(p), C.byref(st))
         if rc != _lib.HDB_OK and (strict or rc != _lib.HDB_ERR_DISCONNECTED):
             _lib.check(rc)
         stats = {f: getattr(st, f) for f, _ in _lib.RunStats._fields_}
-        stats["instance_status"] = [insts[i].status for i in range(len(Xs))]
-        ncl = [insts[i].num_clusters for i in range(len(Xs))]
+        stats["instance_status"] = rec["status"].tolist()
+        ncl = rec["num_clusters"].tolist()
         if want_graphs:
             return labels, ncl, stats, graphs
         return labels, ncl, stats
