@@ -100,6 +100,42 @@ def profiled_traffic(kernel):
     return None
 
 
+def fp32_issue_roofline(stats, d, clk):
+    """The FP32 local join against its FP32 issue bound: each computed pair
+    (join_pairs, counted live) costs d subtractions and d fused multiply-adds,
+    3 FLOP per dimension; the bound is SMs x 128 FP32 lanes x 2 FLOP x the SM
+    clock sampled during the run."""
+    import torch
+    pairs, ms = stats.get("join_pairs", 0), stats.get("join_ms", 0.0)
+    if not pairs or not ms:
+        return None
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    achieved = pairs * d * 3 / (ms / 1e3) / 1e12
+    peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+    launches = max(1, stats.get("join_launches", 1))
+    return {"kernel": "k_join (FP32 local join)", "bound": "fp32_issue",
+            "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 4), "pairs_per_launch": round(pairs / launches),
+            "sm_mhz": mhz, "form": stats.get("join_config")}
+
+
+def tensor_roofline(n_points, d, stats, bf16_peak, iterations):
+    """The tensor-core join against the measured dense BF16 peak: every tile
+    (two rows' joins) is one M = N = 128 MMA chain over the padded dimensions,
+    2 x 128 x 128 x dpad FLOP, about rows / 2 tiles per iteration.  join_ms
+    also holds the slot-list pass before each launch."""
+    ms = stats.get("join_ms", 0.0)
+    if not ms:
+        return None
+    dpad = (d + 63) // 64 * 64
+    flops = iterations * ((n_points + 1) // 2) * 2 * 128 * 128 * dpad
+    achieved = flops / (ms / 1e3) / 1e12
+    return {"kernel": "k_join_tc (tcgen05 Gram tiles)", "bound": "tensor",
+            "achieved": round(achieved, 1), "peak": bf16_peak, "unit": "TFLOP/s",
+            "frac": round(achieved / bf16_peak, 4)}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -394,6 +430,8 @@ def run_ours(args, w):
                    "ms_per_step": round(oms / osteps, 3), "steps": osteps,
                    "stage_ms": {s_: round(ostats[-1][f"ms_{s_}"], 3) for s_ in
                                 ("knn", "graph", "mst", "tree", "total")}}
+        if other == g.HDB_PREC_FP32:
+            compare["issue_roofline"] = fp32_issue_roofline(ostats[-1], w.d, clk)
     recall = {}
     if args.recall_queries > 0:
         qidx = torch.randperm(w.n, generator=torch.Generator().manual_seed(7))[:args.recall_queries]
@@ -484,6 +522,12 @@ def run_ours(args, w):
                                                      if compare else None)},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
                 "gpu_launches": int(sum(s["gpu_launches"] for s in stats))}
+        # the join's compute bound beside the HBM one
+        if jkernel == "k_join_tc":
+            line["tensor_roofline"] = tensor_roofline(w.n, w.d, last, measured_peaks()[1],
+                                                      w.iterations)
+        elif jkernel == "k_join":
+            line["issue_roofline"] = fp32_issue_roofline(last, w.d, clk)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
@@ -734,6 +778,15 @@ def run_ours_batch(args, bw):
                                             if args.shard_instances else None)},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
                 "gpu_launches": int(sum(s_["gpu_launches"] for s_ in stats))}
+        # the join's compute bound beside the HBM one: for the FP32 join with
+        # the points-weighted mean d (pairs are not counted per d); for the
+        # tensor-core join when the batch has one d
+        if prec == g.HDB_PREC_FP32:
+            d_mean = sum(d * c for d, c in per_d.items()) / n_total
+            line["issue_roofline"] = fp32_issue_roofline(last, d_mean, clk)
+        elif len(per_d) == 1:
+            line["tensor_roofline"] = tensor_roofline(n_total, next(iter(per_d)), last,
+                                                      measured_peaks()[1], bw.iterations)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

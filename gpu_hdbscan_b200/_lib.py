@@ -60,7 +60,7 @@ class RunStats(C.Structure):
                 ("join_ms", C.c_float), ("join_launches", C.c_int32),
                 ("join_rows_gathered", C.c_int64), ("join_candidates", C.c_int64),
                 ("gpu_launches", C.c_int64), ("mst_multiplier", C.c_int32),
-                ("join_config", C.c_int32)]
+                ("join_config", C.c_int32), ("join_pairs", C.c_int64)]
 
 
 class Instance(C.Structure):

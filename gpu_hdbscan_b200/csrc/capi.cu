@@ -577,6 +577,8 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
   js_acc->launches += js.launches;
   js_acc->rows_gathered += js.rows_gathered;
   js_acc->candidates += js.candidates;
+  js_acc->pairs += js.pairs;
+  if (js.config) js_acc->config = js.config;  // the FP32 join's form (the last group's)
 }
 
 // hdb_run / hdb_run_with_graph: the whole path on one instance; G_out
@@ -640,6 +642,7 @@ hdb_status run_single(hdb_ctx *h, const float *X, int64_t n, int32_t d, const hd
       rs.join_ms = (float)js.ms;
       rs.join_launches = (int32_t)js.launches;
       rs.join_config = js.config;
+      rs.join_pairs = js.pairs;
       rs.join_rows_gathered = js.rows_gathered;
       rs.join_candidates = js.candidates;
       rs.gpu_launches = ctx->launches - launches0;
@@ -735,6 +738,7 @@ hdb_status run_batched(hdb_ctx *h, hdb_instance *insts, int32_t count, const hdb
       rs.join_ms = (float)js.ms;
       rs.join_launches = (int32_t)js.launches;
       rs.join_config = js.config;
+      rs.join_pairs = js.pairs;
       rs.join_rows_gathered = js.rows_gathered;
       rs.join_candidates = js.candidates;
       rs.gpu_launches = ctx->launches - launches0;

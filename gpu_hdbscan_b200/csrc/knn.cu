@@ -713,7 +713,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
   int32_t *ids = reinterpret_cast<int32_t *>(base + JoinSmem::kBest * 8);
   float *Xs = reinterpret_cast<float *>(base + JoinSmem::kBest * 8 + JoinSmem::kIds * 4);
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
-  unsigned long long w_rows = 0, w_cands = 0;
+  unsigned long long w_rows = 0, w_cands = 0, w_pairs = 0;
   ListCursor cur;  // this warp's space in the candidate list
   for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
        row += (int64_t)gridDim.x * wpb) {
@@ -755,6 +755,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
     __syncwarp();
     if (nn == 0 || nn + no < 2 || (cross_only && no == 0)) continue;
     w_rows += nn + no;
+    w_pairs += (cross_only ? 0 : nn * (nn - 1) / 2) + nn * no;  // the reference's pairs
     const int rg = (nn + 3) >> 2;                              // row groups (new rows)
     const int cgn = cross_only ? 0 : rg, cgo = (no + 3) >> 2;  // column groups: new, old
     const int tiles = (cgn > 0 ? rg * (rg + 1) / 2 : 0) + rg * cgo;
@@ -861,6 +862,7 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
   if (lane == 0) {
     if (w_rows) atomicAdd(&ib.counters[1], w_rows);
     if (w_cands) atomicAdd(&ib.counters[2], w_cands);
+    if (w_pairs) atomicAdd(&ib.counters[4], w_pairs);
   }
 }
 // ---------------------------------------------------------------------------
@@ -1436,7 +1438,7 @@ struct NndState {
     of = Buf<int8_t>(ctx, n);
     inbox = Buf<uint64_t>(ctx, list_only ? 1 : (size_t)n * kInboxCap);
     ovf = Buf<unsigned long long>(ctx, n);
-    dropped = Buf<unsigned long long>(ctx, 4);
+    dropped = Buf<unsigned long long>(ctx, 5);
     // room for a pass's candidates; the joins' warps also leave the unused
     // tail of their last list chunk (at most one chunk per warp: 8 epilogue
     // warps per SM in the tensor-core join, up to 24 in the FP32 join)
@@ -1460,7 +1462,7 @@ struct NndState {
     cudaStream_t st = ctx->stream;
     HDB_CUDA(cudaMemsetAsync(inbox_cnt, 0, n * 4, st));
     HDB_CUDA(cudaMemsetAsync(ovf, 0xff, n * 8, st));
-    HDB_CUDA(cudaMemsetAsync(dropped, 0, 4 * sizeof(unsigned long long), st));
+    HDB_CUDA(cudaMemsetAsync(dropped, 0, 5 * sizeof(unsigned long long), st));
   }
 };
 
@@ -1746,7 +1748,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   }
   k_loc_restore<<<grid_rows, 32 * wpb, 0, st>>>(Gp, order, n, k, G); ctx->launches++;
   HDB_CHECK_LAUNCH();
-  HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 3 * sizeof(unsigned long long),
+  HDB_CUDA(cudaMemcpyAsync(ctx->pinned, dropped, 5 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   ctx->sync();
   if (use_tc)
@@ -1757,6 +1759,7 @@ void nndescent(Context *ctx, const float *X, int64_t n, int32_t d, const hdb_knn
   if (js) {
     js->rows_gathered = hs[1];
     js->candidates = hs[2];
+    js->pairs = hs[4];
     js->launches = p.iterations;
     js->ms = 0.0;
     for (int it = 0; it < p.iterations; it++) {

@@ -8,7 +8,7 @@ namespace hdb {
 // its launches, rows staged in shared memory and candidates pushed.
 struct JoinStats {
   double ms = 0.0;
-  int64_t launches = 0, rows_gathered = 0, candidates = 0;
+  int64_t launches = 0, rows_gathered = 0, candidates = 0, pairs = 0;
   int32_t config = 0;  // FP32 join tile slots per lane (1 or 2); 0: a 16-bit join
 };
 

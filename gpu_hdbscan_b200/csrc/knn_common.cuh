@@ -33,6 +33,7 @@ struct Inbox {
   uint64_t *ovf_key;             // [ovf_cap] overflow: packed candidate (sorted along)
   uint32_t *ostart, *oend;       // [n] segment of each row in the sorted overflow list
   unsigned long long *counters;  // [0] dropped [1] rows gathered [2] candidates [3] overflow
+                                 // [4] distance pairs computed (FP32 join)
   int64_t ovf_cap;
   int32_t inboxes;               // 0: no per-row inboxes (the tensor-core join's list only)
 };

@@ -113,6 +113,9 @@ typedef struct {
   int32_t mst_multiplier;       /* mst_gpu = 1: the weight scale exponent m (single runs) */
   int32_t join_config;          /* FP32 local join: 4 x 4 distance tiles per lane (1 or 2),
                                    forced (hdb_set_join_tiles) or tuned; 0 for a 16-bit join */
+  int64_t join_pairs;           /* FP32 local join: distance pairs computed, all launches
+                                   (the reference's new x new and new x old pairs); 0 for a
+                                   16-bit join */
 } hdb_run_stats;
 
 typedef struct hdb_ctx hdb_ctx;
