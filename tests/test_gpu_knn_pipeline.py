@@ -159,7 +159,10 @@ def test_recall_on_the_100k_blob_config_is_the_references(ctx, oracle, prec):
     make_ref_golden.py --nndescent-recall) or better.  The reference's own
     NN-Descent, compiled for sm_100a and run on the same data, recorded 0.0015:
     its graph stays near the random initial one, so the bound it gives is
-    trivially met and the restatement is the working anchor."""
+    trivially met and the restatement is the working anchor.  The BF16 form is
+    held to the restatement run in the same form (orc_nndescent_form: BF16
+    candidate distances, exact re-rank) within 0.5 pt; what the form itself
+    costs against FP32 at d = 12 (0.4-0.6 pt, measured) stays under 1 pt."""
     from gpu_hdbscan_b200 import HDB_PREC_BF16, HDB_PREC_FP32, synth
     ref = _golden_recall("blobs_100k_d12")
     X = synth.generate(synth.WORKLOADS["blobs_100k_d12"])
@@ -169,7 +172,13 @@ def test_recall_on_the_100k_blob_config_is_the_references(ctx, oracle, prec):
     ids, _ = ctx.knn_split(ctx.NNDescent(X, k=32, sample_num=16, iterations=6, precision=pc))
     r = oracle.recall(_t(ids)[q], gt, 32)
     assert r >= ref["ref_recall32"] - 0.005, (r, ref)
-    assert r >= ref["oracle_recall32"] - 0.005, (r, ref)
+    if prec == "bf16":
+        fids, _ = oracle.nndescent_form(X, "bf16")
+        r_form = oracle.recall(fids[q], gt, 32)
+        assert r >= r_form - 0.005, (r, r_form)
+        assert r >= ref["oracle_recall32"] - 0.010, (r, ref)
+    else:
+        assert r >= ref["oracle_recall32"] - 0.005, (r, ref)
 
 
 @pytest.mark.parametrize("prec", ["fp32", "bf16"])
