@@ -715,14 +715,28 @@ __global__ void __launch_bounds__(32 * kJoinWarps, kTiles == 1 ? 3 : 2)
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   unsigned long long w_rows = 0, w_cands = 0, w_pairs = 0;
   ListCursor cur;  // this warp's space in the candidate list
-  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < n;
-       row += (int64_t)gridDim.x * wpb) {
-    // counts and both sample lists in one memory round trip
-    const int64_t sb = row * (2 * S);
-    const int32_t nraw = lane < 2 * S ? newS[sb + lane] : 0;
-    const int32_t oraw = lane < 2 * S ? oldS[sb + lane] : 0;
-    const int cnf = nf[row], cof = of[row];
-    const int cnr = min(nrev[row], S), cor = min(orev[row], S);
+  const int64_t stride = (int64_t)gridDim.x * wpb;
+  // a row's counts and both sample lists in one memory round trip, loaded one
+  // row ahead so that they are in flight while the previous row is joined
+  int32_t q_nraw = 0, q_oraw = 0;
+  int q_cnf = 0, q_cof = 0, q_cnr = 0, q_cor = 0;
+  auto load_lists = [&](int64_t r) {
+    if (r >= n) return;
+    const int64_t sb = r * (2 * S);
+    q_nraw = lane < 2 * S ? newS[sb + lane] : 0;
+    q_oraw = lane < 2 * S ? oldS[sb + lane] : 0;
+    q_cnf = nf[r];
+    q_cof = of[r];
+    q_cnr = nrev[r];
+    q_cor = orev[r];
+  };
+  int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5);
+  load_lists(row);
+  for (; row < n; row += stride) {
+    const int32_t nraw = q_nraw, oraw = q_oraw;
+    const int cnf = q_cnf, cof = q_cof;
+    const int cnr = min(q_cnr, S), cor = min(q_cor, S);
+    load_lists(row + stride);
     __syncwarp();
     if (lane == 0) { nrev[row] = 0; orev[row] = 0; }
     // slot t < S: forward sample t; slot S + t: reverse sample t
