@@ -31,10 +31,12 @@ _INSTANCE_DTYPE = np.dtype({"names": ["X", "n", "d", "num_clusters", "labels", "
                             "formats": ["<u8", "<i8", "<i4", "<i4", "<u8", "<u8", "<i4", "<i4"],
                             "offsets": [0, 8, 16, 20, 24, 32, 40, 44], "itemsize": 48})
 from ._lib import (HDB_DIST_SQRT, HDB_DIST_SQUARED, HDB_PREC_BF16, HDB_PREC_FP16, HDB_PREC_FP32,
-                   HDB_STAB_FP32, HDB_STAB_FP64, HdbError)
+                   HDB_STAB_FP32, HDB_STAB_FP64, HDB_MST_FLOAT, HDB_MST_QUANTISED,
+                   HDB_MST_ID_ORDER, HDB_ORDER_EDGE, HDB_ORDER_IDS, HdbError)
 
 __all__ = ["Context", "HdbError", "EnhancedGraph", "HDB_PREC_FP32", "HDB_PREC_BF16", "HDB_PREC_FP16",
-           "HDB_DIST_SQRT", "HDB_DIST_SQUARED", "HDB_STAB_FP32", "HDB_STAB_FP64"]
+           "HDB_DIST_SQRT", "HDB_DIST_SQUARED", "HDB_STAB_FP32", "HDB_STAB_FP64",
+           "HDB_MST_FLOAT", "HDB_MST_QUANTISED", "HDB_MST_ID_ORDER", "HDB_ORDER_EDGE", "HDB_ORDER_IDS"]
 
 
 def _ptr(t):
@@ -191,6 +193,21 @@ class Context:
                              self._view(g.eweight, g.edges, torch.float32),
                              self._view(g.antihubs, g.num_antihubs, torch.int32), g)
 
+    def graph_from_csr(self, nindex, nlist, eweight) -> EnhancedGraph:
+        """An ECLgraph over caller arrays (nindex [n+1] int64, nlist [E] int32,
+        eweight [E] float32, copied to the device), e.g. for hdb_mst on a graph
+        that was not built here.  The returned object keeps the arrays alive."""
+        torch = self._torch
+        ni = self._dev(nindex, torch.int64)
+        nl = self._dev(nlist, torch.int32)
+        ew = self._dev(eweight, torch.float32)
+        if ni.dim() != 1 or nl.shape != ew.shape or ni.shape[0] < 2 or int(ni[-1]) != nl.shape[0]:
+            raise ValueError("graph_from_csr: inconsistent CSR arrays")
+        empty = torch.empty(0, dtype=torch.int32, device=self.device)
+        g = _lib.Graph(ni.shape[0] - 1, nl.shape[0], ni.data_ptr(), nl.data_ptr(), ew.data_ptr(),
+                       0, None)
+        return EnhancedGraph(g.nodes, g.edges, ni, nl, ew, empty, g)
+
     def _view(self, ptr, count, dtype):
         """Copies `count` elements of context-owned device memory into a tensor."""
         torch = self._torch
@@ -203,16 +220,22 @@ class Context:
                 raise HdbError(_lib.HDB_ERR_CUDA, f"cudaMemcpy failed ({res})")
         return out
 
-    def buildMST(self, graph: EnhancedGraph, with_in_mst=False):
+    def buildMST(self, graph: EnhancedGraph, with_in_mst=False, order=None):
         """-> (mst [n-1, 3] int32 view of MSTedge sorted by (weight, edge index),
-               in_mst uint8 [edges] or None, Boruvka rounds)."""
+               in_mst uint8 [edges] or None, Boruvka rounds).  order=HDB_ORDER_IDS
+        spans and lists the tree under (weight, min id, max id) instead
+        (hdb_mst_ordered); None or HDB_ORDER_EDGE is the reference's hdb_mst."""
         torch = self._torch
         n = graph.nodes
         mst = torch.empty((n - 1, 3), dtype=torch.int32, device=self.device)
         inm = torch.empty(graph.edges, dtype=torch.uint8, device=self.device) if with_in_mst else None
         rounds = C.c_int32(0)
-        _lib.check(self.L.hdb_mst(self.h, C.byref(graph.raw), _ptr(inm), _ptr(mst),
-                                  C.byref(rounds)))
+        if order is None:
+            _lib.check(self.L.hdb_mst(self.h, C.byref(graph.raw), _ptr(inm), _ptr(mst),
+                                      C.byref(rounds)))
+        else:
+            _lib.check(self.L.hdb_mst_ordered(self.h, C.byref(graph.raw), order, _ptr(inm),
+                                              _ptr(mst), C.byref(rounds)))
         return mst, inm, rounds.value
 
     def buildMST_quantised(self, graph: EnhancedGraph, dist, with_in_mst=False):

@@ -19,6 +19,8 @@ STATUS_NAMES = {0: "HDB_OK", 1: "HDB_ERR_ARG", 2: "HDB_ERR_ALLOC", 3: "HDB_ERR_C
 HDB_PREC_FP32, HDB_PREC_BF16, HDB_PREC_FP16 = 0, 1, 2
 HDB_DIST_SQRT, HDB_DIST_SQUARED = 0, 1
 HDB_STAB_FP32, HDB_STAB_FP64 = 0, 1
+HDB_MST_FLOAT, HDB_MST_QUANTISED, HDB_MST_ID_ORDER = 0, 1, 2
+HDB_ORDER_EDGE, HDB_ORDER_IDS = 0, 1
 
 # Every symbol include/hdb/hdb.h declares.
 EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_set_stream",
@@ -27,7 +29,7 @@ EXPORTS = ("hdb_version", "hdb_last_error", "hdb_create", "hdb_destroy", "hdb_se
            "hdb_sort_edges", "hdb_linkage_tree", "hdb_condense_select", "hdb_run",
            "hdb_run_with_graph", "hdb_run_knn", "hdb_sort_edges_noalloc", "hdb_bf16_distance_tiles",
            "hdb_core_sg", "hdb_run_batched", "hdb_run_knn_batched", "hdb_mst_quantised",
-           "hdb_knn_merge")
+           "hdb_knn_merge", "hdb_mst_ordered")
 
 
 class HdbError(RuntimeError):
@@ -96,6 +98,7 @@ def load(path: str = LIB_PATH):
         "hdb_fix_distances": (C.c_int, [_P, _P, _I64, _I32, _P, _I32, _P]),
         "hdb_enhanced_knng": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, C.POINTER(Graph)]),
         "hdb_mst": (C.c_int, [_P, C.POINTER(Graph), _P, _P, C.POINTER(_I32)]),
+        "hdb_mst_ordered": (C.c_int, [_P, C.POINTER(Graph), _I32, _P, _P, C.POINTER(_I32)]),
         "hdb_mst_quantised": (C.c_int, [_P, C.POINTER(Graph), _P, _I32, _P, _P, C.POINTER(_I32),
                                         C.POINTER(_I32)]),
         "hdb_sort_edges": (C.c_int, [_P, _P, _I64]),

@@ -31,6 +31,8 @@
 //   --fp64              FP64 stability sums (default: the reference's FP32)
 //   --bf16              build the kNN graph with the BF16 tensor-core form
 //   --fp16              build the kNN graph with the FP16 tensor-core form
+//   --id-order          float MST (mst_gpu 0) under the tie order (weight,
+//                       min id, max id) instead of (weight, CSR edge index)
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -120,7 +122,7 @@ int main(int argc, char **argv) {
   std::vector<std::string> pos;
   std::string kgraph, vectors, vectors_txt, write_fvecs, labels_path, save_kgraph, save_fixed,
       save_mst;
-  bool squared = false, fp64 = false, bf16 = false, fp16 = false;
+  bool squared = false, fp64 = false, bf16 = false, fp16 = false, id_order = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     auto val = [&](std::string &dst) {
@@ -138,6 +140,7 @@ int main(int argc, char **argv) {
     else if (a == "--squared") squared = true;
     else if (a == "--fp64") fp64 = true;
     else if (a == "--bf16") bf16 = true;
+    else if (a == "--id-order") id_order = true;
     else if (a == "--fp16") fp16 = true;
     else pos.push_back(a);
   }
@@ -246,8 +249,9 @@ int main(int argc, char **argv) {
     if (hdb_mst_quantised(ctx, &g, dist, k, nullptr, mst, &mult, &rounds) != HDB_OK)
       return fail("hdb_mst_quantised");
     printf("MST WEIGHT MULTIPLIER: 10^%d\n", mult);
-  } else if (hdb_mst(ctx, &g, nullptr, mst, &rounds) != HDB_OK) {
-    return fail("hdb_mst");
+  } else if (hdb_mst_ordered(ctx, &g, id_order ? HDB_ORDER_IDS : HDB_ORDER_EDGE, nullptr, mst,
+                             &rounds) != HDB_OK) {
+    return fail("hdb_mst_ordered");
   }
   const double t_mst = secs_since(t);
   t = std::chrono::steady_clock::now();

@@ -164,6 +164,19 @@ HDB_API hdb_status hdb_mst(hdb_ctx *h, const hdb_graph *graph, uint8_t *in_mst, 
   });
 }
 
+HDB_API hdb_status hdb_mst_ordered(hdb_ctx *h, const hdb_graph *graph, int32_t order,
+                                   uint8_t *in_mst, hdb_mst_edge *mst, int32_t *rounds) {
+  return guard([&] {
+    Context *ctx = C(h);
+    require_ptr(graph, "graph");
+    require_ptr(mst, "mst");
+    HDB_REQUIRE(order == HDB_ORDER_EDGE || order == HDB_ORDER_IDS, HDB_ERR_ARG,
+                "hdb_mst_ordered: unknown tie order");
+    boruvka_mst(ctx, graph, in_mst, mst, rounds, Segments{}, nullptr, nullptr,
+                order == HDB_ORDER_IDS);
+  });
+}
+
 HDB_API hdb_status hdb_mst_quantised(hdb_ctx *h, const hdb_graph *graph, const float *dist,
                                      int32_t k, uint8_t *in_mst, hdb_mst_edge *mst,
                                      int32_t *multiplier, int32_t *rounds) {
@@ -225,7 +238,9 @@ namespace {
 
 void check_run_params(const hdb_params &p) {
   check_knn_params(&p.knn);
-  HDB_REQUIRE(p.mst_gpu == 0 || p.mst_gpu == 1, HDB_ERR_ARG, "mst_gpu must be 0 or 1");
+  HDB_REQUIRE(p.mst_gpu == HDB_MST_FLOAT || p.mst_gpu == HDB_MST_QUANTISED ||
+                  p.mst_gpu == HDB_MST_ID_ORDER,
+              HDB_ERR_ARG, "mst_gpu must be 0, 1 or 2");
   const int32_t k = p.knn.k;
   HDB_REQUIRE(p.mpts >= 2 && p.mpts <= k, HDB_ERR_ARG, "mpts must satisfy 2 <= mpts <= k");
   HDB_REQUIRE(p.distance == HDB_DIST_SQRT || p.distance == HDB_DIST_SQUARED, HDB_ERR_ARG,
@@ -236,7 +251,7 @@ void check_run_params(const hdb_params &p) {
 
 // The stages after the kNN graph (HDBSCAN/_new.cu:243-347) on device arrays:
 // ids [n, k] decoded, core [n], X [n, d] -> labels [n].  Records ev[3..5].
-// first (p.mst_gpu only): every row's first-neighbour distance.
+// first (p.mst_gpu == HDB_MST_QUANTISED only): every row's first-neighbour distance.
 void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const float *X, int64_t n,
                    int32_t d, int32_t k, const hdb_params &p, int32_t *labels, hdb_run_stats *st,
                    const float *first) {
@@ -247,11 +262,12 @@ void run_after_knn(Context *ctx, const int32_t *ids, const float *core, const fl
   int32_t rounds = 0;
   Buf<hdb_mst_edge> mst(ctx, n - 1);
   Buf<double> p10;
-  if (p.mst_gpu) {
+  if (p.mst_gpu == HDB_MST_QUANTISED) {
     p10 = Buf<double>(ctx, 1);
     quant_scales(ctx, first, 1, n, Segments{}, p10, &st->mst_multiplier);
   }
-  boruvka_mst(ctx, &g, nullptr, mst, &rounds, Segments{}, nullptr, p10.get());
+  boruvka_mst(ctx, &g, nullptr, mst, &rounds, Segments{}, nullptr, p10.get(),
+              p.mst_gpu == HDB_MST_ID_ORDER);
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   int32_t ncl = 0;
   {
@@ -368,11 +384,12 @@ void batch_after_knn(Context *ctx, const int32_t *ids, const float *core, const 
   Buf<hdb_mst_edge> mst(ctx, n - T);
   std::vector<int32_t> iedges((size_t)T);
   Buf<double> p10;
-  if (p.mst_gpu) {  // every instance's own scale, as its own run would take it
+  if (p.mst_gpu == HDB_MST_QUANTISED) {  // every instance's own scale, as its own run would take it
     p10 = Buf<double>(ctx, T);
     quant_scales(ctx, first, 1, n, seg, p10, nullptr);
   }
-  const int64_t chosen = boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg, iedges.data(), p10.get());
+  const int64_t chosen = boruvka_mst(ctx, &g, nullptr, mst, &rounds, seg, iedges.data(), p10.get(),
+                                     p.mst_gpu == HDB_MST_ID_ORDER);
   HDB_CUDA(cudaEventRecord(ctx->ev[4], s));
   std::vector<int32_t> keep((size_t)T);
   std::vector<int64_t> pshift((size_t)T), eshift((size_t)T), off2(1, 0);
@@ -524,7 +541,7 @@ void run_batch_group(Context *ctx, hdb_instance *insts, const std::vector<int32_
     if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
     knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
     core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, core);
-    if (p.mst_gpu) {
+    if (p.mst_gpu == HDB_MST_QUANTISED) {
       first = Buf<float>(ctx, n);
       core_distances(ctx, dist.get(), X, ids, n, d, k, p.distance, first, 0);
     }
@@ -626,7 +643,7 @@ hdb_status run_single(hdb_ctx *h, const float *X, int64_t n, int32_t d, const hd
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, G, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
       core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
-      if (p.mst_gpu) {
+      if (p.mst_gpu == HDB_MST_QUANTISED) {
         first = Buf<float>(ctx, n);
         core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, first, 0);
       }
@@ -810,7 +827,7 @@ HDB_API hdb_status hdb_run_knn(hdb_ctx *h, const hdb_nnd_element *G, const float
       if (p.distance == HDB_DIST_SQUARED) dist = Buf<float>(ctx, (size_t)n * k);
       knn_split(ctx, Guse, n, k, ids, p.distance == HDB_DIST_SQUARED ? dist.get() : nullptr);
       core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, core);
-      if (p.mst_gpu) {
+      if (p.mst_gpu == HDB_MST_QUANTISED) {
         first = Buf<float>(ctx, n);
         core_distances(ctx, dist.get(), Xuse, ids, n, d, k, p.distance, first, 0);
       }

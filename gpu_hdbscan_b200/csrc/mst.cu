@@ -12,6 +12,12 @@
 // root), pointer jumping, and compaction of the edges that still cross
 // components.  The chosen keys, radix-sorted, give the reference's sorted
 // MSTedge list directly.
+//
+// The (weight, min id, max id) tie order replaces the edge index in the key's
+// low half by the edge's rank under (row, target, edge index) -- row and
+// target are the min and max id of a canonical entry -- so the same packed
+// comparison spans the graph under that order; the rank is mapped back to the
+// edge index once the tree is sorted.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -121,20 +127,94 @@ __global__ void k_emit_canon(const int64_t *__restrict__ nindex, const int32_t *
   }
 }
 
+// (weight, min id, max id) order, step 1: every canonical entry's
+// (row << bits | target) and edge index, in CSR order (a stable sort of the
+// pairs then breaks a repeated pair's tie by edge index).
+__global__ void k_emit_pairs(const int64_t *__restrict__ nindex, const int32_t *__restrict__ nlist,
+                             const int64_t *__restrict__ off, int64_t n, int bits,
+                             uint64_t *__restrict__ pair, uint32_t *__restrict__ eidx) {
+  const int lane = lane_id();
+  int64_t row = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+  for (; row < n; row += (int64_t)gridDim.x * kWarps) {
+    int64_t b = nindex[row], e = nindex[row + 1];
+    int64_t p = off[row];
+    for (int64_t j0 = b; j0 < e; j0 += 32) {
+      int64_t j = j0 + lane;
+      const int32_t t = j < e ? nlist[j] : -1;
+      bool take = t > row;
+      uint32_t m = __ballot_sync(0xffffffffu, take);
+      if (take) {
+        const int64_t q = p + __popc(m & lanemask_lt());
+        pair[q] = ((uint64_t)row << bits) | (uint64_t)t;
+        eidx[q] = (uint32_t)j;
+      }
+      p += __popc(m);
+    }
+  }
+}
+
+// Step 2: the edges with their rank r under (min id, max id, edge index) in
+// the key's low half.
+__global__ void k_emit_ranked(const uint64_t *__restrict__ pair, const uint32_t *__restrict__ eidx,
+                              const float *__restrict__ ew, int64_t m, int bits,
+                              CEdge *__restrict__ el) {
+  const uint64_t mask = (uint64_t(1) << bits) - 1;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t pk = pair[r];
+    CEdge c;
+    c.a = (int32_t)(pk >> bits);
+    c.b = (int32_t)(pk & mask);
+    c.key = ((uint64_t)weight_key(ew[eidx[r]]) << 32) | (uint64_t)r;
+    el[r] = c;
+  }
+}
+
+// Step 3 (after the chosen keys are sorted): the rank back to the edge index.
+__global__ void k_rank_to_edge(uint64_t *__restrict__ keys, int64_t m,
+                               const uint32_t *__restrict__ eidx) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[t];
+    keys[t] = (k & 0xffffffff00000000ull) | (uint64_t)eidx[(uint32_t)k];
+  }
+}
+
 __global__ void k_iota(int32_t *__restrict__ v, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     v[i] = (int32_t)i;
 }
 
+// Warp-aggregated minimum: the valid lanes that name the same representative
+// reduce their keys (high half, then the low half among the lanes holding the
+// least high half) and one lane of each group updates minkey.  The groups are
+// disjoint, so every lane of a group runs each reduction with that group's mask.
+__device__ __forceinline__ void warp_min_at(uint32_t act, bool valid, int32_t rep, uint64_t key,
+                                            unsigned long long *__restrict__ minkey) {
+  if (!valid) return;
+  const uint32_t grp = __match_any_sync(act, rep);
+  const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
+  const uint32_t mh = __reduce_min_sync(grp, hi);
+  const uint32_t low = grp & __ballot_sync(grp, hi == mh);
+  if (hi != mh) return;
+  const uint32_t ml = __reduce_min_sync(low, lo);
+  if (lane_id() == __ffs(low) - 1) {
+    const unsigned long long k = ((unsigned long long)mh << 32) | ml;
+    if (k < minkey[rep]) atomicMin(&minkey[rep], k);
+  }
+}
+
 __global__ void k_min_edge(const CEdge *__restrict__ el, int64_t m,
                            unsigned long long *__restrict__ minkey) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    CEdge c = el[i];
-    unsigned long long k = c.key;
-    if (k < minkey[c.a]) atomicMin(&minkey[c.a], k);
-    if (k < minkey[c.b]) atomicMin(&minkey[c.b], k);
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < m; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    const bool valid = i < m;
+    CEdge c = {};
+    if (valid) c = el[i];
+    const uint32_t act = __ballot_sync(0xffffffffu, valid);
+    warp_min_at(act, valid, c.a, c.key, minkey);
+    warp_min_at(act, valid, c.b, c.key, minkey);
   }
 }
 
@@ -358,9 +438,11 @@ void quant_scales(Context *ctx, const float *first, int64_t stride, int64_t n, c
 
 int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
                     int32_t *rounds_out, const Segments &seg, int32_t *inst_edges,
-                    const double *quant) {
+                    const double *quant, bool id_order) {
   const int64_t n = g->nodes;
   HDB_REQUIRE(n >= 2, HDB_ERR_ARG, "MST: need at least 2 nodes");
+  HDB_REQUIRE(!(id_order && quant), HDB_ERR_ARG,
+              "MST: the (weight, min id, max id) order is a float-weight mode");
   // one tree per instance: n - (number of instances) edges
   const int64_t me = n - (seg.count > 0 ? seg.count : 1);
   HDB_REQUIRE(g->edges < (int64_t(1) << 32), HDB_ERR_ARG, "MST: 2^32 or more edges");
@@ -378,7 +460,20 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
   ctx->sync();
   int64_t m = h[0];
   Buf<CEdge> el(ctx, m > 0 ? m : 1), el2(ctx, m > 0 ? m : 1);
-  k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, quant, seg, el); ctx->launches++;
+  Buf<uint32_t> eidx;  // id order: the edge index of every rank
+  if (id_order) {
+    int bits = 1;
+    while (bits < 31 && (int64_t(1) << bits) < n) bits++;
+    eidx = Buf<uint32_t>(ctx, m > 0 ? m : 1);
+    Buf<uint64_t> pair(ctx, m > 0 ? m : 1);
+    k_emit_pairs<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, off, n, bits, pair, eidx); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+    radix_sort_u64(ctx, pair, eidx, m, 0, 2 * bits);
+    k_emit_ranked<<<grid_for(ctx, m > 0 ? m : 1, 256), 256, 0, st>>>(pair, eidx, g->eweight, m, bits,
+                                                                     el); ctx->launches++;
+  } else {
+    k_emit_canon<<<gw, 32 * kWarps, 0, st>>>(g->nindex, g->nlist, g->eweight, off, n, quant, seg, el); ctx->launches++;
+  }
   HDB_CHECK_LAUNCH();
 
   Buf<unsigned long long> minkey(ctx, n);
@@ -423,6 +518,12 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
     ctx->sync();
   }
   const int64_t chosen = h[0];
+  if (id_order && chosen > 0 && chosen <= me) {
+    // sorted by (weight, rank) now; the low halves become edge indices after
+    radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
+    k_rank_to_edge<<<grid_for(ctx, chosen, 256), 256, 0, st>>>(keys, chosen, eidx); ctx->launches++;
+    HDB_CHECK_LAUNCH();
+  }
   if (inst_edges && seg.count > 0) {
     // a forest that may miss edges: report each instance's count instead
     HDB_REQUIRE(chosen <= me, HDB_ERR_INTERNAL, "MST: more edges than points");
@@ -453,7 +554,7 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
     k_quant_rekey<<<gm, 256, 0, st>>>(keys, chosen, g->nindex, g->eweight, n, quant, seg); ctx->launches++;
     HDB_CHECK_LAUNCH();
   }
-  radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
+  if (!id_order) radix_sort_u64(ctx, keys, nullptr, chosen, 0, 64);
   if (seg.count > 1) {
     // each instance's edges together, in (weight, edge index) order inside it
     Buf<hdb_mst_edge> tmp(ctx, chosen);

@@ -12,10 +12,13 @@ namespace hdb {
 // quant (device, one per instance or one): 10^m of the reference's mst_gpu = 1
 // mode (quant_scales) -- the tree under (int-quantised weight, edge index),
 // written with dequantised weights in (weight, edge index) order; nullptr for
-// the float weights of cpuMST.
+// the float weights of cpuMST.  id_order (float weights only): the tree and
+// its listing under (weight, min id, max id, edge index) instead of (weight,
+// edge index).
 int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_edge *mst,
                     int32_t *rounds_out, const Segments &seg = Segments{},
-                    int32_t *inst_edges = nullptr, const double *quant = nullptr);
+                    int32_t *inst_edges = nullptr, const double *quant = nullptr,
+                    bool id_order = false);
 // The mst_gpu = 1 scale of every instance (buildGPUgraph, core-sg.cu:8-44, with
 // GetMinDistanceFromKNNG's minimum): first[i * stride] is row i's first kNN
 // distance; p10_dev (device) and mult_out (host, optional) get one value per

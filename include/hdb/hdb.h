@@ -72,6 +72,11 @@ typedef struct {
 enum { HDB_PREC_FP32 = 0, HDB_PREC_BF16 = 1, HDB_PREC_FP16 = 2 };
 enum { HDB_DIST_SQRT = 0, HDB_DIST_SQUARED = 1 };
 enum { HDB_STAB_FP32 = 0, HDB_STAB_FP64 = 1 };
+/* MST modes (hdb_params.mst_gpu): the reference's two, then the float MST
+ * under the tie order (weight, min id, max id) of hdb_mst_ordered. */
+enum { HDB_MST_FLOAT = 0, HDB_MST_QUANTISED = 1, HDB_MST_ID_ORDER = 2 };
+/* Tie orders of hdb_mst_ordered. */
+enum { HDB_ORDER_EDGE = 0, HDB_ORDER_IDS = 1 };
 
 /* The compile-time parameters of gpuknn/nndescent.cuh:9-15 as run-time ones. */
 typedef struct {
@@ -92,8 +97,10 @@ typedef struct {
                           HDB_DIST_SQUARED: NN-Descent's squared distances kept */
   int32_t stability;   /* HDB_STAB_FP32 (tree.cu:494-511 order) or HDB_STAB_FP64 */
   int32_t host_io;     /* hdb_run only: 1 = X and labels are host pointers */
-  int32_t mst_gpu;     /* the reference's argv[4] (HDBSCAN/new.cu:38): 0 = the float
-                          MST of cpuMST; 1 = its int-quantised GPU MST (hdb_mst_quantised) */
+  int32_t mst_gpu;     /* the reference's argv[4] (HDBSCAN/new.cu:38): HDB_MST_FLOAT (0) =
+                          the float MST of cpuMST; HDB_MST_QUANTISED (1) = its int-quantised
+                          GPU MST (hdb_mst_quantised); HDB_MST_ID_ORDER (2, not in the
+                          reference) = the float MST under (weight, min id, max id) */
 } hdb_params;
 
 typedef struct {
@@ -220,6 +227,16 @@ HDB_API hdb_status hdb_mst(hdb_ctx *ctx, const hdb_graph *graph, uint8_t *in_mst
 HDB_API hdb_status hdb_mst_quantised(hdb_ctx *ctx, const hdb_graph *graph, const float *dist,
                                      int32_t k, uint8_t *in_mst, hdb_mst_edge *mst,
                                      int32_t *multiplier, int32_t *rounds);
+
+/* hdb_mst under a chosen tie order.  HDB_ORDER_EDGE: the reference's
+ * (weight, CSR edge index), the same result as hdb_mst.  HDB_ORDER_IDS:
+ * (weight, min id, max id), ties of a repeated pair broken by edge index --
+ * the tree and its listing both follow that order, so it depends only on the
+ * weighted edge set, not on the order of the CSR rows' entries.  Both trees
+ * have the same weight multiset (any two MSTs do); they differ only where
+ * tied weights leave the choice open. */
+HDB_API hdb_status hdb_mst_ordered(hdb_ctx *ctx, const hdb_graph *graph, int32_t order,
+                                   uint8_t *in_mst, hdb_mst_edge *mst, int32_t *rounds);
 
 /* sort_edges, HDBSCAN/merge_sort/merge_sort.cuh:30: stable ascending sort by
  * weight, in place. */

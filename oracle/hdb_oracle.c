@@ -884,6 +884,52 @@ int orc_kruskal(const int64_t *nindex, const int32_t *nlist, const float *eweigh
   return count == 0 ? ORC_OK : ORC_ERR_DISCONNECTED;
 }
 
+/* (weight, min id, max id, edge index): a canonical entry's row is its min id
+ * and its target its max id. */
+static int cmp_kedge_ids(const void *x, const void *y) {
+  const orc_kedge *p = (const orc_kedge *)x, *q = (const orc_kedge *)y;
+  if (p->w < q->w) return -1;
+  if (q->w < p->w) return 1;
+  if (p->a != q->a) return p->a < q->a ? -1 : 1;
+  if (p->b != q->b) return p->b < q->b ? -1 : 1;
+  return (p->j > q->j) - (p->j < q->j);
+}
+
+/* The float MST under a tie order: ORC_ORDER_EDGE is cpuMST's (weight, CSR
+ * edge index), mst.cu:34-78; ORC_ORDER_IDS is (weight, min id, max id, edge
+ * index).  Kruskal over the canonical entries (target > row) in that order;
+ * out[nodes - 1] receives the chosen edges in the order they were taken,
+ * which for ORC_ORDER_EDGE is the list orc_build_mst + orc_sort_edges give.
+ * in_mst [edges] (optional) receives the bool-per-edge result. */
+int orc_mst_ordered(const int64_t *nindex, const int32_t *nlist, const float *eweight,
+                    int32_t nodes, int64_t edges, int32_t order, uint8_t *in_mst,
+                    orc_mst_edge *out) {
+  if (in_mst) memset(in_mst, 0, (size_t)edges);
+  int32_t *parent = (int32_t *)malloc(sizeof(int32_t) * nodes);
+  for (int32_t i = 0; i < nodes; i++) parent[i] = i;
+  int64_t m = 0;
+  for (int32_t i = 0; i < nodes; i++)
+    for (int64_t j = nindex[i]; j < nindex[i + 1]; j++) m += (nlist[j] > i);
+  orc_kedge *list = (orc_kedge *)malloc(sizeof(orc_kedge) * (m > 0 ? m : 1));
+  m = 0;
+  for (int32_t i = 0; i < nodes; i++)
+    for (int64_t j = nindex[i]; j < nindex[i + 1]; j++)
+      if (nlist[j] > i) list[m++] = (orc_kedge){eweight[j], j, i, nlist[j]};
+  qsort(list, m, sizeof(orc_kedge), order == ORC_ORDER_IDS ? cmp_kedge_ids : cmp_kedge);
+  int64_t taken = 0;
+  for (int64_t p = 0; p < m && taken < nodes - 1; p++) {
+    int32_t ar = serial_find(list[p].a, parent), br = serial_find(list[p].b, parent);
+    if (ar != br) {
+      if (in_mst) in_mst[list[p].j] = 1;
+      out[taken++] = (orc_mst_edge){list[p].a, list[p].b, list[p].w};
+      if (ar > br) parent[br] = ar; else parent[ar] = br;
+    }
+  }
+  free(list);
+  free(parent);
+  return taken == nodes - 1 ? ORC_OK : ORC_ERR_DISCONNECTED;
+}
+
 /* buildMST, mst.cu:291-336 (before the sort): MST edges in CSR index order. */
 int orc_build_mst(const int64_t *nindex, const int32_t *nlist, const float *eweight,
                   int32_t nodes, int64_t edges, const uint8_t *in_mst, orc_mst_edge *out) {
@@ -1242,16 +1288,30 @@ int orc_get_clusters(const orc_condensed_node *t, int64_t size, orc_stab *stab,
 int orc_hdbscan_from_knn(const int32_t *ids, const float *dist, const float *X, int64_t n,
                          int32_t d, int32_t k, int32_t mpts, int32_t fp64,
                          orc_mst_edge *mst_out, int32_t *labels, int32_t *ncl) {
+  return orc_hdbscan_from_knn_order(ids, dist, X, n, d, k, mpts, fp64, ORC_ORDER_EDGE, mst_out,
+                                    labels, ncl);
+}
+
+int orc_hdbscan_from_knn_order(const int32_t *ids, const float *dist, const float *X, int64_t n,
+                               int32_t d, int32_t k, int32_t mpts, int32_t fp64, int32_t order,
+                               orc_mst_edge *mst_out, int32_t *labels, int32_t *ncl) {
   int64_t *nindex; int32_t *nlist; float *ew;
   int64_t E = orc_enhanced_knng(ids, dist, X, n, d, k, &nindex, &nlist, &ew, NULL, NULL);
   if (E < 0) return ORC_ERR_ARG;
-  uint8_t *in = (uint8_t *)malloc(E > 0 ? E : 1);
-  int rc = orc_kruskal(nindex, nlist, ew, (int32_t)n, E, in);
   orc_mst_edge *m = mst_out ? mst_out : (orc_mst_edge *)malloc(sizeof(orc_mst_edge) * (n - 1));
-  if (rc == ORC_OK) rc = orc_build_mst(nindex, nlist, ew, (int32_t)n, E, in, m);
-  free(in); free(nindex); free(nlist); free(ew);
-  if (rc != ORC_OK) { if (!mst_out) free(m); return rc; }
-  orc_sort_edges(m, n - 1);
+  int rc;
+  if (order == ORC_ORDER_IDS) {
+    rc = orc_mst_ordered(nindex, nlist, ew, (int32_t)n, E, order, NULL, m);
+    free(nindex); free(nlist); free(ew);
+    if (rc != ORC_OK) { if (!mst_out) free(m); return rc; }
+  } else {
+    uint8_t *in = (uint8_t *)malloc(E > 0 ? E : 1);
+    rc = orc_kruskal(nindex, nlist, ew, (int32_t)n, E, in);
+    if (rc == ORC_OK) rc = orc_build_mst(nindex, nlist, ew, (int32_t)n, E, in, m);
+    free(in); free(nindex); free(nlist); free(ew);
+    if (rc != ORC_OK) { if (!mst_out) free(m); return rc; }
+    orc_sort_edges(m, n - 1);
+  }
   orc_linkage_node *h = (orc_linkage_node *)malloc(sizeof(orc_linkage_node) * (n - 1));
   orc_linkage_tree(m, n, h);
   if (!mst_out) free(m);

@@ -83,6 +83,12 @@ int orc_mst_quantised(const int64_t *nindex, const int32_t *nlist, const float *
                       int32_t nodes, int64_t edges, const float *first_dist, orc_mst_edge *out,
                       int32_t *mult_out);
 void orc_sort_edges(orc_mst_edge *edges, int64_t m);
+/* Tie orders of the float MST: cpuMST's (weight, CSR edge index) and
+ * (weight, min id, max id, edge index). */
+enum { ORC_ORDER_EDGE = 0, ORC_ORDER_IDS = 1 };
+int orc_mst_ordered(const int64_t *nindex, const int32_t *nlist, const float *eweight,
+                    int32_t nodes, int64_t edges, int32_t order, uint8_t *in_mst,
+                    orc_mst_edge *out);
 
 /* ---- trees (HDBSCAN/trees/tree.cu) ---- */
 void orc_linkage_tree(const orc_mst_edge *sorted, int64_t num_points, orc_linkage_node *out);
@@ -98,6 +104,11 @@ int orc_get_clusters(const orc_condensed_node *tree, int64_t size, orc_stab *sta
 int orc_hdbscan_from_knn(const int32_t *ids, const float *dist, const float *X, int64_t n,
                          int32_t d, int32_t k, int32_t mpts, int32_t fp64_stability,
                          orc_mst_edge *mst_out, int32_t *labels_out, int32_t *num_clusters_out);
+/* The same with the MST under a tie order (ORC_ORDER_EDGE is the above). */
+int orc_hdbscan_from_knn_order(const int32_t *ids, const float *dist, const float *X, int64_t n,
+                               int32_t d, int32_t k, int32_t mpts, int32_t fp64_stability,
+                               int32_t order, orc_mst_edge *mst_out, int32_t *labels_out,
+                               int32_t *num_clusters_out);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,7 @@ def lib():
             "orc_enhanced_knng": (_I64, [_P, _P, _P, _I64, _I32, _I32, _P, _P, _P, _P, _P]),
             "orc_core_sg": (_I64, [_P, _P, _P, _I64, _I32, _I32, _P, _P, _P, _P]),
             "orc_kruskal": (C.c_int, [_P, _P, _P, _I32, _I64, _P]),
+            "orc_mst_ordered": (C.c_int, [_P, _P, _P, _I32, _I64, _I32, _P, _P]),
             "orc_build_mst": (C.c_int, [_P, _P, _P, _I32, _I64, _P, _P]),
             "orc_mst_quantised": (C.c_int, [_P, _P, _P, _I32, _I64, _P, _P, _P]),
             "orc_sort_edges": (None, [_P, _I64]),
@@ -71,6 +72,8 @@ def lib():
             "orc_get_clusters": (C.c_int, [_P, _I64, _P, _P, _I64, _I64, _P, _P]),
             "orc_hdbscan_from_knn": (C.c_int, [_P, _P, _P, _I64, _I32, _I32, _I32, _I32, _P,
                                                _P, _P]),
+            "orc_hdbscan_from_knn_order": (C.c_int, [_P, _P, _P, _I64, _I32, _I32, _I32, _I32,
+                                                     _I32, _P, _P, _P]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -267,6 +270,26 @@ def kruskal(nindex, nlist, eweight):
     return inmst[:E].astype(bool)
 
 
+ORDER_EDGE, ORDER_IDS = 0, 1
+
+
+def mst_ordered(nindex, nlist, eweight, order):
+    """The float MST under a tie order (ORDER_EDGE: the reference's (weight,
+    CSR edge index); ORDER_IDS: (weight, min id, max id, edge index)), listed
+    in that order: (MST_EDGE[n-1], in_mst bool[edges])."""
+    nindex = _c(nindex, np.int64)
+    nlist = _c(nlist, np.int32)
+    eweight = _c(eweight, np.float32)
+    n, E = len(nindex) - 1, len(nlist)
+    out = np.zeros(n - 1, MST_EDGE)
+    inmst = np.zeros(max(E, 1), np.uint8)
+    rc = lib().orc_mst_ordered(_p(nindex), _p(nlist), _p(eweight), n, E, order, _p(inmst),
+                               _p(out))
+    if rc:
+        raise RuntimeError("graph is disconnected")
+    return out, inmst[:E].astype(bool)
+
+
 def build_mst(nindex, nlist, eweight, inmst):
     nindex = _c(nindex, np.int64)
     nlist = _c(nlist, np.int32)
@@ -341,8 +364,9 @@ def get_clusters(tree, stab, n, stab64=None):
     return labels, ncl.value
 
 
-def hdbscan_from_knn(ids, dist, X, mpts, fp64=False):
-    """The reference call order from a given kNN graph: (sorted MST, labels)."""
+def hdbscan_from_knn(ids, dist, X, mpts, fp64=False, order=None):
+    """The reference call order from a given kNN graph: (sorted MST, labels).
+    order=ORDER_IDS takes the MST under (weight, min id, max id)."""
     ids = _c(ids, np.int32)
     dist = _c(dist, np.float32)
     X = _c(X, np.float32)
@@ -350,8 +374,13 @@ def hdbscan_from_knn(ids, dist, X, mpts, fp64=False):
     mst = np.zeros(n - 1, MST_EDGE)
     labels = np.empty(n, np.int32)
     ncl = C.c_int32(0)
-    rc = lib().orc_hdbscan_from_knn(_p(ids), _p(dist), _p(X), n, X.shape[1], k, mpts,
-                                    int(fp64), _p(mst), _p(labels), C.byref(ncl))
+    if order is None:
+        rc = lib().orc_hdbscan_from_knn(_p(ids), _p(dist), _p(X), n, X.shape[1], k, mpts,
+                                        int(fp64), _p(mst), _p(labels), C.byref(ncl))
+    else:
+        rc = lib().orc_hdbscan_from_knn_order(_p(ids), _p(dist), _p(X), n, X.shape[1], k, mpts,
+                                              int(fp64), order, _p(mst), _p(labels),
+                                              C.byref(ncl))
     if rc:
         raise RuntimeError(f"orc_hdbscan_from_knn failed ({rc})")
     return mst, labels, ncl.value
