@@ -186,35 +186,43 @@ __global__ void k_iota(int32_t *__restrict__ v, int64_t n) {
     v[i] = (int32_t)i;
 }
 
-// Warp-aggregated minimum: the valid lanes that name the same representative
-// reduce their keys (high half, then the low half among the lanes holding the
-// least high half) and one lane of each group updates minkey.  The groups are
-// disjoint, so every lane of a group runs each reduction with that group's mask.
-__device__ __forceinline__ void warp_min_at(uint32_t act, bool valid, int32_t rep, uint64_t key,
-                                            unsigned long long *__restrict__ minkey) {
-  if (!valid) return;
-  const uint32_t grp = __match_any_sync(act, rep);
-  const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
-  const uint32_t mh = __reduce_min_sync(grp, hi);
-  const uint32_t low = grp & __ballot_sync(grp, hi == mh);
-  if (hi != mh) return;
-  const uint32_t ml = __reduce_min_sync(low, lo);
-  if (lane_id() == __ffs(low) - 1) {
-    const unsigned long long k = ((unsigned long long)mh << 32) | ml;
-    if (k < minkey[rep]) atomicMin(&minkey[rep], k);
-  }
-}
-
+// Minimum incident edge of every representative.  The edge list is written
+// row by row and compaction keeps each warp's order, so lanes that name the
+// same `a` endpoint sit in runs of consecutive lanes: each run reduces its keys
+// with redux.sync (the high halves, then the low halves of the lanes holding
+// the least high half) and one lane of the run updates minkey.  The `b`
+// endpoints of a run are distinct targets; each updates its own entry behind
+// a read of the current minimum.
 __global__ void k_min_edge(const CEdge *__restrict__ el, int64_t m,
                            unsigned long long *__restrict__ minkey) {
+  const int lane = lane_id();
   for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < m; i0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = i0 + threadIdx.x;
     const bool valid = i < m;
-    CEdge c = {};
+    CEdge c;
+    c.a = -1;  // an invalid lane is a run of its own that nobody reduces
+    c.b = -1;
+    c.key = ~0ull;
     if (valid) c = el[i];
-    const uint32_t act = __ballot_sync(0xffffffffu, valid);
-    warp_min_at(act, valid, c.a, c.key, minkey);
-    warp_min_at(act, valid, c.b, c.key, minkey);
+    const int32_t aprev = __shfl_up_sync(0xffffffffu, c.a, 1);
+    const uint32_t heads = __ballot_sync(0xffffffffu, lane == 0 || aprev != c.a);
+    if (!valid) continue;
+    const uint32_t le = heads & (0xffffffffu >> (31 - lane));  // heads at or below this lane
+    const uint32_t gt = heads & ~(0xffffffffu >> (31 - lane));  // heads above it
+    const int first = 31 - __clz(le);
+    const int end = gt ? __ffs(gt) - 1 : 32;
+    const uint32_t run = (end == 32 ? 0xffffffffu : ((1u << end) - 1)) & ~((1u << first) - 1);
+    const uint32_t hi = (uint32_t)(c.key >> 32), lo = (uint32_t)c.key;
+    const uint32_t mh = __reduce_min_sync(run, hi);
+    const uint32_t low = run & __ballot_sync(run, hi == mh);
+    if (hi == mh) {
+      const uint32_t ml = __reduce_min_sync(low, lo);
+      if (lane == __ffs(low) - 1) {
+        const unsigned long long k = ((unsigned long long)mh << 32) | ml;
+        if (k < minkey[c.a]) atomicMin(&minkey[c.a], k);
+      }
+    }
+    if (c.key < minkey[c.b]) atomicMin(&minkey[c.b], c.key);
   }
 }
 

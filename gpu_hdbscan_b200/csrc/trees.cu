@@ -110,17 +110,40 @@ __global__ void k_validate_mst(const hdb_mst_edge *__restrict__ mst, int64_t m, 
   }
 }
 
+// Tags every component with its largest rank and counts its points.  At the
+// upper levels most active edges of a block share one root, so the lanes that
+// share the first active lane's root combine their rank maximum and point
+// count with redux.sync and one of them updates the root; the other lanes
+// update their own roots.
 __global__ void k_level_tag(const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
                             int64_t m, int64_t S, int64_t n, UfNode *u,
                             const int32_t *__restrict__ size) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    if (!active_lower(r, S, m)) continue;
-    int32_t a = la[r], b = lb[r];
-    int32_t root = uf_find(u, a);
-    atomicMax(&u[root].maxr, (int32_t)r);
-    if (atomicExch(&u[a].seen, 1) == 0) atomicAdd(&u[root].acc, a < n ? 1 : size[a]);
-    if (atomicExch(&u[b].seen, 1) == 0) atomicAdd(&u[root].acc, b < n ? 1 : size[b]);
+  const int lane = lane_id();
+  for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x; r0 < m; r0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = r0 + threadIdx.x;
+    const bool act = r < m && active_lower(r, S, m);
+    int32_t root = -1, add = 0;
+    if (act) {
+      const int32_t a = la[r], b = lb[r];
+      root = uf_find(u, a);
+      if (atomicExch(&u[a].seen, 1) == 0) add += a < n ? 1 : size[a];
+      if (atomicExch(&u[b].seen, 1) == 0) add += b < n ? 1 : size[b];
+    }
+    const uint32_t am = __ballot_sync(0xffffffffu, act);
+    if (!act) continue;
+    const int32_t lead = __shfl_sync(am, root, __ffs(am) - 1);
+    const uint32_t same = __ballot_sync(am, root == lead);
+    if (root == lead) {
+      const int32_t mr = __reduce_max_sync(same, (int32_t)r);
+      const int32_t sum = __reduce_add_sync(same, add);
+      if (lane == __ffs(same) - 1) {
+        atomicMax(&u[root].maxr, mr);
+        if (sum != 0) atomicAdd(&u[root].acc, sum);
+      }
+    } else {
+      atomicMax(&u[root].maxr, (int32_t)r);
+      if (add != 0) atomicAdd(&u[root].acc, add);
+    }
   }
 }
 
