@@ -33,8 +33,11 @@ namespace {
 // ---------------------------------------------------------------------------
 // Linkage tree
 // ---------------------------------------------------------------------------
-// Union-find over labels [0, 2n-1); hooks always point to a smaller label, so
-// every path ends at a root.  The step bounds only guard against corrupted
+// Union-find over labels [0, 2n-1); hooks always point to a larger label, so
+// every path ends at a root.  Hooking the smaller root keeps the hot labels
+// -- a big component's internal label n + rank, which many edges of a level
+// name -- as parents: the vertices joining it each hook their own record
+// instead of contending for the hot one.  The step bounds only guard against corrupted
 // state and report through the device error word.  A label's state at one
 // level -- parent, the largest rank tagged to it (as a root), whether it was
 // counted, the points its root accumulated -- is one 16-byte record, so the
@@ -61,7 +64,7 @@ __device__ __forceinline__ void uf_union(UfNode *u, int32_t a, int32_t b, uint32
     a = uf_find(u, a);
     b = uf_find(u, b);
     if (a == b) return;
-    if (a > b) { int32_t t = a; a = b; b = t; }
+    if (a < b) { int32_t t = a; a = b; b = t; }
     if (atomicCAS(&u[b].p, b, a) == b) return;
   }
   atomicOr(err, DEVERR_TIMEOUT);
