@@ -236,21 +236,33 @@ __global__ void k_winner(const CEdge *__restrict__ el, int64_t m,
   }
 }
 
-// Hook every representative to the component across its minimum edge.
+// Hook every representative to the component across its minimum edge.  The
+// chosen keys are appended with one atomicAdd per warp.
 __global__ void k_hook(const int32_t *__restrict__ reps, int64_t nr,
                        unsigned long long *__restrict__ minkey, const int32_t *__restrict__ other,
                        int32_t *__restrict__ parent, uint64_t *__restrict__ mst_keys,
                        unsigned long long *__restrict__ mst_count, int64_t cap) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nr;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int32_t v = reps[t];
-    unsigned long long mk = minkey[v];
-    if (mk == ~0ull) continue;
-    int32_t o = other[v];
-    bool mutual = other[o] == v;
-    parent[v] = (mutual && v < o) ? v : o;
-    if (!(mutual && v > o)) {
-      unsigned long long idx = atomicAdd(mst_count, 1ull);
+  const int lane = lane_id();
+  for (int64_t t0 = (int64_t)blockIdx.x * blockDim.x; t0 < nr; t0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = t0 + threadIdx.x;
+    bool emit = false;
+    unsigned long long mk = ~0ull;
+    if (t < nr) {
+      const int32_t v = reps[t];
+      mk = minkey[v];
+      if (mk != ~0ull) {
+        const int32_t o = other[v];
+        const bool mutual = other[o] == v;
+        parent[v] = (mutual && v < o) ? v : o;
+        emit = !(mutual && v > o);
+      }
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, emit);
+    unsigned long long base = 0;
+    if (lane == 0 && bal) base = atomicAdd(mst_count, (unsigned long long)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (emit) {
+      const unsigned long long idx = base + __popc(bal & lanemask_lt());
       if ((int64_t)idx < cap) mst_keys[idx] = mk;
     }
   }
@@ -287,26 +299,62 @@ __global__ void k_jump(const int32_t *__restrict__ reps, int64_t nr, int32_t *pa
 }
 
 // Relabel both endpoints to their new roots and keep the edges that still
-// join two components (warp-aggregated append; order does not matter).
-__global__ void k_relabel_filter(const CEdge *__restrict__ el, int64_t m,
-                                 const int32_t *__restrict__ parent, CEdge *__restrict__ out,
-                                 unsigned long long *__restrict__ out_count) {
-  const int lane = lane_id();
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < m; i0 += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i = i0 + threadIdx.x;
-    CEdge c;
-    bool keep = false;
-    if (i < m) {
-      c = el[i];
-      c.a = parent[c.a];
-      c.b = parent[c.b];
-      keep = c.a != c.b;
+// join two components (order does not matter).  Each thread takes kRfItems
+// edges per tile, so their parent gathers are in flight together, and the
+// block reserves its output with one atomicAdd per tile: the count is a single
+// address, and one atomic per warp serialised on it at the first rounds' edge
+// counts.
+constexpr int kRfItems = 4, kRfThreads = 256;
+__global__ void __launch_bounds__(kRfThreads)
+    k_relabel_filter(const CEdge *__restrict__ el, int64_t m, const int32_t *__restrict__ parent,
+                     CEdge *__restrict__ out, unsigned long long *__restrict__ out_count) {
+  __shared__ uint32_t wofs[kRfThreads / 32];
+  __shared__ unsigned long long bbase;
+  const int lane = lane_id(), w = threadIdx.x >> 5;
+  const int64_t tile = (int64_t)kRfThreads * kRfItems;
+  for (int64_t t0 = (int64_t)blockIdx.x * tile; t0 < m; t0 += (int64_t)gridDim.x * tile) {
+    CEdge c[kRfItems];
+    bool keep[kRfItems];
+#pragma unroll
+    for (int j = 0; j < kRfItems; j++) {
+      const int64_t i = t0 + (int64_t)j * kRfThreads + threadIdx.x;
+      keep[j] = i < m;
+      if (keep[j]) c[j] = el[i];
     }
-    uint32_t bal = __ballot_sync(0xffffffffu, keep);
-    unsigned long long base = 0;
-    if (lane == 0 && bal) base = atomicAdd(out_count, (unsigned long long)__popc(bal));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (keep) out[base + __popc(bal & lanemask_lt())] = c;
+#pragma unroll
+    for (int j = 0; j < kRfItems; j++) {
+      if (keep[j]) {
+        c[j].a = parent[c[j].a];
+        c[j].b = parent[c[j].b];
+        keep[j] = c[j].a != c[j].b;
+      }
+    }
+    uint32_t bal[kRfItems];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int j = 0; j < kRfItems; j++) {
+      bal[j] = __ballot_sync(0xffffffffu, keep[j]);
+      cnt += __popc(bal[j]);
+    }
+    if (lane == 0) wofs[w] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t tot = 0;
+      for (int k = 0; k < kRfThreads / 32; k++) {
+        const uint32_t v = wofs[k];
+        wofs[k] = tot;
+        tot += v;
+      }
+      bbase = tot ? atomicAdd(out_count, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long p = bbase + wofs[w];
+#pragma unroll
+    for (int j = 0; j < kRfItems; j++) {
+      if (keep[j]) out[p + __popc(bal[j] & lanemask_lt())] = c[j];
+      p += __popc(bal[j]);
+    }
+    __syncthreads();  // wofs and bbase are rewritten by the next tile
   }
 }
 
@@ -509,7 +557,8 @@ int64_t boruvka_mst(Context *ctx, const hdb_graph *g, uint8_t *in_mst, hdb_mst_e
     k_reset_minkey<<<gr, 256, 0, st>>>(rp, nr, minkey); ctx->launches++;
     k_jump<<<gr, 256, 0, st>>>(rp, nr, parent, ctx->dev_err); ctx->launches++;
     HDB_CUDA(cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(unsigned long long), st));
-    k_relabel_filter<<<ge, 256, 0, st>>>(ep, m, parent, ep2, counters.get() + 1); ctx->launches++;
+    k_relabel_filter<<<grid_for(ctx, (m + kRfItems - 1) / kRfItems, kRfThreads), kRfThreads, 0, st>>>(
+        ep, m, parent, ep2, counters.get() + 1); ctx->launches++;
     k_roots<<<gr, 256, 0, st>>>(rp, nr, parent, rp2, counters.get() + 2); ctx->launches++;
     HDB_CHECK_LAUNCH();
     HDB_CUDA(cudaMemcpyAsync(h, counters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
