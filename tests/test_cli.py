@@ -104,3 +104,24 @@ def test_text_vectors_and_fvecs_conversion(tmp_path):
     r = run(0, 8, 1, 0, "--vectors", fv, "--kgraph", kg, "--labels", lb)
     assert r.returncode == 0, r.stderr
     np.testing.assert_array_equal(np.loadtxt(la), np.loadtxt(lb))
+
+
+@pytest.mark.gpu
+def test_id_order_option(tmp_path, oracle):
+    """--id-order: the float MST under (weight, min id, max id), its sorted dump
+    and the labels equal the oracle's path in that order on the same graph."""
+    X = blobs(3000, 8, seed=7, blobs=6, spread=4.0)
+    vec = tmp_path / "vectors.fvecs"
+    write_fvecs(vec, X)
+    kg, ms, lab = tmp_path / "raw.kgraph", tmp_path / "mst.bin", tmp_path / "labels.txt"
+    r = run(3000, 16, 1, 0, "--vectors", vec, "--save-kgraph", kg)
+    assert r.returncode == 0, r.stderr
+    r = run(3000, 16, 1, 0, "--vectors", vec, "--kgraph", kg, "--id-order", "--save-mst", ms,
+            "--labels", lab)
+    assert r.returncode == 0, r.stderr
+    ids = decode(read_kgraph(kg)["label"])
+    fd = oracle.fix_distances(X, ids)
+    mst, labels, _ = oracle.hdbscan_from_knn(ids, fd, X, 16, order=oracle.ORDER_IDS)
+    np.testing.assert_array_equal(np.fromfile(ms, oracle.MST_EDGE).view(np.int32),
+                                  mst.view(np.int32))
+    np.testing.assert_array_equal(np.loadtxt(lab, dtype=np.int32), labels)
