@@ -94,7 +94,7 @@ static int cmp_i32(const void *x, const void *y) {
 typedef struct { int32_t target, id; float d; } orc_cand;
 
 /* Candidate distances of a precision form inside the local join (the
- * evaluation of the north star's BF16 and FP8 forms; the reference computes
+ * evaluation of the BF16, FP16 and FP8 e4m3 forms; the reference computes
  * every candidate distance as the FP32 difference sum).  q holds each row's
  * quantised coordinates (of the column-centred rows), scale a per-row scale
  * (NULL: 1), nrm the squared norm of the dequantised row; a pair's distance
