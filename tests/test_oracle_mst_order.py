@@ -4,6 +4,9 @@
 different trees, the edge order against the reference's own Kruskal +
 buildMST + sort_edges restatement, and the id order against a plain-Python
 Kruskal on tie-heavy graphs."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -105,3 +108,26 @@ def test_pipeline_with_the_id_order(oracle):
     want, _ = oracle.mst_ordered(ni, nl, ew, oracle.ORDER_IDS)
     np.testing.assert_array_equal(mst_i.view(np.int32), want.view(np.int32))
     assert lab_i.shape == lab_e.shape
+
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.rsplit("/", 1)[-1][4:-4])
+def test_orders_on_the_reference_fixtures(oracle, path):
+    """The edge order reproduces the reference's own sorted MST (cpuMST +
+    buildMST + sort_edges output stored in the fixture); the id order spans
+    the same weight multiset and differs only on tied weights."""
+    g = dict(np.load(path))
+    ref = next(g[k] for k in sorted(g) if k.startswith("mst_"))
+    e_mst, e_in = oracle.mst_ordered(g["nindex"], g["nlist"], g["eweight"], oracle.ORDER_EDGE)
+    np.testing.assert_array_equal(e_mst.view(np.int32), ref.view(np.int32))
+    i_mst, i_in = oracle.mst_ordered(g["nindex"], g["nlist"], g["eweight"], oracle.ORDER_IDS)
+    np.testing.assert_array_equal(np.sort(i_mst["weight"]), np.sort(ref["weight"]))
+    w = g["eweight"][e_in != i_in]
+    if len(w):
+        # every edge the orders disagree on has a weight that at least two
+        # undirected edges carry (each appears twice in the symmetric CSR)
+        vals, counts = np.unique(g["eweight"], return_counts=True)
+        tied = set(vals[counts > 2].tolist())
+        assert all(float(x) in tied for x in w)
