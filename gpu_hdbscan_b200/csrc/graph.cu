@@ -358,12 +358,22 @@ __global__ void __launch_bounds__(32 * kCoreWarps)
     for (int c0 = 0; c0 < d; c0 += kCoreCols) {
       const int wd = min(kCoreCols, d - c0);
       __syncwarp();
-      for (int i = 0; i < 32; i++) {
-        if (!((act >> i) & 1u)) continue;
-        const int32_t vi = __shfl_sync(0xffffffffu, v, i);  // the loop is warp-uniform
-        if (lane < wd) {
-          own[i * kCoreLd + lane] = X[(r0 + i) * d + c0 + lane];
-          nb[i * kCoreLd + lane] = X[(int64_t)vi * d + c0 + lane];
+      // eight rows' segments (own and neighbour) loaded before any is stored,
+      // so sixteen loads of the warp are in flight at a time
+      for (int i0 = 0; i0 < 32; i0 += 8) {
+        float xo[8], xn[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u;
+          const int32_t vi = __shfl_sync(0xffffffffu, v, i);
+          const bool ok = ((act >> i) & 1u) && lane < wd;
+          xo[u] = ok ? X[(r0 + i) * d + c0 + lane] : 0.0f;
+          xn[u] = ok ? X[(int64_t)vi * d + c0 + lane] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          own[(i0 + u) * kCoreLd + lane] = xo[u];
+          nb[(i0 + u) * kCoreLd + lane] = xn[u];
         }
       }
       __syncwarp();
